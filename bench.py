@@ -1,0 +1,420 @@
+"""Benchmark: the fused stencil-graph executor on the 512^3 field workload.
+
+Workload (one step): ``divergence(gradient(f)) + l2norm(curl(u))`` with the global
+sum / mean / variance of the result, periodic boundaries, unit spacing, on
+f: 512^3 scalar field (sum of 3 sinusoids + noise) and u: 512^3 x 3 vector field
+(N(0,1) per component, 5-point box filtered), seeded synthetic data. The
+expression rewrites div∘grad → laplacian, so a step is two fused passes
+(||curl u||^2 partials; then lap f + c with three reductions) plus finalizes.
+
+Storage forms, compute always FP32 with FP64 reductions:
+  fp32 — fields and result in FP32 (20 algorithmic bytes / voxel)
+  fp16 — fields and result in FP16 (10 B / voxel)   <- headline ("chosen form")
+  bf16 — fields and result in BF16 (10 B / voxel)
+
+``value`` = Gvoxel/s of the headline form, inputs resident in HBM, one step = one
+CUDA-graph replay of the whole plan (kernels + finalizes). ``e2e`` = the same step
+through the public API (compile_expression + Runtime.run) from pinned host
+buffers, with host->device copies of f and u and device->host reads of the result
+field and the three scalars inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--size S] [--forms fp32,fp16,bf16]
+
+Multi-GPU (torchrun): every rank runs an independent replica on its own fields
+(the path does not exchange data at this configuration); the step time is the
+max over ranks and ``value`` counts every rank's voxels.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+
+EXPR = "divergence(gradient(f)) + l2norm(curl(u))"
+REDS = ("sum", "mean", "variance")
+FORM_DT = {"fp32": torch.float32, "fp16": torch.float16, "bf16": torch.bfloat16}
+ALG_BYTES = {"fp32": 20, "fp16": 10, "bf16": 10}   # f + u(3) + out, each once
+HEADLINE = "fp16"
+
+
+def _peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def _barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(x: float, world: int, dev) -> float:
+    if world == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_fields(size, device):
+    from stenpy_b200.synth import sinusoid_field, smoothed_vector
+    f = sinusoid_field((size,) * 3, seed=0, device=device)
+    u = smoothed_vector((size,) * 3, seed=2, device=device)
+    return f, u
+
+
+def build(form, f, u, device):
+    import stenpy_b200 as S
+    from stenpy_b200 import fused_compiler as FC
+    dt = FORM_DT[form]
+    g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
+                                       field_map={"f": f.to(dt), "u": u.to(dt)})
+    wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
+    plan = FC.get_plan(g, wanted, out_dtype=dt)
+    values, back = FC.bind(plan, g, wanted)
+    prog = FC.build_program(plan, values, device)
+    return g, wanted, plan, prog
+
+
+def time_graph(replay, stream, steps, warmup, world, dev):
+    for _ in range(warmup):
+        replay()
+    torch.cuda.synchronize()
+    _barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for a, b in ev:
+        a.record(stream)
+        replay()
+        b.record(stream)
+    end.record(stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    torch.cuda.synchronize()
+    total = start.elapsed_time(end)
+    per = [a.elapsed_time(b) for a, b in ev]
+    return _max_over_ranks(total / steps, world, dev), per
+
+
+def kernel_times(prog, stream, reps=10):
+    """Average duration of each launch of the program, timed alone with CUDA events
+    on the launching stream (the same stream the step runs on)."""
+    from stenpy_b200 import _native as N
+    from stenpy_b200 import fused_compiler as FC
+    out = []
+    for op in prog.ops:
+        if not isinstance(op, FC.Launch):
+            continue
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            N.launch(op.module, op.grid, op.block, op.smem, stream.cuda_stream, op.params)
+        a.record(stream)
+        for _ in range(reps):
+            N.launch(op.module, op.grid, op.block, op.smem, stream.cuda_stream, op.params)
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append((op, a.elapsed_time(b) / reps))
+    return out
+
+
+def e2e_step(f_host, u_host, form, device):
+    """One step through the public API from pinned host buffers."""
+    import stenpy_b200 as S
+    dt = FORM_DT[form]
+    g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
+                                       field_map={"f": f_host, "u": u_host})
+    wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
+    res = S.Runtime(device=device, out_dtype=dt, check_errors=False).run(g, wanted=wanted)
+    out = res[sink].to("cpu")
+    scal = [res[w].to("cpu") for w in wanted[1:]]
+    return out, scal
+
+
+def measure_e2e(f, u, form, device, steps, world, dev):
+    dt = FORM_DT[form]
+    f_host = f.to(dt).cpu().pin_memory()
+    u_host = u.to(dt).cpu().pin_memory()
+    for _ in range(2):
+        e2e_step(f_host, u_host, form, device)
+    torch.cuda.synchronize()
+    _barrier(world)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    n = max(2, min(steps, 5))
+    t0.record()
+    for _ in range(n):
+        out, scal = e2e_step(f_host, u_host, form, device)
+    t1.record()
+    torch.cuda.synchronize()
+    ms = _max_over_ranks(t0.elapsed_time(t1) / n, world, dev)
+    es = f_host.element_size()
+    h2d = f_host.numel() * es + u_host.numel() * es
+    d2h = out.numel() * out.element_size() + 8 * len(scal)
+    return ms, h2d, d2h
+
+
+def cpu_reference_step(f_sample, u_sample):
+    """The reference algorithm (CPU FP64 oracle) on one bounded sample."""
+    from oracle import stenpy_oracle as O
+    import stenpy_b200 as S
+    g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
+                                       field_map={"f": f_sample.double(), "u": u_sample.double()})
+    wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
+    return O.evaluate(g, wanted), wanted
+
+
+def sample_planes(size):
+    return max(4, min(size, 32))
+
+
+def run_reference(args):
+    """--impl reference: the reference algorithm on the host cores (oracle port)."""
+    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    torch.set_num_threads(os.cpu_count() or 1)
+    from stenpy_b200.synth import sinusoid_field, smoothed_vector
+    P = sample_planes(args.size)
+    shape = (P, args.size, args.size)
+    f = sinusoid_field(shape, seed=0)
+    u = smoothed_vector(shape, seed=2)
+    for _ in range(args.warmup):
+        cpu_reference_step(f, u)
+    ts = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        cpu_reference_step(f, u)
+        ts.append(time.perf_counter() - t)
+    vox = P * args.size * args.size
+    v = vox / statistics.median(ts) / 1e9
+    line = {"metric": "fused-expr throughput (Gvoxel/s)", "value": v, "unit": "Gvoxel/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(ts) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{EXPR} + sum/mean/variance, periodic, {args.size}^3 (sample)",
+                       "sample": f"{P}x{args.size}x{args.size} planes per step"},
+            "cpu_baseline": {"value": v, "unit": "Gvoxel/s", "cores": torch.get_num_threads(), "kind": "port",
+                             "sample": f"{P}x{args.size}x{args.size} voxels per step, FP64 torch CPU oracle"},
+            "e2e": {"value": v, "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def errors_vs_fp64(f, u, device, forms):
+    """Norm-wise (max|y-y64|/max|y64|) and RMS relative errors of each form's result
+    and scalars against the FP64 oracle, on a 32-plane sample of the workload
+    (treated as its own periodic field). For narrow forms the error is reported
+    against FP64 on the stored (rounded) inputs and on the FP32 originals."""
+    import stenpy_b200 as S
+    P = sample_planes(f.shape[0])
+    fs, us = f[:P].contiguous(), u[:P].contiguous()
+    ref32, wanted = cpu_reference_step(fs.cpu(), us.cpu())
+    out = {}
+    for form in forms:
+        dt = FORM_DT[form]
+        g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
+                                           field_map={"f": fs.to(dt), "u": us.to(dt)})
+        w = [sink] + [g.add(r, (sink,), {}) for r in REDS]
+        res = S.Runtime(device=device, out_dtype=dt).run(g, wanted=w)
+        y = res[sink].double().cpu()
+        refq, wq = cpu_reference_step(fs.to(dt).cpu(), us.to(dt).cpu())
+        d = {}
+        for tag, ref, ws in (("vs_fp64_of_stored_inputs", refq, wq), ("vs_fp64_of_fp32_inputs", ref32, wanted)):
+            y64 = ref[ws[0]]
+            scale = y64.abs().max().item()
+            d[tag] = {"max_rel": (y - y64).abs().max().item() / scale,
+                      "rms_rel": ((y - y64) ** 2).mean().sqrt().item() / scale,
+                      "scalars_rel": {r: abs(float(res[w[i + 1]]) - float(ref[ws[i + 1]])) /
+                                      max(abs(float(ref[ws[i + 1]])), 1e-300) for i, r in enumerate(REDS)}}
+        out[form] = d
+    return out, f"{P}x{f.shape[1]}x{f.shape[2]} sample"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--forms", default="fp32,fp16,bf16")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error sample")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    world, rank, local = _dist()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from stenpy_b200 import fused_compiler as FC
+    forms = [x for x in args.forms.split(",") if x]
+    f, u = make_fields(args.size, dev)
+    n_vox = args.size ** 3
+    stream = torch.cuda.Stream(dev)
+    peak, peak_kind = _peaks()
+    results = {}
+    clocks = None
+    for form in forms:
+        g, wanted, plan, prog = build(form, f, u, dev)
+        with torch.cuda.stream(stream):
+            FC.enqueue(prog, stream)
+        torch.cuda.synchronize()
+        cg = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(cg, stream=stream):
+            n_launch = FC.enqueue(prog, stream)
+        if form == HEADLINE or clocks is None:
+            with ClockSampler(local) as cs:
+                ms, per = time_graph(cg.replay, stream, args.steps, args.warmup, world, dev)
+            if form == HEADLINE:
+                clocks = cs.summary()
+        else:
+            ms, per = time_graph(cg.replay, stream, args.steps, args.warmup, world, dev)
+        FC.ErrorFlag.check(dev)
+        kt = kernel_times(prog, stream)
+        main_k = [(op, t) for op, t in kt if op.module in [p.module for p in plan.passes]]
+        dom_op, dom_ms = max(main_k, key=lambda x: x[1])
+        dom_pass = [p for p in plan.passes if p.module == dom_op.module][0]
+        es = FORM_DT[form].itemsize
+        alg = sum(ESZ * nc for ESZ, nc in ((es, f_.nc) for f_ in dom_pass.spec.fields)) * n_vox
+        alg += sum(es * dom_pass.spec.graph.nodes[r.node].nc for r in dom_pass.spec.roots if r.kind == "out") * n_vox
+        results[form] = {
+            "gvox_s": n_vox * world / (ms * 1e-3) / 1e9, "ms_per_step": ms,
+            "step_GBps": ALG_BYTES[form] * n_vox / (ms * 1e-3) / 1e9,
+            "step_frac_of_peak": ALG_BYTES[form] * n_vox / (ms * 1e-3) / 1e9 / peak,
+            "launches_per_step": n_launch,
+            "kernels_ms": [round(t, 4) for _, t in kt],
+            "dominant": {"ms": dom_ms, "alg_bytes": alg, "GBps": alg / (dom_ms * 1e-3) / 1e9},
+        }
+        del cg
+    head = results[HEADLINE] if HEADLINE in results else results[forms[0]]
+    head_form = HEADLINE if HEADLINE in results else forms[0]
+    line = {"metric": "fused-expr throughput (Gvoxel/s), HBM roofline fraction, error vs FP64",
+            "value": head["gvox_s"], "unit": "Gvoxel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": head_form, "data": "synthetic",
+            "config": {"workload": f"{EXPR} + sum/mean/variance of the result, periodic, dx=1, "
+                                   f"{args.size}^3 f and {args.size}^3x3 u",
+                       "global_voxels": n_vox * world, "l2": "inputs (f, u) larger than L2 (126 MB)",
+                       "step": "one CUDA-graph replay of the fused plan (inputs resident in HBM)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": head["dominant"]["GBps"], "peak": peak, "unit": "GB/s",
+                         "frac": head["dominant"]["GBps"] / peak, "peak_kind": peak_kind,
+                         "traffic": None, "kernel": "dominant pass of the headline form",
+                         "step_frac": head["step_frac_of_peak"]},
+            "forms": results, "gpu_launches": head["launches_per_step"] * args.steps, "clocks": clocks}
+    if not args.no_e2e:
+        ms, h2d, d2h = measure_e2e(f, u, head_form, dev, args.steps, world, dev)
+        line["e2e"] = {"value": n_vox * world / (ms * 1e-3) / 1e9, "unit": "Gvoxel/s",
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms}
+    if rank == 0 and not args.no_cpu:
+        errs, sample = errors_vs_fp64(f, u, dev, forms)
+        line["error_vs_fp64"] = {"sample": sample, **errs}
+        torch.set_num_threads(os.cpu_count() or 1)
+        P = sample_planes(args.size)
+        fs, us = f[:P].cpu(), u[:P].cpu()
+        cpu_reference_step(fs, us)
+        ts = []
+        for _ in range(3):
+            t = time.perf_counter()
+            cpu_reference_step(fs, us)
+            ts.append(time.perf_counter() - t)
+        line["cpu_baseline"] = {"value": P * args.size ** 2 / statistics.median(ts) / 1e9, "unit": "Gvoxel/s",
+                                "cores": torch.get_num_threads(), "kind": "port",
+                                "sample": f"{P}x{args.size}x{args.size} voxels of the workload, FP64 torch CPU "
+                                          "oracle, median of 3 after 1 warm-up"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

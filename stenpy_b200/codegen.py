@@ -1,0 +1,941 @@
+"""CUDA C++ generation for one fused pass over a 3-D grid.
+
+A *pass* is one launch of a z-marching stencil kernel over an (n0, n1, n2) grid
+(C order, dim 2 contiguous). It evaluates a DAG of primitive per-voxel nodes
+(``PNode``) whose leaves are fields in HBM and scalars from the device scalar
+table, and for every voxel delivers its *roots*: values stored to output fields,
+values folded into FP64 reduction partials, and running (scan) integrals.
+
+Primitives (every graph operator is lowered onto these, see ``lowering.py``):
+
+* ``field`` / ``scalar`` leaves;
+* pointwise math: add sub mul div neg exp log sqrt sin cos tanh abs clamp, trace,
+  eig (3×3 symmetric eigenvalues), select, stack, normalize, norm;
+* ``d1``: first derivative of (one component of) a node along one axis, with the
+  edge rule of the operator that produced it — ``periodic`` (wrapped central
+  difference, torch.roll semantics), ``edge2`` / ``edge1`` (torch.gradient's
+  one-sided second/first-order edges), ``zero`` (axis of length 1);
+* ``lap``: compact 7-point Laplacian with a padding rule (periodic, replicate,
+  zero, reflect).
+
+Kernel shape (``emit_pass``): a CTA owns a TJ × TK tile of the (dim1, dim2) plane
+and marches along dim 0 over a segment of planes. Every field read at an offset
+is staged plane by plane into a shared-memory ring of 2R+1+P slots (R = the
+pass's stencil reach, P = prefetch depth), by TMA (``cp.async.bulk.tensor``, one
+elected thread, mbarrier completion) when the layout allows it, else by plain
+cooperative loads. Voxels at least R away from every face take the *fast* path:
+central formulas reading the ring at compile-time offsets. Voxels within R of a
+face take the *slow* path: the same DAG evaluated from global memory with each
+operator's own boundary rule. Compute is FP32; reductions accumulate in FP64.
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field as dc_field
+from typing import Dict, List, Optional, Sequence, Tuple
+
+HEADER_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "include", "sten_device.cuh")
+
+CTYPE = {"f32": "float", "f64": "double", "bf16": "bf16_t", "f16": "f16_t"}
+ESIZE = {"f32": 4, "f64": 8, "bf16": 2, "f16": 2}
+
+
+# ----------------------------------------------------------------------------- IR
+@dataclass
+class PNode:
+    id: int
+    op: str
+    ins: Tuple[int, ...]
+    nc: int
+    attrs: Tuple[Tuple[str, object], ...] = ()
+    radius: int = 0
+
+    def a(self, key, default=None):
+        for k, v in self.attrs:
+            if k == key:
+                return v
+        return default
+
+
+class PGraph:
+    """Hash-consed DAG of primitive nodes for one pass."""
+
+    def __init__(self) -> None:
+        self.nodes: List[PNode] = []
+        self._memo: Dict[Tuple, int] = {}
+
+    def add(self, op: str, ins: Sequence[int], nc: int, radius: int = 0, **attrs) -> int:
+        items = tuple(sorted(attrs.items()))
+        key = (op, tuple(ins), nc, items)
+        hit = self._memo.get(key)
+        if hit is not None:
+            return hit
+        nid = len(self.nodes)
+        self.nodes.append(PNode(nid, op, tuple(ins), nc, items, radius))
+        self._memo[key] = nid
+        return nid
+
+    def radius_of(self, nid: int) -> int:
+        return self.nodes[nid].radius
+
+
+@dataclass
+class FieldSpec:
+    slot: int           # index into Params::fld
+    dtype: str          # f32 / bf16 / f16 / f64
+    nc: int             # interleaved components per voxel (1, 3, 9)
+    staged: bool = False  # held in a shared-memory plane ring
+    tma: bool = False     # ring filled by TMA (else by cooperative loads)
+    halo: int = 0         # j/k halo of the staged tile (0 for fields read only at the voxel)
+
+
+@dataclass
+class RootSpec:
+    kind: str           # "out" | "red" | "scan" | "hist"
+    node: int           # PNode id
+    out_slot: int = -1  # for out/scan: index into Params::out
+    out_dtype: str = "f32"
+    red: str = ""       # sum | sumsq | var | entropy | integrate | minmax | hist
+    slot: int = -1      # first partial slot (red) / histogram base (hist)
+    bins: int = 0
+    lohi_index: int = -1  # hist: scalar-table index of (min, max)
+    dx: Tuple[float, float, float] = (1.0, 1.0, 1.0)  # integrate / scan spacing
+    method: str = "simpson"
+
+
+@dataclass
+class PassConfig:
+    tj: int = 8
+    tk: int = 64
+    threads: int = 128
+    prefetch: int = 2
+    seg_len: int = 64
+    min_blocks: int = 1
+
+
+@dataclass
+class PassSpec:
+    graph: PGraph
+    fields: List[FieldSpec]
+    roots: List[RootSpec]
+    n_scalars: int
+    nslots: int                 # FP64 partial slots per CTA
+    radius: int
+    cfg: PassConfig = dc_field(default_factory=PassConfig)
+    has_scan: bool = False
+
+    def hk(self, f: FieldSpec) -> int:
+        """k-halo in elements, rounded so TMA x-coordinates stay 16-byte aligned."""
+        if f.halo == 0:
+            return 0
+        a = 16 // ESIZE[f.dtype]
+        return ((f.halo + a - 1) // a) * a
+
+    def box(self, f: FieldSpec) -> Tuple[int, int]:
+        """(row width in elements, rows) of one staged plane tile."""
+        return ((self.cfg.tk + 2 * self.hk(f)) * f.nc, self.cfg.tj + 2 * f.halo)
+
+
+def _lit(x: float) -> str:
+    if x != x:
+        return "__int_as_float(0x7fc00000)"
+    if math.isinf(x):
+        return "__int_as_float(0x7f800000)" if x > 0 else "__int_as_float(0xff800000)"
+    return repr(float(x)) + "f"
+
+
+# ----------------------------------------------------------------------------- emitter
+class _Emitter:
+    def __init__(self, spec: PassSpec):
+        self.s = spec
+        self.g = spec.graph
+        self.R = spec.radius
+        self.lines: List[str] = []
+        self.tmp = 0
+        # which nodes need offset (fast) / point (slow) functions
+        self.need_fn = set()
+        for n in self.g.nodes:
+            if n.op in ("d1", "lap"):
+                self._mark(n.ins[0])
+
+    def _mark(self, nid: int) -> None:
+        if nid in self.need_fn:
+            return
+        self.need_fn.add(nid)
+        for i in self.g.nodes[nid].ins:
+            self._mark(i)
+
+    def t(self) -> str:
+        self.tmp += 1
+        return f"t{self.tmp}"
+
+    # -- pointwise op body: inputs are C array names, output array name o
+    def pointwise(self, n: PNode, ins: List[str], o: str, out: List[str]) -> None:
+        op = n.op
+        g = self.g
+
+        def comp(arr, nid, c):
+            return f"{arr}[{0 if g.nodes[nid].nc == 1 else c}]"
+
+        if op in ("add", "sub", "mul", "div"):
+            a, b = ins
+            for c in range(n.nc):
+                x, y = comp(a, n.ins[0], c), comp(b, n.ins[1], c)
+                if op == "div":
+                    out.append(f"{o}[{c}] = sten_div({x}, {y}, {_lit(n.a('eps', 1e-15))});")
+                else:
+                    sym = {"add": "+", "sub": "-", "mul": "*"}[op]
+                    out.append(f"{o}[{c}] = {x} {sym} {y};")
+        elif op == "mulk":
+            for c in range(n.nc):
+                out.append(f"{o}[{c}] = {ins[0]}[{c}] * {_lit(n.a('k'))};")
+        elif op in ("neg", "exp", "sin", "cos", "tanh", "abs"):
+            fn = {"neg": "-", "exp": "expf", "sin": "sinf", "cos": "cosf", "tanh": "tanhf", "abs": "fabsf"}[op]
+            for c in range(n.nc):
+                out.append(f"{o}[{c}] = {fn}({ins[0]}[{c}]);")
+        elif op == "log":
+            for c in range(n.nc):
+                out.append(f"{o}[{c}] = sten_log({ins[0]}[{c}], {_lit(n.a('eps', 1e-15))});")
+        elif op == "sqrt":
+            for c in range(n.nc):
+                out.append(f"{o}[{c}] = sten_sqrt({ins[0]}[{c}], {_lit(n.a('eps', 0.0))});")
+        elif op == "clamp":
+            lo = comp(ins[1], n.ins[1], 0) if len(ins) > 1 else _lit(n.a("lo", 0.0))
+            hi = comp(ins[2], n.ins[2], 0) if len(ins) > 2 else _lit(n.a("hi", 1.0))
+            for c in range(n.nc):
+                lo_c = comp(ins[1], n.ins[1], c) if len(ins) > 1 else lo
+                hi_c = comp(ins[2], n.ins[2], c) if len(ins) > 2 else hi
+                out.append(f"{o}[{c}] = sten_clamp({ins[0]}[{c}], {lo_c}, {hi_c});")
+        elif op == "trace":
+            out.append(f"{o}[0] = {ins[0]}[0] + {ins[0]}[4] + {ins[0]}[8];")
+        elif op == "eig":
+            out.append(f"eig3_sym({ins[0]}, {o});")
+        elif op == "select":
+            k = int(n.a("index"))
+            for c in range(n.nc):
+                out.append(f"{o}[{c}] = {ins[0]}[{k * n.nc + c}];")
+        elif op == "stack":
+            c = 0
+            for arr, nid in zip(ins, n.ins):
+                for cc in range(g.nodes[nid].nc):
+                    out.append(f"{o}[{c}] = {arr}[{cc}];")
+                    c += 1
+        elif op == "normalize":
+            a = ins[0]
+            m = self.t()
+            out.append(f"float {m} = sqrtf({a}[0]*{a}[0] + {a}[1]*{a}[1] + {a}[2]*{a}[2]);")
+            out.append(f"{m} = fmaxf({m}, {_lit(n.a('eps', 1e-15))});")
+            for c in range(3):
+                out.append(f"{o}[{c}] = {a}[{c}] / {m};")
+        elif op == "norm":
+            a = ins[0]
+            out.append(f"{o}[0] = sqrtf({' + '.join(f'{a}[{c}]*{a}[{c}]' for c in range(self.g.nodes[n.ins[0]].nc))});")
+        else:
+            raise NotImplementedError(f"codegen: pointwise op {op}")
+
+    # -- fast (interior) functions: template offsets
+    def emit_fast_fns(self) -> None:
+        for n in self.g.nodes:
+            if n.id not in self.need_fn:
+                continue
+            body: List[str] = []
+            self.fast_value(n, "DI", "DJ", "DK", "o", body)
+            self.lines.append(f"template <int DI, int DJ, int DK> __device__ __forceinline__ void "
+                              f"FF{n.id}(const FCtx& x, float* o) {{")
+            self.lines += ["  " + b for b in body]
+            self.lines.append("}")
+
+    def fast_call(self, nid: int, di: str, dj: str, dk: str, body: List[str]) -> str:
+        arr = self.t()
+        body.append(f"float {arr}[{self.g.nodes[nid].nc}];")
+        n = self.g.nodes[nid]
+        if n.op == "field":
+            self.field_fast(n, di, dj, dk, arr, body)
+        elif n.op == "scalar":
+            body.append(f"{arr}[0] = x.sc[{n.a('index')}];")
+        else:
+            body.append(f"FF{nid}<{di}, {dj}, {dk}>(x, {arr});")
+        return arr
+
+    def field_fast(self, n: PNode, di, dj, dk, arr, body):
+        f = self.s.fields[n.a("field")]
+        if f.staged:
+            w = self.s.box(f)[0]
+            for c in range(n.nc):
+                body.append(f"{arr}[{c}] = ld_as_f32(x.pl{f.slot}[({di}) + {self.R}] + x.o{f.slot}"
+                            f" + ({dj}) * {w} + ({dk}) * {f.nc} + {c});")
+        elif di != "0" or dj != "0" or dk != "0":
+            raise AssertionError("unstaged field read at an offset")
+        else:
+            for c in range(n.nc):
+                body.append(f"{arr}[{c}] = ldg_as_f32(x.gp{f.slot} + {c});")
+
+    def fast_value(self, n: PNode, di: str, dj: str, dk: str, o: str, body: List[str]) -> None:
+        """Statements computing node n at offset (di,dj,dk) into array o (interior)."""
+        if n.op == "field":
+            self.field_fast(n, di, dj, dk, o, body)
+            return
+        if n.op == "scalar":
+            body.append(f"{o}[0] = x.sc[{n.a('index')}];")
+            return
+        if n.op == "d1":
+            ax = n.a("axis")
+            comp = n.a("comp")
+            mode = n.a("mode")
+            if mode == "zero":
+                for c in range(n.nc):
+                    body.append(f"{o}[{c}] = 0.0f;")
+                return
+            off = [di, dj, dk]
+            plus = list(off); plus[ax] = f"({off[ax]}) + 1"
+            minus = list(off); minus[ax] = f"({off[ax]}) - 1"
+            a = self.fast_call(n.ins[0], *plus, body)
+            b = self.fast_call(n.ins[0], *minus, body)
+            s = _lit(n.a("inv2h"))
+            for c in range(n.nc):
+                cc = c if comp is None else comp
+                body.append(f"{o}[{c}] = ({a}[{cc}] - {b}[{cc}]) * {s};")
+            return
+        if n.op == "lap":
+            off = [di, dj, dk]
+            ctr = self.fast_call(n.ins[0], di, dj, dk, body)
+            terms = []
+            for ax in range(3):
+                plus = list(off); plus[ax] = f"({off[ax]}) + 1"
+                minus = list(off); minus[ax] = f"({off[ax]}) - 1"
+                a = self.fast_call(n.ins[0], *plus, body)
+                b = self.fast_call(n.ins[0], *minus, body)
+                terms.append((a, b, _lit(n.a("invh2")[ax])))
+            for c in range(n.nc):
+                parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
+                body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
+            return
+        ins = [self.fast_call(i, di, dj, dk, body) for i in n.ins]
+        self.pointwise(n, ins, o, body)
+
+    # -- slow (boundary) functions: runtime global coordinates
+    def emit_slow_fns(self) -> None:
+        order = sorted(self.need_fn)
+        for nid in order:
+            self.lines.append(f"__device__ __noinline__ void SS{nid}(const Params& p, "
+                              f"int i, int j, int k, float* o);")
+        for nid in order:
+            n = self.g.nodes[nid]
+            body: List[str] = []
+            self.slow_value(n, "i", "j", "k", "o", body)
+            self.lines.append(f"__device__ __noinline__ void SS{nid}(const Params& p, "
+                              f"int i, int j, int k, float* o) {{")
+            self.lines += ["  " + b for b in body]
+            self.lines.append("}")
+
+    def slow_call(self, nid: int, i: str, j: str, k: str, body: List[str]) -> str:
+        arr = self.t()
+        n = self.g.nodes[nid]
+        body.append(f"float {arr}[{n.nc}];")
+        if n.op == "field":
+            self.field_slow(n, i, j, k, arr, body)
+        elif n.op == "scalar":
+            body.append(f"{arr}[0] = (float)p.scal[{n.a('index')}];")
+        elif nid in self.need_fn:
+            body.append(f"SS{nid}(p, {i}, {j}, {k}, {arr});")
+        else:
+            self.slow_value(n, i, j, k, arr, body)
+        return arr
+
+    def field_slow(self, n: PNode, i, j, k, arr, body):
+        f = self.s.fields[n.a("field")]
+        ct = CTYPE[f.dtype]
+        base = self.t()
+        body.append(f"const {ct}* {base} = (const {ct}*)p.fld[{f.slot}] + "
+                    f"(((size_t)sten_plane(p, {i}) * p.n1 + ({j})) * p.n2 + ({k})) * {f.nc};")
+        for c in range(n.nc):
+            body.append(f"{arr}[{c}] = ldg_as_f32({base} + {c});")
+
+    def slow_value(self, n: PNode, i: str, j: str, k: str, o: str, body: List[str]) -> None:
+        if n.op == "field":
+            self.field_slow(n, i, j, k, o, body)
+            return
+        if n.op == "scalar":
+            body.append(f"{o}[0] = (float)p.scal[{n.a('index')}];")
+            return
+        if n.op == "d1":
+            self.slow_d1(n, i, j, k, o, body)
+            return
+        if n.op == "lap":
+            self.slow_lap(n, i, j, k, o, body)
+            return
+        ins = [self.slow_call(x, i, j, k, body) for x in n.ins]
+        self.pointwise(n, ins, o, body)
+
+    def slow_d1(self, n: PNode, i, j, k, o, body):
+        ax = n.a("axis")
+        mode = n.a("mode")
+        comp = n.a("comp")
+        nn = ["p.n0g", "p.n1", "p.n2"][ax]
+        crd = [i, j, k]
+        cc = (lambda c: c) if comp is None else (lambda c: comp)
+        if mode == "zero":
+            for c in range(n.nc):
+                body.append(f"{o}[{c}] = 0.0f;")
+            return
+
+        def at(expr):
+            q = list(crd)
+            q[ax] = expr
+            return q
+
+        x = crd[ax]
+        s2 = _lit(n.a("inv2h"))
+        if mode == "periodic":
+            a = self.slow_call(n.ins[0], *at(f"wrap_idx(({x}) + 1, {nn})"), body)
+            b = self.slow_call(n.ins[0], *at(f"wrap_idx(({x}) - 1, {nn})"), body)
+            for c in range(n.nc):
+                body.append(f"{o}[{c}] = ({a}[{cc(c)}] - {b}[{cc(c)}]) * {s2};")
+            return
+        # torch.gradient edges: second order (edge2) or first order (edge1)
+        body.append(f"if (({x}) == 0) {{")
+        sub: List[str] = []
+        if mode == "edge2":
+            e0 = self.slow_call(n.ins[0], *at("0"), sub)
+            e1 = self.slow_call(n.ins[0], *at("1"), sub)
+            e2 = self.slow_call(n.ins[0], *at("2"), sub)
+            for c in range(n.nc):
+                sub.append(f"{o}[{c}] = ((-3.0f * {e0}[{cc(c)}] + 4.0f * {e1}[{cc(c)}]) - {e2}[{cc(c)}]) * {s2};")
+        else:
+            s1 = _lit(n.a("invh"))
+            e0 = self.slow_call(n.ins[0], *at("0"), sub)
+            e1 = self.slow_call(n.ins[0], *at("1"), sub)
+            for c in range(n.nc):
+                sub.append(f"{o}[{c}] = ({e1}[{cc(c)}] - {e0}[{cc(c)}]) * {s1};")
+        body += ["  " + s for s in sub]
+        body.append(f"}} else if (({x}) == {nn} - 1) {{")
+        sub = []
+        if mode == "edge2":
+            e0 = self.slow_call(n.ins[0], *at(f"{nn} - 1"), sub)
+            e1 = self.slow_call(n.ins[0], *at(f"{nn} - 2"), sub)
+            e2 = self.slow_call(n.ins[0], *at(f"{nn} - 3"), sub)
+            for c in range(n.nc):
+                sub.append(f"{o}[{c}] = ((3.0f * {e0}[{cc(c)}] - 4.0f * {e1}[{cc(c)}]) + {e2}[{cc(c)}]) * {s2};")
+        else:
+            s1 = _lit(n.a("invh"))
+            e0 = self.slow_call(n.ins[0], *at(f"{nn} - 1"), sub)
+            e1 = self.slow_call(n.ins[0], *at(f"{nn} - 2"), sub)
+            for c in range(n.nc):
+                sub.append(f"{o}[{c}] = ({e0}[{cc(c)}] - {e1}[{cc(c)}]) * {s1};")
+        body += ["  " + s for s in sub]
+        body.append("} else {")
+        sub = []
+        a = self.slow_call(n.ins[0], *at(f"({x}) + 1"), sub)
+        b = self.slow_call(n.ins[0], *at(f"({x}) - 1"), sub)
+        for c in range(n.nc):
+            sub.append(f"{o}[{c}] = ({a}[{cc(c)}] - {b}[{cc(c)}]) * {s2};")
+        body += ["  " + s for s in sub]
+        body.append("}")
+
+    def slow_lap(self, n: PNode, i, j, k, o, body):
+        pad = n.a("pad")
+        crd = [i, j, k]
+        dims = ["p.n0g", "p.n1", "p.n2"]
+        ctr = self.slow_call(n.ins[0], i, j, k, body)
+        terms = []
+        for ax in range(3):
+            nn = dims[ax]
+            x = crd[ax]
+            vals = []
+            for sgn in ("+ 1", "- 1"):
+                q = list(crd)
+                arr = self.t()
+                body.append(f"float {arr}[{n.nc}];")
+                if pad == "periodic":
+                    q[ax] = f"wrap_idx(({x}) {sgn}, {nn})"
+                    got = self.slow_call(n.ins[0], *q, body)
+                    body.append(f"for (int c = 0; c < {n.nc}; ++c) {arr}[c] = {got}[c];")
+                elif pad == "replicate":
+                    q[ax] = f"clamp_idx(({x}) {sgn}, {nn})"
+                    got = self.slow_call(n.ins[0], *q, body)
+                    body.append(f"for (int c = 0; c < {n.nc}; ++c) {arr}[c] = {got}[c];")
+                elif pad == "reflect":
+                    q[ax] = f"reflect_idx(({x}) {sgn}, {nn})"
+                    body.append(f"if ({nn} > 1) {{")
+                    sub: List[str] = []
+                    got = self.slow_call(n.ins[0], *q, sub)
+                    sub.append(f"for (int c = 0; c < {n.nc}; ++c) {arr}[c] = {got}[c];")
+                    body += ["  " + s for s in sub]
+                    body.append(f"}} else {{ for (int c = 0; c < {n.nc}; ++c) {arr}[c] = 0.0f; }}")
+                else:  # zero padding
+                    q[ax] = f"(({x}) {sgn})"
+                    body.append(f"if (({x}) {sgn} >= 0 && ({x}) {sgn} < {nn}) {{")
+                    sub = []
+                    got = self.slow_call(n.ins[0], *q, sub)
+                    sub.append(f"for (int c = 0; c < {n.nc}; ++c) {arr}[c] = {got}[c];")
+                    body += ["  " + s for s in sub]
+                    body.append(f"}} else {{ for (int c = 0; c < {n.nc}; ++c) {arr}[c] = 0.0f; }}")
+                vals.append(arr)
+            terms.append((vals[0], vals[1], _lit(n.a("invh2")[ax])))
+        for c in range(n.nc):
+            parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
+            body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
+
+    # -- per-voxel root evaluation
+    def emit_eval(self) -> None:
+        roots = self.s.roots
+        widths = [self.g.nodes[r.node].nc for r in roots]
+        self.offsets = []
+        acc = 0
+        for w in widths:
+            self.offsets.append(acc)
+            acc += w
+        self.nroot = max(acc, 1)
+        # fast
+        body: List[str] = []
+        memo: Dict[int, str] = {}
+
+        def point(nid: int) -> str:
+            if nid in memo:
+                return memo[nid]
+            n = self.g.nodes[nid]
+            if n.op in ("d1", "lap") or n.op == "field" or n.op == "scalar":
+                arr = self.t()
+                body.append(f"float {arr}[{n.nc}];")
+                self.fast_value(n, "0", "0", "0", arr, body)
+            else:
+                ins = [point(i) for i in n.ins]
+                arr = self.t()
+                body.append(f"float {arr}[{n.nc}];")
+                self.pointwise(n, ins, arr, body)
+            memo[nid] = arr
+            return arr
+
+        for r, off in zip(roots, self.offsets):
+            arr = point(r.node)
+            for c in range(self.g.nodes[r.node].nc):
+                body.append(f"rv[{off + c}] = {arr}[{c}];")
+        self.lines.append("__device__ __forceinline__ void eval_fast(const FCtx& x, float* rv) {")
+        self.lines += ["  " + b for b in body]
+        self.lines.append("}")
+        # slow
+        body = []
+        memo_s: Dict[int, str] = {}
+
+        def spoint(nid: int) -> str:
+            if nid in memo_s:
+                return memo_s[nid]
+            n = self.g.nodes[nid]
+            if nid in self.need_fn or n.op in ("d1", "lap", "field", "scalar"):
+                arr = self.t()
+                body.append(f"float {arr}[{n.nc}];")
+                self.slow_value(n, "i", "j", "k", arr, body)
+            else:
+                ins = [spoint(i) for i in n.ins]
+                arr = self.t()
+                body.append(f"float {arr}[{n.nc}];")
+                self.pointwise(n, ins, arr, body)
+            memo_s[nid] = arr
+            return arr
+
+        for r, off in zip(roots, self.offsets):
+            arr = spoint(r.node)
+            for c in range(self.g.nodes[r.node].nc):
+                body.append(f"rv[{off + c}] = {arr}[{c}];")
+        self.lines.append("__device__ __forceinline__ void eval_slow(const Params& p, "
+                          "int i, int j, int k, float* rv) {")
+        self.lines += ["  " + b for b in body]
+        self.lines.append("}")
+
+
+# ----------------------------------------------------------------------------- params layout
+@dataclass
+class ParamLayout:
+    size: int
+    offsets: Dict[str, int]
+
+
+def param_layout(spec: PassSpec) -> ParamLayout:
+    """Byte layout of ``struct Params`` (mirrors C++ alignment rules)."""
+    off = 0
+    offs: Dict[str, int] = {}
+
+    def put(name, size, align):
+        nonlocal off
+        off = (off + align - 1) // align * align
+        offs[name] = off
+        off += size
+
+    ntma = sum(1 for f in spec.fields if f.tma)
+    if ntma:
+        put("tmap", 128 * ntma, 64)
+    put("fld", 8 * max(len(spec.fields), 1), 8)
+    nout = sum(1 for r in spec.roots if r.kind in ("out", "scan"))
+    put("out", 8 * max(nout, 1), 8)
+    put("scal", 8, 8)
+    put("part", 8, 8)
+    put("hist", 8, 8)
+    put("err", 8, 8)
+    for name in ("n0g", "n1", "n2", "nl", "i_base", "out_lo", "n_out", "seg_len", "tiles_k", "cta_off"):
+        put(name, 4, 4)
+    size = (off + 63) // 64 * 64
+    return ParamLayout(size, offs)
+
+
+# ----------------------------------------------------------------------------- kernel
+def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
+    """(total bytes, byte offset of each staged field's ring, offset of the
+    block-reduction scratch). Ring slots are 128-byte aligned (TMA destinations)."""
+    nslot = 2 * spec.radius + 1 + spec.cfg.prefetch
+    off = 128  # mbarriers: up to 16 slots
+    rings: Dict[int, int] = {}
+    for f in spec.fields:
+        if f.staged:
+            rings[f.slot] = off
+            off += plane_bytes(spec, f) * nslot
+    off = (off + 127) // 128 * 128
+    red_off = off
+    off += 3 * 32 * 8
+    return off, rings, red_off
+
+
+def plane_bytes(spec: PassSpec, f: FieldSpec) -> int:
+    w, h = spec.box(f)
+    return ((w * h * ESIZE[f.dtype]) + 127) // 128 * 128
+
+
+def _simpson_fn() -> str:
+    return r"""
+__device__ __forceinline__ double sten_simpson_w(int idx, int n, double h, int simpson) {
+  // weight of sample idx in _simpson_1d's composite rule (or the trapezoid rule)
+  if (!simpson || n < 3) {
+    if (n < 2) return 0.0;
+    return (idx == 0 || idx == n - 1) ? 0.5 * h : h;
+  }
+  const int m = (n % 2 == 1) ? n : n - 1;   // Simpson over the first m points
+  double w = 0.0;
+  if (idx < m) {
+    w = (idx == 0 || idx == m - 1) ? 1.0 : ((idx % 2 == 1) ? 4.0 : 2.0);
+    w *= h / 3.0;
+  }
+  if (n % 2 == 0 && (idx == n - 2 || idx == n - 1)) w += 0.5 * h;
+  return w;
+}
+"""
+
+
+def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
+    """Per-voxel root handling (stores, reduction accumulation, scans). Expects
+    ``rv`` (root values), ``vox`` (linear voxel index), ``gi, j, k`` and, for scans,
+    the register slot ``m``."""
+    K: List[str] = []
+    ri = si = 0
+    for r, off in zip(spec.roots, e.offsets):
+        nc = e.g.nodes[r.node].nc
+        if r.kind == "out":
+            ct = CTYPE[r.out_dtype]
+            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - (size_t)p.out_lo * p.n1 * p.n2) * {nc};")
+            for c in range(nc):
+                K.append(f"  st_from_f32(o_ + {c}, rv[{off + c}]);")
+            K.append("}")
+        elif r.kind == "scan":
+            assert scan_ok
+            ct = CTYPE[r.out_dtype]
+            half = repr(0.5 * float(r.dx[0]))
+            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - (size_t)p.out_lo * p.n1 * p.n2) * {nc};")
+            for c in range(nc):
+                q = f"m * {nc} + {c}"
+                K.append(f"  if (gi > 0) sc{si}_acc[{q}] += ((double)sc{si}_prev[{q}] + (double)rv[{off + c}]) * {half};")
+                K.append(f"  sc{si}_prev[{q}] = rv[{off + c}];")
+                K.append(f"  st_from_f64(o_ + {c}, sc{si}_acc[{q}]);")
+            K.append("}")
+            si += 1
+        elif r.kind == "red":
+            for c in range(nc):
+                val = f"(double)rv[{off + c}]"
+                if r.red == "sum":
+                    K.append(f"rv{ri}_a += {val};")
+                elif r.red == "sumsq":
+                    K.append(f"{{ const double t_ = {val}; rv{ri}_a += t_ * t_; }}")
+                elif r.red == "var":
+                    K.append(f"{{ const double t_ = {val}; if (!rv{ri}_h) {{ rv{ri}_piv = t_; rv{ri}_h = true; }}"
+                             f" const double d_ = t_ - rv{ri}_piv; rv{ri}_s1 += d_; rv{ri}_s2 += d_ * d_; rv{ri}_n += 1.0; }}")
+                elif r.red == "entropy":
+                    K.append(f"{{ const double a_ = fabs({val}); rv{ri}_a += a_; if (a_ > 0.0) rv{ri}_b += a_ * log(a_); }}")
+                elif r.red == "minmax":
+                    K.append(f"{{ const double t_ = {val}; rv{ri}_a = fmin(rv{ri}_a, t_); rv{ri}_b = fmax(rv{ri}_b, t_); }}")
+                elif r.red == "integrate":
+                    sm = 1 if r.method == "simpson" else 0
+                    K.append(f"rv{ri}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
+                             f" * sten_simpson_w(j, p.n1, {r.dx[1]!r}, {sm}) * sten_simpson_w(k, p.n2, {r.dx[2]!r}, {sm});")
+                else:
+                    raise NotImplementedError(r.red)
+            ri += 1
+        else:
+            raise NotImplementedError(r.kind)
+    return K
+
+
+def _red_decls(spec: PassSpec) -> List[str]:
+    K: List[str] = []
+    for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
+        if r.red == "var":
+            K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0, rv{ri}_n = 0.0; bool rv{ri}_h = false;")
+        elif r.red in ("entropy",):
+            K.append(f"double rv{ri}_a = 0.0, rv{ri}_b = 0.0;")
+        elif r.red == "minmax":
+            K.append(f"double rv{ri}_a = __longlong_as_double(0x7ff0000000000000ll), "
+                     f"rv{ri}_b = __longlong_as_double(0xfff0000000000000ll);")
+        else:
+            K.append(f"double rv{ri}_a = 0.0;")
+    return K
+
+
+def _red_flush(spec: PassSpec, cta: str) -> List[str]:
+    """Block-reduce each accumulator and write this CTA's partial row."""
+    K: List[str] = []
+    for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
+        base = f"p.part[(size_t)({cta}) * NSLOTS_RED + {r.slot}"
+        if r.red == "var":
+            K.append(f"{{ double n_ = rv{ri}_n, mu_ = 0.0, q_ = 0.0;")
+            K.append(f"  if (n_ > 0.0) {{ mu_ = rv{ri}_piv + rv{ri}_s1 / n_; q_ = rv{ri}_s2 - rv{ri}_s1 * rv{ri}_s1 / n_; if (q_ < 0.0) q_ = 0.0; }}")
+            K.append("  block_chan(n_, mu_, q_, red_scratch);")
+            K.append(f"  if (tid == 0) {{ {base}] = n_; {base} + 1] = mu_; {base} + 2] = q_; }} }}")
+        elif r.red == "entropy":
+            K.append(f"{{ const double a_ = block_sum(rv{ri}_a, red_scratch); const double b_ = block_sum(rv{ri}_b, red_scratch);")
+            K.append(f"  if (tid == 0) {{ {base}] = a_; {base} + 1] = b_; }} }}")
+        elif r.red == "minmax":
+            K.append(f"{{ const double a_ = block_min(rv{ri}_a, red_scratch); const double b_ = block_max(rv{ri}_b, red_scratch);")
+            K.append(f"  if (tid == 0) {{ {base}] = a_; {base} + 1] = b_; }} }}")
+        else:
+            K.append(f"{{ const double a_ = block_sum(rv{ri}_a, red_scratch); if (tid == 0) {base}] = a_; }}")
+    return K
+
+
+def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Optional[int] = None) -> int:
+    """Voxels of global planes [g_lo, g_hi) that lie within R of a face (the shell
+    kernel's domain); mirrors the decode in ``sten_shell``."""
+    n0, n1, n2 = shape
+    g_hi = n0 if g_hi is None else g_hi
+    a1, a2 = max(n1 - 2 * R, 0), max(n2 - 2 * R, 0)
+    c_low = max(0, min(g_hi, R) - g_lo)
+    hs = max(g_lo, max(n0 - R, R))
+    c_high = max(0, g_hi - hs)
+    ii0 = max(g_lo, R)
+    n_int = max(0, min(g_hi, n0 - R) - ii0)
+    return (c_low + c_high) * n1 * n2 + n_int * (n1 - a1) * n2 + n_int * a1 * (n2 - a2)
+
+
+SHELL_THREADS = 256
+
+
+def emit_pass(spec: PassSpec) -> str:
+    """Source of the pass: ``sten_kernel`` (z-march over the tile grid) and, when the
+    pass has a stencil reach R > 0 and no scan, ``sten_shell`` (one thread per voxel
+    within R of a face, evaluated from global memory with boundary rules)."""
+    with open(HEADER_PATH) as fh:
+        header = fh.read()
+    e = _Emitter(spec)
+    cfg = spec.cfg
+    R = spec.radius
+    split = R > 0 and not spec.has_scan
+    nslot = 2 * R + 1 + cfg.prefetch
+    assert nslot <= 16, "too many ring slots"
+    assert cfg.tk % 32 == 0 and (cfg.tj * cfg.tk) % cfg.threads == 0 and cfg.prefetch >= 1
+    vpt = cfg.tj * cfg.tk // cfg.threads
+    L = e.lines
+    L.append(header)
+    L.append(f"#define TJ {cfg.tj}\n#define TK {cfg.tk}\n#define NT {cfg.threads}\n#define RAD {R}"
+             f"\n#define NSLOT {nslot}\n#define VPT {vpt}\n#define NSLOTS_RED {max(spec.nslots, 1)}")
+    ntma = sum(1 for f in spec.fields if f.tma)
+    nout = sum(1 for r in spec.roots if r.kind in ("out", "scan"))
+    L.append("struct __align__(64) Params {")
+    if ntma:
+        L.append(f"  TmaDesc tmap[{ntma}];")
+    L.append(f"  const void* fld[{max(len(spec.fields), 1)}];")
+    L.append(f"  void* out[{max(nout, 1)}];")
+    L.append("  const double* scal; double* part; unsigned int* hist; int* err;")
+    L.append("  int n0g, n1, n2, nl, i_base, out_lo, n_out, seg_len, tiles_k, cta_off;")
+    L.append("};")
+    L.append("__device__ __forceinline__ int sten_plane(const Params& p, int gi) {")
+    L.append("  // global plane index -> plane of the (possibly chunked) arrays")
+    L.append("  int l = gi - p.i_base;")
+    L.append("  if (l < 0) l += p.n0g; else if (l >= p.nl) l -= p.n0g;")
+    L.append("  return l;")
+    L.append("}")
+    L.append("struct FCtx {")
+    for f in spec.fields:
+        ct = CTYPE[f.dtype]
+        if f.staged:
+            L.append(f"  const {ct}* pl{f.slot}[2 * RAD + 1]; int o{f.slot};")
+        else:
+            L.append(f"  const {ct}* gp{f.slot};")
+    L.append(f"  float sc[{max(spec.n_scalars, 1)}];")
+    L.append("};")
+    e.emit_fast_fns()
+    e.emit_slow_fns()
+    e.emit_eval()
+    nroot = e.nroot
+    L.append(_simpson_fn())
+    tma_fields = [f for f in spec.fields if f.tma]
+    lsu_fields = [f for f in spec.fields if f.staged and not f.tma]
+    total_smem, rings, red_off = smem_layout(spec)
+    tma_bytes = sum(spec.box(f)[0] * spec.box(f)[1] * ESIZE[f.dtype] for f in tma_fields)
+    reds = [r for r in spec.roots if r.kind == "red"]
+    scans = [r for r in spec.roots if r.kind == "scan"]
+
+    K: List[str] = []
+    K.append(f'extern "C" __global__ void __launch_bounds__(NT, {cfg.min_blocks}) '
+             f"sten_kernel(const __grid_constant__ Params p) {{")
+    K.append("  extern __shared__ __align__(128) unsigned char smem[];")
+    K.append("  u64* bars = (u64*)smem;")
+    K.append(f"  double* red_scratch = (double*)(smem + {red_off});")
+    K.append("  const int tid = threadIdx.x;")
+    K.append("  const int tile = blockIdx.x;")
+    K.append("  const int tk0 = (tile % p.tiles_k) * TK;")
+    K.append("  const int tj0 = (tile / p.tiles_k) * TJ;")
+    K.append("  const int ib = p.out_lo + (int)blockIdx.y * p.seg_len;")
+    K.append("  const int ie = min(ib + p.seg_len, p.out_lo + p.n_out);")
+    K.append("  const int cta = p.cta_off + (int)(blockIdx.y * gridDim.x + blockIdx.x);")
+    K.append("  FCtx x;")
+    K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
+             f"x.sc[s] = (s < {spec.n_scalars}) ? (float)p.scal[s] : 0.0f;")
+    K += ["  " + k for k in _red_decls(spec)]
+    for si, r in enumerate(scans):
+        nc = e.g.nodes[r.node].nc
+        K.append(f"  double sc{si}_acc[VPT * {nc}]; float sc{si}_prev[VPT * {nc}];")
+        K.append(f"  #pragma unroll\n  for (int q = 0; q < VPT * {nc}; ++q) {{ sc{si}_acc[q] = 0.0; sc{si}_prev[q] = 0.0f; }}")
+    staged = tma_fields or lsu_fields
+    K.append("  const int p_first = ib - RAD;")
+    if tma_fields:
+        K.append("  if (tid == 0) {")
+        K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
+        K.append("    fence_mbar_init();")
+        for ti in range(len(tma_fields)):
+            K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
+        K.append("  }")
+        K.append("  __syncthreads();")
+    if staged:
+        K.append("  auto request = [&](int q) {")
+        K.append("    const int s = (q - p_first) % NSLOT;")
+        if tma_fields:
+            K.append("    if (tid == 0) {")
+            K.append("      fence_proxy_async();")
+            K.append(f"      mbar_arrive_expect_tx(&bars[s], {tma_bytes}u);")
+            for ti, f in enumerate(tma_fields):
+                K.append(f"      tma_load_3d(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}, &p.tmap[{ti}], &bars[s], "
+                         f"(tk0 - {spec.hk(f)}) * {f.nc}, tj0 - {f.halo}, q);")
+            K.append("    }")
+        for f in lsu_fields:
+            w, h = spec.box(f)
+            ct = CTYPE[f.dtype]
+            K.append("    {")
+            K.append(f"      {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
+            K.append(f"      const {ct}* src = (const {ct}*)p.fld[{f.slot}];")
+            K.append(f"      const int x0 = (tk0 - {spec.hk(f)}) * {f.nc};")
+            K.append(f"      const int rowlen = p.n2 * {f.nc};")
+            K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
+            K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
+            K.append(f"        const int jg = tj0 - {f.halo} + yy, xg = x0 + xx;")
+            K.append(f"        {ct} v; v.bits = 0;" if ESIZE[f.dtype] == 2 else f"        {ct} v = ({ct})0;")
+            K.append("        if (q >= 0 && q < p.nl && jg >= 0 && jg < p.n1 && xg >= 0 && xg < rowlen)")
+            K.append("          v = src[((size_t)q * p.n1 + jg) * (size_t)rowlen + xg];")
+            K.append("        dst[e] = v;")
+            K.append("      }")
+            K.append("    }")
+        K.append("  };")
+        K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
+        if lsu_fields:
+            K.append("  __syncthreads();")
+    K.append("  bool ok = true;")
+    if tma_fields:
+        K.append("  for (int q = p_first; q < ib + RAD && q < ie + RAD; ++q) {")
+        K.append("    const int rel = q - p_first;")
+        K.append("    ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+        K.append("  }")
+    K.append("  for (int i = ib; i < ie; ++i) {")
+    K.append("    const int gi = i + p.i_base;")
+    if tma_fields:
+        K.append("    { const int rel = i + RAD - p_first;")
+        K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS); }")
+    for f in spec.fields:
+        if f.staged:
+            ct = CTYPE[f.dtype]
+            K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD + 1; ++d) "
+                     f"x.pl{f.slot}[d] = (const {ct}*)(smem + {rings[f.slot]} + "
+                     f"((i + d - RAD - p_first) % NSLOT) * {plane_bytes(spec, f)});")
+    K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
+    if split:
+        K.append("    if (i_in) {")
+    K.append("    #pragma unroll")
+    K.append("    for (int m = 0; m < VPT; ++m) {")
+    K.append("      const int v = tid + m * NT;")
+    K.append("      const int tj = v / TK, tk = v - (v / TK) * TK;")
+    K.append("      const int j = tj0 + tj, k = tk0 + tk;")
+    K.append("      if (j >= p.n1 || k >= p.n2) continue;")
+    K.append("      const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
+    if split:
+        K.append("      if (!inter) continue;")
+    K.append("      const size_t vox = ((size_t)i * p.n1 + j) * p.n2 + k;")
+    for f in spec.fields:
+        if f.staged:
+            K.append(f"      x.o{f.slot} = (tj + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc};")
+        else:
+            ct = CTYPE[f.dtype]
+            K.append(f"      x.gp{f.slot} = (const {ct}*)p.fld[{f.slot}] + vox * {f.nc};")
+    K.append(f"      float rv[{nroot}];")
+    if split or R == 0:
+        K.append("      eval_fast(x, rv);")
+    else:
+        K.append("      if (inter) eval_fast(x, rv); else eval_slow(p, gi, j, k, rv);")
+    K += ["      " + k for k in _epilogue(spec, e, scan_ok=True)]
+    K.append("    }")
+    if split:
+        K.append("    }")
+    K.append("    ok = __syncthreads_and(ok);")
+    K.append("    if (!ok) break;")
+    if staged:
+        K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
+    K.append("  }")
+    K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return; }")
+    K += ["  " + k for k in _red_flush(spec, "cta")]
+    K.append("}")
+
+    if split:
+        # shell: voxels within RAD of a face, one per thread, evaluated from global memory
+        K.append(f'extern "C" __global__ void __launch_bounds__({SHELL_THREADS}) '
+                 f"sten_shell(const __grid_constant__ Params p) {{")
+        K.append(f"  __shared__ double red_scratch[96];")
+        K.append("  const int tid = threadIdx.x;")
+        K += ["  " + k for k in _red_decls(spec)]
+        K.append("  const long long n0 = p.n0g, n1 = p.n1, n2 = p.n2;")
+        K.append("  const long long g_lo = (long long)p.out_lo + p.i_base, g_hi = g_lo + p.n_out;")
+        K.append("  const long long a1 = max(n1 - 2 * RAD, 0ll), a2 = max(n2 - 2 * RAD, 0ll);")
+        K.append("  const long long c_low = max(0ll, min(g_hi, (long long)RAD) - g_lo);")
+        K.append("  const long long hs = max(g_lo, max(n0 - RAD, (long long)RAD));")
+        K.append("  const long long c_high = max(0ll, g_hi - hs);")
+        K.append("  const long long ii0 = max(g_lo, (long long)RAD), n_int = max(0ll, min(g_hi, n0 - RAD) - ii0);")
+        K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
+        K.append("  const long long t = (long long)blockIdx.x * blockDim.x + tid;")
+        K.append("  if (t < cA + cB + cC) {")
+        K.append("    long long i, j, k;")
+        K.append("    if (t < cA) {            // planes within RAD of a dim-0 face")
+        K.append("      const long long q = t / (n1 * n2), r = t - q * n1 * n2;")
+        K.append("      i = q < c_low ? g_lo + q : hs + (q - c_low);")
+        K.append("      j = r / n2; k = r - j * n2;")
+        K.append("    } else if (t < cA + cB) { // interior planes, rows within RAD of a dim-1 face")
+        K.append("      const long long u = t - cA, w1 = n1 - a1;")
+        K.append("      const long long q = u / (w1 * n2), r = u - q * w1 * n2;")
+        K.append("      const long long jr = r / n2, lo = min((long long)RAD, n1);")
+        K.append("      i = ii0 + q; j = jr < lo ? jr : n1 - (w1 - jr); k = r - jr * n2;")
+        K.append("    } else {                  // interior rows, columns within RAD of a dim-2 face")
+        K.append("      const long long u = t - cA - cB, w2 = n2 - a2;")
+        K.append("      const long long q = u / (a1 * w2), r = u - q * a1 * w2;")
+        K.append("      const long long jr = r / w2, kr = r - jr * w2, lo = min((long long)RAD, n2);")
+        K.append("      i = ii0 + q; j = RAD + jr; k = kr < lo ? kr : n2 - (w2 - kr);")
+        K.append("    }")
+        K.append("    const int gi = (int)i;")
+        K.append("    const size_t vox = ((size_t)(sten_plane(p, gi)) * p.n1 + j) * p.n2 + k;")
+        K.append(f"    float rv[{nroot}];")
+        K.append("    eval_slow(p, gi, (int)j, (int)k, rv);")
+        K += ["    " + k for k in _epilogue(spec, e, scan_ok=False)]
+        K.append("  }")
+        K += ["  " + k for k in _red_flush(spec, "p.cta_off + blockIdx.x")]
+        K.append("}")
+    return "\n".join(L) + "\n" + "\n".join(K) + "\n"

@@ -1,0 +1,269 @@
+// sten_device.cuh — device-side building blocks for the per-graph stencil kernels.
+//
+// The code generator (stenpy_b200/codegen.py) prepends this header to every kernel it
+// emits; kernels are compiled at run time with NVRTC for sm_100a. The header is
+// self-contained (no CUDA headers), so NVRTC needs no include path.
+//
+// Contents
+//   * storage-dtype loads/stores (fp32, bf16, fp16, fp64) — compute is always fp32
+//   * mbarrier + TMA (cp.async.bulk.tensor, no multicast) plane loads with bounded waits
+//   * boundary index helpers for periodic / replicate / zero / reflect padding
+//   * fp64 block reductions: sum, Chan-merged (n, mean, M2), min/max
+//   * closed-form symmetric 3x3 eigenvalues (trigonometric method of O. K. Smith,
+//     "Eigenvalues of a symmetric 3x3 matrix", CACM 4(4):168, 1961) in fp32 with an
+//     fp64 re-evaluation when the spread of the spectrum is small against its centre.
+#pragma once
+
+typedef unsigned long long u64;
+typedef long long i64;
+typedef unsigned int u32;
+typedef unsigned short u16;
+
+#define STEN_DEV __device__ __forceinline__
+
+// ------------------------------------------------------------------ dtype I/O
+struct bf16_t { u16 bits; };
+struct f16_t { u16 bits; };
+
+STEN_DEV float ld_as_f32(const float* p) { return *p; }
+STEN_DEV float ld_as_f32(const double* p) { return (float)(*p); }
+STEN_DEV float ld_as_f32(const bf16_t* p) { return __int_as_float(((u32)p->bits) << 16); }
+STEN_DEV float ld_as_f32(const f16_t* p) {
+  float f; asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(p->bits)); return f;
+}
+STEN_DEV float ldg_as_f32(const float* p) { return __ldg(p); }
+STEN_DEV float ldg_as_f32(const double* p) { return (float)__ldg(p); }
+STEN_DEV float ldg_as_f32(const bf16_t* p) {
+  return __int_as_float(((u32)__ldg((const u16*)p)) << 16);
+}
+STEN_DEV float ldg_as_f32(const f16_t* p) {
+  u16 b = __ldg((const u16*)p); float f; asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(b)); return f;
+}
+STEN_DEV void st_from_f32(float* p, float v) { *p = v; }
+STEN_DEV void st_from_f32(double* p, float v) { *p = (double)v; }
+STEN_DEV void st_from_f32(bf16_t* p, float v) {
+  u16 b; asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(b) : "f"(v)); p->bits = b;
+}
+STEN_DEV void st_from_f32(f16_t* p, float v) {
+  u16 b; asm("cvt.rn.f16.f32 %0, %1;" : "=h"(b) : "f"(v)); p->bits = b;
+}
+STEN_DEV void st_from_f64(double* p, double v) { *p = v; }
+STEN_DEV void st_from_f64(float* p, double v) { *p = (float)v; }
+STEN_DEV void st_from_f64(bf16_t* p, double v) { st_from_f32(p, (float)v); }
+STEN_DEV void st_from_f64(f16_t* p, double v) { st_from_f32(p, (float)v); }
+
+// ------------------------------------------------------------------ math helpers
+STEN_DEV float sten_clamp(float a, float lo, float hi) {
+  // torch.clamp: min(max(a, lo), hi), NaN propagates
+  return (a != a) ? a : fminf(fmaxf(a, lo), hi);
+}
+STEN_DEV float sten_div(float a, float b, float eps) {
+  // divisor with |b| < eps replaced by +-eps
+  float bs = (fabsf(b) < eps) ? (b < 0.0f ? -eps : eps) : b;
+  return a / bs;
+}
+STEN_DEV float sten_log(float a, float eps) { return logf((a != a) ? a : fmaxf(a, eps)); }
+STEN_DEV float sten_sqrt(float a, float eps) { return sqrtf((a != a) ? a : fmaxf(a, eps)); }
+
+// ------------------------------------------------------------------ boundary indices
+STEN_DEV int wrap_idx(int x, int n) { x %= n; return x < 0 ? x + n : x; }
+STEN_DEV int clamp_idx(int x, int n) { return x < 0 ? 0 : (x >= n ? n - 1 : x); }
+// mirror without repeating the edge, radius 1: -1 -> 1, n -> n-2
+STEN_DEV int reflect_idx(int x, int n) {
+  if (x < 0) x = -x;
+  if (x > n - 1) x = 2 * (n - 1) - x;
+  return x < 0 ? 0 : (x > n - 1 ? n - 1 : x);
+}
+
+// ------------------------------------------------------------------ mbarrier + TMA
+struct __align__(64) TmaDesc { u64 opaque[16]; };
+
+STEN_DEV u32 smem_u32(const void* p) {
+  return (u32)__cvta_generic_to_shared(p);
+}
+STEN_DEV void mbar_init(u64* bar, u32 count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+STEN_DEV void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+STEN_DEV void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+STEN_DEV void mbar_arrive_expect_tx(u64* bar, u32 bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+STEN_DEV bool mbar_try_wait(u64* bar, u32 parity) {
+  u32 ok;
+  asm volatile("{\n .reg .pred p;\n"
+               " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+STEN_DEV u64 global_ns() {
+  u64 t; asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t)); return t;
+}
+// Bounded wait: gives up after `limit_ns` of wall time and returns false.
+STEN_DEV bool mbar_wait_bounded(u64* bar, u32 parity, u64 limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  u64 t0 = global_ns();
+  while (!mbar_try_wait(bar, parity)) {
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+  return true;
+}
+// 3-D tiled TMA load of one box into shared memory; completion counted on `bar`.
+// Coordinates: x innermost (elements), y, z. x * elem_size must be a multiple of 16.
+STEN_DEV void tma_load_3d(void* smem_dst, const TmaDesc* map, u64* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];"
+      :: "r"(smem_u32(smem_dst)), "l"((u64)map), "r"(smem_u32(bar)),
+         "r"(x), "r"(y), "r"(z) : "memory");
+}
+STEN_DEV void tma_prefetch_desc(const TmaDesc* map) {
+  asm volatile("prefetch.tensormap [%0];" :: "l"((u64)map) : "memory");
+}
+
+// ------------------------------------------------------------------ fp64 reductions
+STEN_DEV double warp_sum(double v) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+STEN_DEV double warp_min(double v) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+STEN_DEV double warp_max(double v) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+// Chan et al. pairwise merge of (n, mean, M2) moments.
+STEN_DEV void chan_merge(double& n, double& mean, double& m2, double nb, double meanb, double m2b) {
+  double nt = n + nb;
+  if (nt == 0.0) return;
+  double d = meanb - mean;
+  double w = nb / nt;
+  mean += d * w;
+  m2 += m2b + d * d * n * w;
+  n = nt;
+}
+STEN_DEV void warp_chan(double& n, double& mean, double& m2) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double nb = __shfl_xor_sync(0xffffffffu, n, o);
+    double mb = __shfl_xor_sync(0xffffffffu, mean, o);
+    double qb = __shfl_xor_sync(0xffffffffu, m2, o);
+    // fixed operand order per lane pair keeps the result identical on both lanes
+    if ((threadIdx.x & o) == 0) { chan_merge(n, mean, m2, nb, mb, qb); }
+    else { double n2 = nb, m2_ = mb, q2 = qb; chan_merge(n2, m2_, q2, n, mean, m2); n = n2; mean = m2_; m2 = q2; }
+  }
+}
+
+// Block-level reductions through a small shared scratch (one value per warp).
+// All threads of the block must call these; `scratch` holds >= 3*32 doubles.
+STEN_DEV double block_sum(double v, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    r = lane < nw ? scratch[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;  // valid in thread 0
+}
+STEN_DEV double block_min(double v, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_min(v);
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double r = __longlong_as_double(0x7ff0000000000000ll);
+  if (warp == 0) { r = lane < nw ? scratch[lane] : r; r = warp_min(r); }
+  return r;
+}
+STEN_DEV double block_max(double v, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) scratch[warp] = v;
+  __syncthreads();
+  double r = __longlong_as_double(0xfff0000000000000ll);
+  if (warp == 0) { r = lane < nw ? scratch[lane] : r; r = warp_max(r); }
+  return r;
+}
+STEN_DEV void block_chan(double& n, double& mean, double& m2, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  warp_chan(n, mean, m2);
+  __syncthreads();
+  if (lane == 0) { scratch[warp] = n; scratch[32 + warp] = mean; scratch[64 + warp] = m2; }
+  __syncthreads();
+  if (warp == 0) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    if (lane < nw) { a = scratch[lane]; b = scratch[32 + lane]; c = scratch[64 + lane]; }
+    warp_chan(a, b, c);
+    n = a; mean = b; m2 = c;
+  }
+}
+
+// ------------------------------------------------------------------ 3x3 symmetric eigenvalues
+STEN_DEV float m_sqrt(float x) { return sqrtf(x); }
+STEN_DEV double m_sqrt(double x) { return sqrt(x); }
+STEN_DEV float m_acos(float x) { return acosf(x); }
+STEN_DEV double m_acos(double x) { return acos(x); }
+STEN_DEV float m_cos(float x) { return cosf(x); }
+STEN_DEV double m_cos(double x) { return cos(x); }
+// Ascending eigenvalues of the symmetric matrix whose lower triangle is
+// (a00; a10 a11; a20 a21 a22), trigonometric closed form.
+template <typename T>
+STEN_DEV void eig3_trig(T a00, T a10, T a11, T a20, T a21, T a22, T* w) {
+  const T p1 = a10 * a10 + a20 * a20 + a21 * a21;
+  const T q = (a00 + a11 + a22) / T(3);
+  const T b00 = a00 - q, b11 = a11 - q, b22 = a22 - q;
+  const T p2 = b00 * b00 + b11 * b11 + b22 * b22 + T(2) * p1;
+  if (p2 <= T(0)) { w[0] = q; w[1] = q; w[2] = q; return; }
+  const T p = m_sqrt(p2 / T(6));
+  const T ip = T(1) / p;
+  const T c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip;
+  const T c10 = a10 * ip, c20 = a20 * ip, c21 = a21 * ip;
+  // det(B)/2
+  T r = (c00 * (c11 * c22 - c21 * c21) - c10 * (c10 * c22 - c21 * c20) + c20 * (c10 * c21 - c11 * c20)) / T(2);
+  r = r < T(-1) ? T(-1) : (r > T(1) ? T(1) : r);
+  const T phi = m_acos(r) / T(3);
+  const T two_pi_3 = T(2.0943951023931954923);
+  const T e_hi = q + T(2) * p * m_cos(phi);
+  const T e_lo = q + T(2) * p * m_cos(phi + two_pi_3);
+  const T e_mid = T(3) * q - e_hi - e_lo;
+  w[0] = e_lo; w[1] = e_mid; w[2] = e_hi;
+}
+// fp32 evaluation; when the spectrum spread p is below 1e-3 of the matrix scale the
+// fp32 shift A - qI loses digits, so the eigenvalues are re-evaluated in fp64.
+STEN_DEV void eig3_sym(const float* m, float* w) {
+  const float a00 = m[0], a10 = m[3], a11 = m[4], a20 = m[6], a21 = m[7], a22 = m[8];
+  const float scale = fmaxf(fmaxf(fabsf(a00), fabsf(a11)), fmaxf(fabsf(a22),
+                      fmaxf(fmaxf(fabsf(a10), fabsf(a20)), fabsf(a21))));
+  const float q = (a00 + a11 + a22) * (1.0f / 3.0f);
+  const float p2 = (a00 - q) * (a00 - q) + (a11 - q) * (a11 - q) + (a22 - q) * (a22 - q)
+                 + 2.0f * (a10 * a10 + a20 * a20 + a21 * a21);
+  if (p2 > 1e-6f * scale * scale) {
+    eig3_trig<float>(a00, a10, a11, a20, a21, a22, w);
+  } else {
+    double wd[3];
+    eig3_trig<double>((double)a00, (double)a10, (double)a11, (double)a20, (double)a21, (double)a22, wd);
+    w[0] = (float)wd[0]; w[1] = (float)wd[1]; w[2] = (float)wd[2];
+  }
+}
+
+// ------------------------------------------------------------------ status word
+// Device-side error codes written to Params::err (host raises on non-zero).
+#define STEN_ERR_TMA_TIMEOUT 1
+#define STEN_ERR_BAD_ALIGN 2
+#define STEN_WAIT_LIMIT_NS 2000000000ull

@@ -1,0 +1,117 @@
+"""CPU-only checks: the C ABI library loads and exports every declared symbol,
+the front end keeps the reference's graph semantics, the planner/code generator
+produces kernels NVRTC accepts for sm_100a, and the boundary-shell index decode
+covers exactly the voxels within R of a face. No GPU calls."""
+import ctypes
+import itertools
+import os
+import re
+
+import pytest
+import torch
+
+import stenpy_b200 as S
+from stenpy_b200 import _native as N
+from stenpy_b200 import fused_compiler as FC
+from stenpy_b200.codegen import shell_count
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(REPO, "include", "stenpy_b200.h")).read()
+    return sorted(set(re.findall(r"\b(stenpy_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(N.LIB_PATH)
+    declared = _declared_symbols()
+    assert declared, "no declarations found"
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(N.ABI_SYMBOLS) <= set(declared)
+    assert lib.stenpy_abi_version() == 1
+
+
+def test_abi_rejects_bad_arguments_without_gpu():
+    L = N.lib()
+    buf = ctypes.create_string_buffer(128)
+    # misaligned base / bad strides are refused before any driver call
+    assert L.stenpy_encode_tmap_3d(buf, 4, ctypes.c_void_p(8), 64, 8, 8, 256, 2048, 72, 10, 1) == -1
+    assert b"aligned" in L.stenpy_last_error()
+    assert L.stenpy_encode_tmap_3d(buf, 4, ctypes.c_void_p(256), 64, 8, 8, 100, 2048, 72, 10, 1) == -1
+    assert L.stenpy_encode_tmap_3d(buf, 4, ctypes.c_void_p(256), 64, 8, 8, 256, 2048, 300, 10, 1) == -1
+    assert L.stenpy_finalize(None, 1, 1, None, 1, None, None) == -1
+
+
+def test_front_end_graph_semantics():
+    f = torch.zeros(4, 4, 4, dtype=torch.float64)
+    g, sink, warns, ids, _ = S.compile_expression("divergence(gradient(f)) + norm_l2(curl(u))",
+                                                  field_map={"f": f, "u": torch.zeros(4, 4, 4, 3)})
+    ops = [g._nodes[n].op_name for n in g._order]
+    assert ops.count("laplacian") == 1 and ops.count("gradient") == 1  # orphan kept, as in the reference
+    assert any("Simplified" in w for w in warns)
+    orphan = [n for n in g._order if g._nodes[n].op_name == "gradient"][0]
+    assert orphan in g._orphans and orphan in g.sinks()
+    from stenpy_b200.runtime import default_wanted
+    assert default_wanted(g) == [sink]
+    # CSE: repeated subexpressions map to one node
+    g2, s2, *_ = S.compile_expression("tanh(f)*exp(f) + tanh(f)", field_map={"f": f})
+    assert sum(1 for n in g2._order if g2._nodes[n].op_name == "tanh") == 1
+    # hessian spelled both ways, l2norm alias, abs, kwargs
+    for e in ("hessian(f)", "_hessian(f)"):
+        g3, s3, *_ = S.compile_expression(e, field_map={"f": f})
+        assert g3._nodes[s3].op_name == "hessian"
+    g4, s4, *_ = S.compile_expression("l2norm(abs(f))", field_map={"f": f})
+    assert g4._nodes[s4].op_name == "norm_l2"
+    g5, s5, *_ = S.compile_expression("gradient(f, dx=0.25, boundary=periodic)", field_map={"f": f})
+    assert g5._nodes[s5].params == {"dx": 0.25, "boundary": "periodic"}
+    with pytest.raises(ValueError):
+        S.compile_expression("nosuchop(f)", field_map={"f": f})
+
+
+def test_plan_structure_config1():
+    f = torch.zeros(64, 64, 64)
+    u = torch.zeros(64, 64, 64, 3)
+    g, sink, *_ = S.compile_expression("divergence(gradient(f)) + norm_l2(curl(u))", boundary="periodic",
+                                       field_map={"f": f, "u": u})
+    wanted = [sink] + [g.add(r, (sink,), {}) for r in ("sum", "mean", "variance")]
+    plan = FC.Planner(g, wanted).plan()
+    # pass 0: ||curl u||^2 partials; pass 1: lap f + c, with sum/mean/var partials
+    assert len(plan.passes) == 2
+    assert [r.kind for r in plan.passes[0].spec.roots] == ["red"]
+    assert sorted(r.kind for r in plan.passes[1].spec.roots) == ["out", "red", "red", "red"]
+    assert plan.passes[0].spec.fields[0].nc == 3 and plan.passes[0].spec.radius == 1
+
+
+@pytest.mark.parametrize("expr,boundary", [
+    ("f**2 + tanh(f)*exp(f) + laplacian(g)", "periodic"),
+    ("eigenvalues(hessian(f)) + 0*mean_curvature(f)", "neumann"),
+    ("curl(u) * 2", "dirichlet"),
+    ("cumulative_integral(exp(f)) + integrate(g) + entropy(f) + variance(g)", "periodic"),
+])
+def test_generated_kernels_compile_for_sm100a(expr, boundary):
+    fm = {"f": torch.zeros(20, 24, 32), "g": torch.zeros(20, 24, 32, dtype=torch.bfloat16),
+          "u": torch.zeros(20, 24, 32, 3)}
+    g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map=fm)
+    plan = FC.Planner(g, [sink]).plan()
+    for pp in plan.passes:
+        key, cubin = N.compile_cached(FC.emit_pass(pp.spec), FC.NVRTC_OPTS)
+        assert len(cubin) > 1000
+
+
+def test_shell_decode_matches_boundary_shell():
+    """Every global plane range of small grids: count formula == true shell size
+    (the kernel's decode is exercised on the GPU; its count is what the host sizes)."""
+    for shape in [(5, 7, 33), (3, 3, 3), (1, 4, 5), (9, 10, 11), (6, 2, 7)]:
+        for R in (1, 2, 3):
+            n0, n1, n2 = shape
+            for g_lo, g_hi in [(0, n0), (1, n0), (0, max(1, n0 - 1))]:
+                truth = sum(1 for i in range(g_lo, g_hi) for j in range(n1) for k in range(n2)
+                            if not (R <= i < n0 - R and R <= j < n1 - R and R <= k < n2 - R))
+                assert shell_count(shape, R, g_lo, g_hi) == truth
+
+
+def test_cpu_device_is_rejected():
+    with pytest.raises(NotImplementedError):
+        S.Runtime(device="cpu")

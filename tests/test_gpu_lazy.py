@@ -1,0 +1,69 @@
+"""Lazy (out-of-core) mode: chunked runs from pinned host memory must reproduce the
+whole-field run voxel for voxel (same arithmetic at every voxel: seam test), and
+match the CPU FP64 oracle."""
+import pytest
+import torch
+
+from golden_cases import rel_err
+from oracle import stenpy_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+@pytest.mark.parametrize("boundary", ["periodic", "neumann"])
+@pytest.mark.parametrize("chunk", [5, 7, 16])
+def test_chunked_equals_whole_field(boundary, chunk):
+    import stenpy_b200 as S
+    from stenpy_b200.lazy import LazyPipeline
+    from stenpy_b200.synth import sinusoid_field
+    dev = _dev()
+    shape = (37, 24, 64)
+    f = sinusoid_field(shape, seed=5)
+    exprs = {"eig": "eigenvalues(hessian(f))", "mc": "mean_curvature(f)", "lap": "laplacian(f)*2 + exp(f)"}
+    g, sinks, *_ = S.compile_expressions(exprs, boundary=boundary, field_map={"f": f.to(dev)})
+    mean_id = g.add("mean", (sinks["mc"],), {})
+    wanted = list(sinks.values()) + [mean_id]
+    whole = S.Runtime(device=dev).run(g, wanted=wanted)
+    gh, sinks_h, *_ = S.compile_expressions(exprs, boundary=boundary, field_map={"f": f.pin_memory()})
+    mean_h = gh.add("mean", (sinks_h["mc"],), {})
+    lp = LazyPipeline(gh, list(sinks_h.values()) + [mean_h], dev, chunk=chunk)
+    res = lp.run()
+    assert len(lp.passes[0]["chunks"]) == -(-shape[0] // max(chunk, 2 * lp.passes[0]["H"] + 1))
+    for k in exprs:
+        a = whole[sinks[k]].cpu()
+        b = res[sinks_h[k]]
+        assert torch.equal(a, b), (k, (a - b).abs().max().item())
+    assert abs(float(whole[mean_id]) - float(res[mean_h])) <= 1e-12 * max(1.0, abs(float(whole[mean_id])))
+
+
+def test_lazy_config2_shape_against_oracle():
+    """Config-2 graph (eigenvalues of the hessian and mean curvature, BF16 outputs,
+    FP32 compute, FP64 reductions) on a reduced grid with a budget forcing chunks."""
+    import stenpy_b200 as S
+    from stenpy_b200.lazy import LazyPipeline
+    from stenpy_b200.synth import sinusoid_field
+    dev = _dev()
+    shape = (96, 64, 64)
+    f = sinusoid_field(shape, seed=0)
+    exprs = {"eig": "eigenvalues(hessian(f))", "mc": "mean_curvature(f)"}
+    g, sinks, *_ = S.compile_expressions(exprs, boundary="periodic", field_map={"f": f.pin_memory()})
+    mn = g.add("mean", (sinks["mc"],), {})
+    budget = 12 * 64 * 64 * 4 * 6
+    lp = LazyPipeline(g, list(sinks.values()) + [mn], dev, budget_bytes=budget + (256 << 20),
+                      out_dtype=torch.bfloat16)
+    res = lp.run()
+    assert len(lp.passes[0]["chunks"]) > 1
+    g2, sinks2, *_ = S.compile_expressions(exprs, boundary="periodic", field_map={"f": f.double()})
+    mn2 = g2.add("mean", (sinks2["mc"],), {})
+    ref = O.evaluate(g2, list(sinks2.values()) + [mn2])
+    # BF16 storage of the outputs: unit roundoff 2^-9
+    assert rel_err(res[sinks["eig"]], ref[sinks2["eig"]]) <= 4e-3
+    assert rel_err(res[sinks["mc"]], ref[sinks2["mc"]]) <= 2e-2
+    # the FP64 mean is formed from the FP32 values before BF16 rounding
+    assert abs(float(res[mn]) - float(ref[mn2])) <= 1e-4 * max(1.0, abs(float(ref[mn2])))

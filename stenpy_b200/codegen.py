@@ -626,7 +626,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
     the register slot ``m``."""
     K: List[str] = []
     ri = si = 0
-    for r, off in zip(spec.roots, e.offsets):
+    for r, off in zip(spec.roots, e.offsets):  # noqa: C901
         nc = e.g.nodes[r.node].nc
         if r.kind == "out":
             ct = CTYPE[r.out_dtype]
@@ -647,26 +647,34 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
             K.append("}")
             si += 1
         elif r.kind == "red":
+            ri_here = ri
+            ri += 1
+            if r.red == "sum" and _sum_from_var(spec, r) is not None:
+                continue  # derived from the variance accumulator of the same value
+            if r.red == "sumsq" and nc > 1:
+                terms = " + ".join(f"rv[{off + c}] * rv[{off + c}]" for c in range(nc))
+                K.append(f"rv{ri_here}_a += (double)({terms});")
+                continue
             for c in range(nc):
                 val = f"(double)rv[{off + c}]"
                 if r.red == "sum":
-                    K.append(f"rv{ri}_a += {val};")
+                    K.append(f"rv{ri_here}_a += {val};")
                 elif r.red == "sumsq":
-                    K.append(f"{{ const double t_ = {val}; rv{ri}_a += t_ * t_; }}")
+                    K.append(f"{{ const double t_ = {val}; rv{ri_here}_a = fma(t_, t_, rv{ri_here}_a); }}")
                 elif r.red == "var":
-                    K.append(f"{{ const double t_ = {val}; if (!rv{ri}_h) {{ rv{ri}_piv = t_; rv{ri}_h = true; }}"
-                             f" const double d_ = t_ - rv{ri}_piv; rv{ri}_s1 += d_; rv{ri}_s2 += d_ * d_; rv{ri}_n += 1.0; }}")
+                    K.append(f"{{ const double t_ = {val}; rv{ri_here}_piv = rv{ri_here}_h ? rv{ri_here}_piv : t_; rv{ri_here}_h = true;"
+                             f" const double d_ = t_ - rv{ri_here}_piv; rv{ri_here}_s1 += d_; rv{ri_here}_s2 = fma(d_, d_, rv{ri_here}_s2);"
+                             f" rv{ri_here}_n += 1.0; }}")
                 elif r.red == "entropy":
-                    K.append(f"{{ const double a_ = fabs({val}); rv{ri}_a += a_; if (a_ > 0.0) rv{ri}_b += a_ * log(a_); }}")
+                    K.append(f"{{ const double a_ = fabs({val}); rv{ri_here}_a += a_; if (a_ > 0.0) rv{ri_here}_b += a_ * log(a_); }}")
                 elif r.red == "minmax":
-                    K.append(f"{{ const double t_ = {val}; rv{ri}_a = fmin(rv{ri}_a, t_); rv{ri}_b = fmax(rv{ri}_b, t_); }}")
+                    K.append(f"{{ const double t_ = {val}; rv{ri_here}_a = fmin(rv{ri_here}_a, t_); rv{ri_here}_b = fmax(rv{ri_here}_b, t_); }}")
                 elif r.red == "integrate":
                     sm = 1 if r.method == "simpson" else 0
-                    K.append(f"rv{ri}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
+                    K.append(f"rv{ri_here}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
                              f" * sten_simpson_w(j, p.n1, {r.dx[1]!r}, {sm}) * sten_simpson_w(k, p.n2, {r.dx[2]!r}, {sm});")
                 else:
                     raise NotImplementedError(r.red)
-            ri += 1
         else:
             raise NotImplementedError(r.kind)
     return K
@@ -687,16 +695,34 @@ def _red_decls(spec: PassSpec) -> List[str]:
     return K
 
 
+def _sum_from_var(spec: PassSpec, r: RootSpec) -> Optional[int]:
+    """Index (among reduction roots) of a variance root over the same value as the
+    sum root ``r``: the sum then comes from its (n, mean) instead of a second
+    accumulator."""
+    reds = [x for x in spec.roots if x.kind == "red"]
+    for i, x in enumerate(reds):
+        if x.red == "var" and x.node == r.node:
+            return i
+    return None
+
+
 def _red_flush(spec: PassSpec, cta: str) -> List[str]:
     """Block-reduce each accumulator and write this CTA's partial row."""
     K: List[str] = []
-    for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
+    reds = [r for r in spec.roots if r.kind == "red"]
+    for ri, r in enumerate(reds):
         base = f"p.part[(size_t)({cta}) * NSLOTS_RED + {r.slot}"
         if r.red == "var":
             K.append(f"{{ double n_ = rv{ri}_n, mu_ = 0.0, q_ = 0.0;")
             K.append(f"  if (n_ > 0.0) {{ mu_ = rv{ri}_piv + rv{ri}_s1 / n_; q_ = rv{ri}_s2 - rv{ri}_s1 * rv{ri}_s1 / n_; if (q_ < 0.0) q_ = 0.0; }}")
             K.append("  block_chan(n_, mu_, q_, red_scratch);")
-            K.append(f"  if (tid == 0) {{ {base}] = n_; {base} + 1] = mu_; {base} + 2] = q_; }} }}")
+            K.append(f"  if (tid == 0) {{ {base}] = n_; {base} + 1] = mu_; {base} + 2] = q_;")
+            for r2 in reds:
+                if r2.red == "sum" and r2.node == r.node:
+                    K.append(f"    p.part[(size_t)({cta}) * NSLOTS_RED + {r2.slot}] = n_ * mu_;")
+            K.append("  } }")
+        elif r.red == "sum" and _sum_from_var(spec, r) is not None:
+            continue
         elif r.red == "entropy":
             K.append(f"{{ const double a_ = block_sum(rv{ri}_a, red_scratch); const double b_ = block_sum(rv{ri}_b, red_scratch);")
             K.append(f"  if (tid == 0) {{ {base}] = a_; {base} + 1] = b_; }} }}")
@@ -849,6 +875,28 @@ def emit_pass(spec: PassSpec) -> str:
         K.append("    const int rel = q - p_first;")
         K.append("    ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
         K.append("  }")
+    # each thread owns column tk of the tile and VPT consecutive rows; everything that
+    # does not depend on the plane is computed once, before the march
+    K.append("  const int tk = tid % TK, tjb = (tid / TK) * VPT;")
+    K.append("  const int k = tk0 + tk;")
+    if split:
+        K.append("  const bool k_ok = k >= RAD && k < p.n2 - RAD;")
+    else:
+        K.append("  const bool k_ok = k < p.n2;")
+    K.append("  bool m_ok[VPT];")
+    K.append("  #pragma unroll")
+    K.append("  for (int m = 0; m < VPT; ++m) {")
+    K.append("    const int j = tj0 + tjb + m;")
+    if split:
+        K.append("    m_ok[m] = k_ok && j >= RAD && j < p.n1 - RAD;")
+    else:
+        K.append("    m_ok[m] = k_ok && j < p.n1;")
+    K.append("  }")
+    for f in spec.fields:
+        if f.staged:
+            K.append(f"  const int ob{f.slot} = (tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc};")
+    K.append("  const size_t col = (size_t)(tj0 + tjb) * p.n2 + k;")
+    K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
     K.append("  for (int i = ib; i < ie; ++i) {")
     K.append("    const int gi = i + p.i_base;")
     if tma_fields:
@@ -861,21 +909,17 @@ def emit_pass(spec: PassSpec) -> str:
                      f"x.pl{f.slot}[d] = (const {ct}*)(smem + {rings[f.slot]} + "
                      f"((i + d - RAD - p_first) % NSLOT) * {plane_bytes(spec, f)});")
     K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
+    K.append("    const size_t pbase = (size_t)i * plane_n + col;")
     if split:
         K.append("    if (i_in) {")
     K.append("    #pragma unroll")
     K.append("    for (int m = 0; m < VPT; ++m) {")
-    K.append("      const int v = tid + m * NT;")
-    K.append("      const int tj = v / TK, tk = v - (v / TK) * TK;")
-    K.append("      const int j = tj0 + tj, k = tk0 + tk;")
-    K.append("      if (j >= p.n1 || k >= p.n2) continue;")
-    K.append("      const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-    if split:
-        K.append("      if (!inter) continue;")
-    K.append("      const size_t vox = ((size_t)i * p.n1 + j) * p.n2 + k;")
+    K.append("      if (!m_ok[m]) continue;")
+    K.append("      const int j = tj0 + tjb + m;")
+    K.append("      const size_t vox = pbase + (size_t)m * p.n2;")
     for f in spec.fields:
         if f.staged:
-            K.append(f"      x.o{f.slot} = (tj + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc};")
+            K.append(f"      x.o{f.slot} = ob{f.slot} + m * {spec.box(f)[0]};")
         else:
             ct = CTYPE[f.dtype]
             K.append(f"      x.gp{f.slot} = (const {ct}*)p.fld[{f.slot}] + vox * {f.nc};")
@@ -883,6 +927,7 @@ def emit_pass(spec: PassSpec) -> str:
     if split or R == 0:
         K.append("      eval_fast(x, rv);")
     else:
+        K.append("      const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
         K.append("      if (inter) eval_fast(x, rv); else eval_slow(p, gi, j, k, rv);")
     K += ["      " + k for k in _epilogue(spec, e, scan_ok=True)]
     K.append("    }")

@@ -66,7 +66,8 @@ STEN_DEV float sten_log(float a, float eps) { return logf((a != a) ? a : fmaxf(a
 STEN_DEV float sten_sqrt(float a, float eps) { return sqrtf((a != a) ? a : fmaxf(a, eps)); }
 
 // ------------------------------------------------------------------ boundary indices
-STEN_DEV int wrap_idx(int x, int n) { x %= n; return x < 0 ? x + n : x; }
+// x is within one period of [0, n): every stencil tap moves one cell per level
+STEN_DEV int wrap_idx(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 STEN_DEV int clamp_idx(int x, int n) { return x < 0 ? 0 : (x >= n ? n - 1 : x); }
 // mirror without repeating the edge, radius 1: -1 -> 1, n -> n-2
 STEN_DEV int reflect_idx(int x, int n) {

@@ -120,6 +120,35 @@ int stenpy_finalize(const double* partials, int ncta, int nslots,
                     const StenReduceDesc* descs, int nred, double* scalars,
                     void* stream);
 
+/* ---- allocation-free variant ------------------------------------------------
+ * No counterpart in the reference. For hosts that cannot allocate device memory
+ * (an application that owns a fixed arena and forbids further cudaMalloc, code
+ * running while another component owns the allocator, latency-critical loops
+ * where cudaMalloc/cudaFree would synchronise the device): runs a fused
+ * reduction pass — its kernel launches, then the finalize — with the FP64
+ * partials in a static device array of STENPY_NOALLOC_MAX_PARTIALS doubles
+ * (4 MiB, held by every device that loads the library until exit) instead of a
+ * caller-allocated buffer. Each launch's packed parameters are copied and the
+ * partials pointer at byte offset `part_offset` is replaced by the static
+ * array's device address (looked up per device on the first call, which should
+ * therefore precede any stream capture). Requests with ncta_total * nslots above
+ * the maximum fail with STENPY_E_INVALID. Calls share the array: every partial
+ * row is rewritten each call, but calls that overlap on one GPU race. */
+#define STENPY_NOALLOC_MAX_PARTIALS (1u << 19)
+
+typedef struct StenLaunchDesc {
+  StenModule* module;
+  uint32_t grid[3];
+  uint32_t block[3];
+  uint32_t dyn_smem;
+  uint32_t part_offset;   /* byte offset of the partials pointer in params */
+  const void* params;     /* packed kernel parameters (<= 8 KiB) */
+  size_t params_bytes;
+} StenLaunchDesc;
+
+int stenpy_pass_noalloc(const StenLaunchDesc* launches, int n_launch, int ncta_total, int nslots,
+                        const StenReduceDesc* descs, int nred, double* scalars, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,7 @@ CACHE_DIR = os.environ.get("STENPY_JIT_CACHE", os.path.join(_PKG, "_jit_cache"))
 ABI_SYMBOLS = (
     "stenpy_abi_version", "stenpy_last_error", "stenpy_nvrtc_version", "stenpy_device_props",
     "stenpy_nvrtc_compile", "stenpy_free", "stenpy_module_load", "stenpy_module_free",
-    "stenpy_launch", "stenpy_encode_tmap_3d", "stenpy_finalize",
+    "stenpy_launch", "stenpy_encode_tmap_3d", "stenpy_finalize", "stenpy_pass_noalloc",
 )
 
 
@@ -37,6 +37,14 @@ class ReduceDesc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("slot", ctypes.c_int32), ("out_index", ctypes.c_int32),
                 ("unbiased", ctypes.c_int32), ("count", ctypes.c_double), ("eps", ctypes.c_double)]
 
+
+class LaunchDesc(ctypes.Structure):
+    _fields_ = [("module", ctypes.c_void_p), ("grid", ctypes.c_uint32 * 3), ("block", ctypes.c_uint32 * 3),
+                ("dyn_smem", ctypes.c_uint32), ("part_offset", ctypes.c_uint32), ("params", ctypes.c_void_p),
+                ("params_bytes", ctypes.c_size_t)]
+
+
+NOALLOC_MAX_PARTIALS = 1 << 19
 
 RED_SUM, RED_MEAN, RED_NORM_L2, RED_VARIANCE, RED_ENTROPY, RED_INTEGRATE, RED_MIN_MAX = range(7)
 MAX_REDUCTIONS = 32
@@ -76,6 +84,8 @@ def lib() -> ctypes.CDLL:
                                             c.c_uint32]
         L.stenpy_finalize.argtypes = [c.c_void_p, c.c_int, c.c_int, c.POINTER(ReduceDesc), c.c_int,
                                       c.c_void_p, c.c_void_p]
+        L.stenpy_pass_noalloc.argtypes = [c.POINTER(LaunchDesc), c.c_int, c.c_int, c.c_int,
+                                          c.POINTER(ReduceDesc), c.c_int, c.c_void_p, c.c_void_p]
         for name in ABI_SYMBOLS:
             if not hasattr(L, name):
                 raise NativeUnavailable(f"{LIB_PATH} lacks {name}; rebuild it")
@@ -166,3 +176,25 @@ def finalize(partials_ptr: int, ncta: int, nslots: int, descs: Sequence[ReduceDe
     arr = (ReduceDesc * len(descs))(*descs)
     _check(lib().stenpy_finalize(ctypes.c_void_p(partials_ptr), ncta, nslots, arr, len(descs),
                                  ctypes.c_void_p(scalars_ptr), ctypes.c_void_p(stream)), "finalize")
+
+
+def pass_noalloc(launches, ncta_total: int, nslots: int, descs: Sequence[ReduceDesc], scalars_ptr: int,
+                 stream: int) -> None:
+    """Run one fused reduction pass with the library's static partials array (no
+    device allocation). ``launches``: (module, grid, block, dyn_smem, params bytes,
+    byte offset of the partials pointer in params)."""
+    keep = []
+    arr = (LaunchDesc * len(launches))()
+    for d, (module, grid, block, smem, params, part_offset) in zip(arr, launches):
+        buf = ctypes.create_string_buffer(params, len(params))
+        keep.append(buf)
+        d.module = module
+        d.grid[:] = list(grid)
+        d.block[:] = list(block)
+        d.dyn_smem = smem
+        d.part_offset = part_offset
+        d.params = ctypes.cast(buf, ctypes.c_void_p)
+        d.params_bytes = len(params)
+    rd = (ReduceDesc * len(descs))(*descs)
+    _check(lib().stenpy_pass_noalloc(arr, len(launches), ncta_total, nslots, rd, len(descs),
+                                     ctypes.c_void_p(scalars_ptr), ctypes.c_void_p(stream)), "pass_noalloc")

@@ -125,6 +125,9 @@ struct StenModule {
 
 extern "C" {
 
+// Lets other translation units of the library report errors through stenpy_last_error.
+void sten_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 int stenpy_abi_version(void) { return STENPY_ABI_VERSION; }
 
 const char* stenpy_last_error(void) { return g_last_error.c_str(); }

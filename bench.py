@@ -35,6 +35,7 @@ import subprocess
 import sys
 import threading
 import time
+from typing import Tuple
 
 import torch
 
@@ -147,8 +148,11 @@ def make_fields(size, device):
     return f, u
 
 
-def build(form, f, u, device):
+def build(form, f, u, device, tune=True):
+    """Plan the step for one storage form; with ``tune`` every pass gets the schedule
+    the autotuner measured fastest (exhaustive over its candidates, cached)."""
     import stenpy_b200 as S
+    from stenpy_b200 import autotune as AT
     from stenpy_b200 import fused_compiler as FC
     dt = FORM_DT[form]
     g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
@@ -156,8 +160,9 @@ def build(form, f, u, device):
     wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
     plan = FC.get_plan(g, wanted, out_dtype=dt)
     values, back = FC.bind(plan, g, wanted)
+    tuned = AT.tune_plan(plan, values, device, tag=f"bench-{form}") if tune else []
     prog = FC.build_program(plan, values, device)
-    return g, wanted, plan, prog
+    return g, wanted, plan, prog, tuned
 
 
 def time_graph(replay, stream, steps, warmup, world, dev):
@@ -315,6 +320,95 @@ def errors_vs_fp64(f, u, device, forms):
     return out, f"{P}x{f.shape[1]}x{f.shape[2]} sample"
 
 
+def _pinned_copy_gbps(nbytes: int, dev) -> Tuple[float, float]:
+    """Plain pinned host<->device copy bandwidth (GB/s), the link roofline."""
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = []
+    for src, dst in ((h, d), (d, h)):
+        for _ in range(2):
+            dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(3):
+            dst.copy_(src, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        out.append(3 * nbytes / (a.elapsed_time(b) * 1e-3) / 1e9)
+    return out[0], out[1]
+
+
+def run_lazy(args):
+    """Config 2: out-of-core eigenvalues(hessian(f)) and mean_curvature(f) of a
+    1536x1536x1024 FP32 field held in pinned host memory, 8 GB device budget,
+    BF16 outputs, FP32 compute, FP64 reductions; reports the H2D / compute / D2H
+    overlap and the host-link roofline."""
+    import stenpy_b200 as S
+    from stenpy_b200.lazy import LazyPipeline
+    from stenpy_b200.synth import sinusoid_field
+    dev = torch.device("cuda", 0)
+    shape = tuple(int(x) for x in args.lazy_shape.split("x"))
+    n0 = shape[0]
+    f = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    step = 64
+    for s0 in range(0, n0, step):  # generate on the GPU in slabs (same generator, seed 0)
+        f[s0:s0 + step].copy_(sinusoid_field((min(step, n0 - s0),) + shape[1:], seed=1000 + s0, device=dev).cpu())
+    exprs = {"eig": "eigenvalues(hessian(f))", "mc": "mean_curvature(f)"}
+    g, sinks, *_ = S.compile_expressions(exprs, boundary="periodic", field_map={"f": f})
+    reds = [g.add("mean", (sinks["mc"],), {}), g.add("norm_l2", (sinks["eig"],), {})]
+    budget = int(args.budget_gb * (1 << 30))
+    lp = LazyPipeline(g, list(sinks.values()) + reds, dev, budget_bytes=budget, out_dtype=torch.bfloat16)
+    lp.prepare()
+    stamps = lp.enqueue(timing=True)
+    torch.cuda.synchronize()
+    rep = LazyPipeline.overlap_report(stamps)
+    # timed: eager enqueue (events) and CUDA-graph replay of the whole schedule
+    ts = []
+    for _ in range(max(1, args.steps)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        lp.enqueue()
+        b.record()
+        torch.cuda.synchronize()
+        ts.append(a.elapsed_time(b))
+    graph = lp.capture()
+    gs = []
+    for _ in range(max(1, args.steps)):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        graph.replay()
+        b.record()
+        torch.cuda.synchronize()
+        gs.append(a.elapsed_time(b))
+    FC_check(dev)
+    vox = shape[0] * shape[1] * shape[2]
+    P = lp.passes[0]
+    h2d = sum((c.hi - c.lo) for c in P["chunks"]) * shape[1] * shape[2] * 4
+    d2h = vox * 4 * 2
+    up, down = _pinned_copy_gbps(1 << 30, dev)
+    ms = statistics.median(gs)
+    link_ms = max(h2d / (up * 1e9), d2h / (down * 1e9)) * 1e3
+    line = {"metric": "lazy out-of-core throughput (Gvoxel/s)", "value": vox / (ms * 1e-3) / 1e9,
+            "unit": "Gvoxel/s", "n_gpus": 1, "steps": args.steps, "ms_per_step": ms, "higher_is_better": True,
+            "dtype": "f32", "storage": "bf16 outputs", "data": "synthetic",
+            "config": {"workload": f"eigenvalues(hessian(f)) + mean_curvature(f), periodic, {args.lazy_shape} fp32 "
+                                   f"in pinned host memory, {args.budget_gb} GB device budget",
+                       "chunks": len(P["chunks"]), "chunk_planes": P["C"], "halo": P["H"]},
+            "eager_enqueue_ms": statistics.median(ts), "graph_replay_ms": ms,
+            "overlap": rep, "link": {"h2d_GBps": up, "d2h_GBps": down, "h2d_bytes": h2d, "d2h_bytes": d2h,
+                                      "roofline_ms": link_ms, "frac": link_ms / ms},
+            "reductions": {"mean_mc": float(lp.table[lp.plan.red_index[reds[0]]]),
+                           "norm_l2_eig": float(lp.table[lp.plan.red_index[reds[1]]])},
+            "gpu_launches": lp.n_kernels}
+    print(json.dumps(line), flush=True)
+
+
+def FC_check(dev):
+    from stenpy_b200 import fused_compiler as FC
+    FC.ErrorFlag.check(dev)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -325,10 +419,18 @@ def main():
     ap.add_argument("--forms", default="fp32,fp16,bf16")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error sample")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default schedules instead of autotuned ones")
+    ap.add_argument("--workload", default="fields", choices=["fields", "lazy"],
+                    help="fields: the 512^3 fused step (default); lazy: the out-of-core run")
+    ap.add_argument("--lazy-shape", default="1536x1536x1024")
+    ap.add_argument("--budget-gb", type=float, default=8.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "lazy":
+        run_lazy(args)
         return
     world, rank, local = _dist()
     dev = torch.device("cuda", local)
@@ -342,7 +444,7 @@ def main():
     results = {}
     clocks = None
     for form in forms:
-        g, wanted, plan, prog = build(form, f, u, dev)
+        g, wanted, plan, prog, tuned = build(form, f, u, dev, tune=not args.no_tune)
         with torch.cuda.stream(stream):
             FC.enqueue(prog, stream)
         torch.cuda.synchronize()
@@ -376,6 +478,7 @@ def main():
             "step_GBps": ALG_BYTES[form] * n_vox / (ms * 1e-3) / 1e9,
             "step_frac_of_peak": ALG_BYTES[form] * n_vox / (ms * 1e-3) / 1e9 / peak,
             "launches_per_step": n_launch,
+            "schedules": [dict(vars(p.spec.cfg)) for p in plan.passes],
             "kernels_ms": [round(t, 4) for _, t in kt],
             "dominant": {"ms": dom_ms, "alg_bytes": alg, "GBps": alg / (dom_ms * 1e-3) / 1e9},
         }

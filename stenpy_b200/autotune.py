@@ -28,7 +28,8 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, plane_bytes, shell_count, smem_layout
+from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, plane_bytes, shell_count,
+                      shell_regions, smem_layout)
 
 LOG_PATH = os.environ.get("STENPY_TUNE_LOG", os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                                           "_tune", "timings.jsonl"))
@@ -115,15 +116,8 @@ def _launches(pp: FC.PassPlan, spec: PassSpec, values: Dict[str, Any], shape, de
     tiles_j = -(-n1 // cfg.tj)
     grid = (tiles_j * tiles_k, -(-n0 // cfg.seg_len), 1)
     ncta = grid[0] * grid[1]
-    fptrs, tmaps = [], []
-    for f, nid in zip(spec.fields, pp.field_nodes):
-        t = values[nid]
-        fptrs.append(t.data_ptr())
-        if f.tma:
-            w, h = spec.box(f)
-            es = ESIZE[f.dtype]
-            tmaps.append(N.encode_tmap_3d(es, t.data_ptr(), n2 * f.nc, n1, n0, n2 * f.nc * es,
-                                          n1 * n2 * f.nc * es, (w, h, 1)))
+    fptrs = [values[nid].data_ptr() for nid in pp.field_nodes]
+    tmaps = FC.encode_tmaps(spec, fptrs, n0, n1, n2)
     outs = []
     for (nid, kind, nc), r in zip(pp.out_nodes, [r for r in spec.roots if r.kind in ("out", "scan")]):
         outs.append(torch.empty((n0, n1, n2) + FC.comp_shape(nc), dtype=FC.DT_TORCH[r.out_dtype], device=device))
@@ -132,7 +126,7 @@ def _launches(pp: FC.PassPlan, spec: PassSpec, values: Dict[str, Any], shape, de
                 seg_len=cfg.seg_len, tiles_k=tiles_k, cta_off=0)
     ls = [(grid, (cfg.threads, 1, 1), FC.pack_params(spec, vals, tmaps))]
     if FC.has_shell(spec):
-        sh = -(-shell_count(shape, spec.radius) // SHELL_THREADS)
+        sh = -(-shell_count(shape, spec.radius, regions=shell_regions(spec)) // SHELL_THREADS)
         ls.append(((sh, 1, 1), (SHELL_THREADS, 1, 1), FC.pack_params(spec, dict(vals, cta_off=ncta), tmaps)))
     return ls, outs, ncta
 
@@ -147,7 +141,7 @@ def time_schedule(pp: FC.PassPlan, cfg: PassConfig, values: Dict[str, Any], shap
     key, cubin = N.compile_cached(src, FC.NVRTC_OPTS)
     mod = N.load_module(key, cubin, "sten_kernel", smem, dev_idx)
     shell_mod = N.load_module(key + ":shell", cubin, "sten_shell", 0, dev_idx) if FC.has_shell(spec) else None
-    n_shell = -(-shell_count(shape, spec.radius) // SHELL_THREADS) if FC.has_shell(spec) else 0
+    n_shell = -(-shell_count(shape, spec.radius, regions=shell_regions(spec)) // SHELL_THREADS)
     tiles = (-(-shape[1] // cfg.tj)) * (-(-shape[2] // cfg.tk)) * (-(-shape[0] // cfg.seg_len))
     part = torch.empty(max((tiles + n_shell) * spec.nslots, 1), dtype=torch.float64, device=device)
     table = torch.zeros(max(spec.n_scalars, 1) + 8, dtype=torch.float64, device=device)

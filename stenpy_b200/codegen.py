@@ -88,6 +88,8 @@ class FieldSpec:
     staged: bool = False  # held in a shared-memory plane ring
     tma: bool = False     # ring filled by TMA (else by cooperative loads)
     halo: int = 0         # j/k halo of the staged tile (0 for fields read only at the voxel)
+    wrap_k: bool = False  # periodic ghosts along dim 2 come from extra TMA strips
+    wrap_j: bool = False  # periodic ghosts along dim 1 come from extra TMA strips
 
 
 @dataclass
@@ -124,6 +126,9 @@ class PassSpec:
     radius: int
     cfg: PassConfig = dc_field(default_factory=PassConfig)
     has_scan: bool = False
+    # ghost-cell mode: {(field slot, axis): rule}; None when some stencil is nested
+    ghosts: Optional[Dict[Tuple[int, int], str]] = None
+    i_periodic: bool = False   # every tap along dim 0 wraps: planes are loaded wrapped
 
     def hk(self, f: FieldSpec) -> int:
         """k-halo in elements, rounded so TMA x-coordinates stay 16-byte aligned."""
@@ -135,6 +140,77 @@ class PassSpec:
     def box(self, f: FieldSpec) -> Tuple[int, int]:
         """(row width in elements, rows) of one staged plane tile."""
         return ((self.cfg.tk + 2 * self.hk(f)) * f.nc, self.cfg.tj + 2 * f.halo)
+
+
+_REMAP_RULES = ("periodic", "replicate", "reflect")
+
+
+def analyse_ghosts(spec: "PassSpec") -> None:
+    """Decide whether the z-march can evaluate the dim-1/dim-2 faces itself.
+
+    It can when every stencil is single-level (no d1/lap below another): then each
+    boundary rule is reproduced by a ghost cell next to the face — periodic wrap,
+    replicate, reflect and zero padding by the value they read; torch.gradient's
+    one-sided edges by extrapolation (quadratic for edge order 2: with
+    f[-1] = 3f0 - 3f1 + f2 the central difference equals (-3f0 + 4f1 - f2)/2h;
+    linear for edge order 1). Index-remap rules commute with pointwise ops, so they
+    also apply through pointwise subexpressions; zero padding and extrapolation only
+    when the stencil reads the field directly. Each (field, axis) must get one rule.
+    """
+    g = spec.graph
+    spec.ghosts = None
+    spec.i_periodic = False
+    if spec.radius == 0 or spec.has_scan:
+        return
+
+    def subtree(nid, acc):
+        n = g.nodes[nid]
+        acc.add(nid)
+        for x in n.ins:
+            subtree(x, acc)
+        return acc
+
+    rules: Dict[Tuple[int, int], str] = {}
+    i_periodic = True
+    for n in g.nodes:
+        if n.op not in ("d1", "lap"):
+            continue
+        sub = subtree(n.ins[0], set())
+        if any(g.nodes[x].op in ("d1", "lap") for x in sub):
+            return
+        direct = g.nodes[n.ins[0]].op == "field"
+        if n.op == "lap":
+            rule, axes = n.a("pad"), (0, 1, 2)
+        else:
+            rule, axes = n.a("mode"), (n.a("axis"),)
+            if rule == "zero":
+                continue
+        if rule not in _REMAP_RULES and not direct:
+            return
+        for x in sub:
+            if g.nodes[x].op != "field":
+                continue
+            slot = g.nodes[x].a("field")
+            for ax in axes:
+                if rules.setdefault((slot, ax), rule) != rule:
+                    return
+                if ax == 0 and rule != "periodic":
+                    i_periodic = False
+    spec.ghosts = rules
+    spec.i_periodic = i_periodic
+    for f in spec.fields:
+        f.wrap_k = f.tma and f.halo > 0 and rules.get((f.slot, 2)) == "periodic"
+        f.wrap_j = f.tma and f.halo > 0 and rules.get((f.slot, 1)) == "periodic"
+
+
+def shell_regions(spec: "PassSpec") -> str:
+    """Which boundary regions the shell kernel evaluates: all faces ("ABC"), only the
+    dim-0 faces ("A", ghost mode), or none."""
+    if spec.radius == 0 or spec.has_scan:
+        return ""
+    if spec.ghosts is None:
+        return "ABC"
+    return "" if spec.i_periodic else "A"
 
 
 def _lit(x: float) -> str:
@@ -562,7 +638,7 @@ def param_layout(spec: PassSpec) -> ParamLayout:
         offs[name] = off
         off += size
 
-    ntma = sum(1 for f in spec.fields if f.tma)
+    ntma = len(tmap_specs(spec))
     if ntma:
         put("tmap", 128 * ntma, 64)
     put("fld", 8 * max(len(spec.fields), 1), 8)
@@ -595,9 +671,53 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
     return off, rings, red_off
 
 
-def plane_bytes(spec: PassSpec, f: FieldSpec) -> int:
+def _a128(x: int) -> int:
+    return (x + 127) // 128 * 128
+
+
+def strip_boxes(spec: PassSpec, f: FieldSpec) -> Tuple[Tuple[int, int], Tuple[int, int]]:
+    """TMA boxes (elements wide, rows) of the periodic wrap strips: a dim-2 strip of
+    hk columns for the tile's rows, and a dim-1 strip of ``halo`` rows across the
+    tile's (haloed) width."""
+    hk = spec.hk(f)
+    return (hk * f.nc, spec.cfg.tj), ((spec.cfg.tk + 2 * hk) * f.nc, f.halo)
+
+
+def slot_layout(spec: PassSpec, f: FieldSpec) -> Dict[str, int]:
+    """Byte offsets inside one ring slot: the plane box, then wrap strips
+    (left/right along dim 2, top/bottom along dim 1) when the field has them."""
     w, h = spec.box(f)
-    return ((w * h * ESIZE[f.dtype]) + 127) // 128 * 128
+    es = ESIZE[f.dtype]
+    off = {"box": 0}
+    o = _a128(w * h * es)
+    (kw, kh), (jw, jh) = strip_boxes(spec, f)
+    if f.wrap_k:
+        off["kl"], off["kr"] = o, o + _a128(kw * kh * es)
+        o += 2 * _a128(kw * kh * es)
+    if f.wrap_j:
+        off["jt"], off["jb"] = o, o + _a128(jw * jh * es)
+        o += 2 * _a128(jw * jh * es)
+    off["size"] = o
+    return off
+
+
+def plane_bytes(spec: PassSpec, f: FieldSpec) -> int:
+    return slot_layout(spec, f)["size"]
+
+
+def tmap_specs(spec: PassSpec) -> List[Tuple[int, str, Tuple[int, int]]]:
+    """Ordered TMA descriptors of a pass: (field slot, "box" | "kstrip" | "jstrip", box)."""
+    out = []
+    for f in spec.fields:
+        if not f.tma:
+            continue
+        out.append((f.slot, "box", spec.box(f)))
+        ks, js = strip_boxes(spec, f)
+        if f.wrap_k:
+            out.append((f.slot, "kstrip", ks))
+        if f.wrap_j:
+            out.append((f.slot, "jstrip", js))
+    return out
 
 
 def _simpson_fn() -> str:
@@ -734,7 +854,98 @@ def _red_flush(spec: PassSpec, cta: str) -> List[str]:
     return K
 
 
-def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Optional[int] = None) -> int:
+def _ghost_expr(rule: str, at, n: str, side: str) -> Optional[str]:
+    """Ghost value next to a face for ``rule``; ``at(idx)`` reads the field at an
+    in-domain index along the axis (fp32). None: nothing to write."""
+    if side == "lo":
+        v = {"replicate": f"{at('0')}",
+             "reflect": f"({n} > 1 ? {at('1')} : 0.0f)",
+             "edge2": f"(3.0f * {at('0')} - 3.0f * {at('1')} + {at('2')})",
+             "edge1": f"(2.0f * {at('0')} - {at('1')})"}
+    else:
+        v = {"replicate": f"{at(n + ' - 1')}",
+             "reflect": f"({n} > 1 ? {at(n + ' - 2')} : 0.0f)",
+             "edge2": f"(3.0f * {at(n + ' - 1')} - 3.0f * {at(n + ' - 2')} + {at(n + ' - 3')})",
+             "edge1": f"(2.0f * {at(n + ' - 1')} - {at(n + ' - 2')})"}
+    return v.get(rule)
+
+
+def _ghost_fill(spec: PassSpec, rings: Dict[int, int]) -> List[str]:
+    """``ghost_fill(q)``: write the ghost cells next to the dim-1/dim-2 faces of the
+    tile in the ring slot of plane q (edge tiles only). Sources: the tile itself
+    (replicate / reflect / extrapolation; along dim 1 the tile may be too thin at the
+    last face, then global memory), the TMA wrap strips (periodic), or nothing when
+    the cooperative fill already applied the rule (remap rules without TMA)."""
+    K = ["auto ghost_fill = [&](int q) {",
+         "  const int s = (q - p_first) % NSLOT;",
+         "  const int zq = sten_plane(p, q + p.i_base);",
+         "  if (zq < 0 || zq >= p.nl) return;"]
+    for f in spec.fields:
+        if not f.staged or f.halo == 0:
+            continue
+        rk = spec.ghosts.get((f.slot, 2))
+        rj = spec.ghosts.get((f.slot, 1))
+        lsu_done = ("periodic", "replicate", "reflect", "zero")
+        todo_k = rk is not None and rk != "zero" and (f.tma or rk not in lsu_done)
+        todo_j = rj is not None and rj != "zero" and (f.tma or rj not in lsu_done)
+        if not (todo_k or todo_j):
+            continue
+        ct = CTYPE[f.dtype]
+        w = spec.box(f)[0]
+        hk = spec.hk(f)
+        nc = f.nc
+        lay = slot_layout(spec, f)
+        (kw, _), (jw, _) = strip_boxes(spec, f)
+        K.append("  {")
+        K.append(f"    unsigned char* slot_ = smem + {rings[f.slot]} + s * {plane_bytes(spec, f)};")
+        K.append(f"    {ct}* dst = ({ct}*)slot_;")
+        if todo_k:
+            for side, cond, col in (("lo", "tk0 == 0", f"{hk} - 1"), ("hi", "tk0 + TK >= p.n2", f"p.n2 - tk0 + {hk}")):
+                K.append(f"    if ({cond}) for (int e = tid; e < TJ * {nc}; e += NT) {{")
+                K.append(f"      const int yy = e / {nc}, c = e - yy * {nc};")
+                K.append("      if (tj0 + yy < p.n1) {")
+                if rk == "periodic":
+                    buf = "kl" if side == "lo" else "kr"
+                    scol = f"{hk} - 1" if side == "lo" else "0"
+                    K.append(f"        const {ct}* st = ({ct}*)(slot_ + {lay[buf]});")
+                    K.append(f"        dst[(yy + {f.halo}) * {w} + ({col}) * {nc} + c] = st[yy * {kw} + ({scol}) * {nc} + c];")
+                else:
+                    rowp = f"dst + (yy + {f.halo}) * {w}"
+                    expr = _ghost_expr(rk, lambda ix: f"ld_as_f32({rowp} + (({ix}) - tk0 + {hk}) * {nc} + c)", "p.n2", side)
+                    K.append(f"        st_from_f32(dst + (yy + {f.halo}) * {w} + ({col}) * {nc} + c, {expr});")
+                K.append("      }")
+                K.append("    }")
+        if todo_j:
+            for side, cond, row in (("lo", "tj0 == 0", f"{f.halo} - 1"), ("hi", "tj0 + TJ >= p.n1", f"p.n1 - tj0 + {f.halo}")):
+                K.append(f"    if ({cond}) for (int e = tid; e < TK * {nc}; e += NT) {{")
+                K.append(f"      const int xx = e / {nc}, c = e - xx * {nc};")
+                K.append("      if (tk0 + xx < p.n2) {")
+                if rj == "periodic":
+                    buf = "jt" if side == "lo" else "jb"
+                    srow = f"{f.halo} - 1" if side == "lo" else "0"
+                    K.append(f"        const {ct}* st = ({ct}*)(slot_ + {lay[buf]});")
+                    K.append(f"        dst[({row}) * {w} + (xx + {hk}) * {nc} + c] = st[({srow}) * {jw} + (xx + {hk}) * {nc} + c];")
+                else:
+                    def at_s(ix, f=f, w=w, hk=hk, nc=nc):
+                        return f"ld_as_f32(dst + (({ix}) - tj0 + {f.halo}) * {w} + (xx + {hk}) * {nc} + c)"
+
+                    def at_g(ix, ct=ct, nc=nc, f=f):
+                        return (f"ldg_as_f32((const {ct}*)p.fld[{f.slot}] + (((size_t)zq * p.n1 + ({ix})) * p.n2"
+                                f" + tk0 + xx) * {nc} + c)")
+                    es_ = _ghost_expr(rj, at_s, "p.n1", side)
+                    if side == "hi":
+                        eg_ = _ghost_expr(rj, at_g, "p.n1", side)
+                        es_ = f"((p.n1 - tj0 >= 3 - {f.halo}) ? {es_} : {eg_})"
+                    K.append(f"        st_from_f32(dst + ({row}) * {w} + (xx + {hk}) * {nc} + c, {es_});")
+                K.append("      }")
+                K.append("    }")
+        K.append("  }")
+    K.append("};")
+    return K
+
+
+def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Optional[int] = None,
+                regions: str = "ABC") -> int:
     """Voxels of global planes [g_lo, g_hi) that lie within R of a face (the shell
     kernel's domain); mirrors the decode in ``sten_shell``."""
     n0, n1, n2 = shape
@@ -745,6 +956,10 @@ def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Option
     c_high = max(0, g_hi - hs)
     ii0 = max(g_lo, R)
     n_int = max(0, min(g_hi, n0 - R) - ii0)
+    if regions == "":
+        return 0
+    if regions == "A":
+        return (c_low + c_high) * n1 * n2
     return (c_low + c_high) * n1 * n2 + n_int * (n1 - a1) * n2 + n_int * a1 * (n2 - a2)
 
 
@@ -760,7 +975,9 @@ def emit_pass(spec: PassSpec) -> str:
     e = _Emitter(spec)
     cfg = spec.cfg
     R = spec.radius
-    split = R > 0 and not spec.has_scan
+    regions = shell_regions(spec)
+    ghost = spec.ghosts is not None
+    split = R > 0 and not spec.has_scan          # main kernel never takes the slow path
     nslot = 2 * R + 1 + cfg.prefetch
     assert nslot <= 16, "too many ring slots"
     assert cfg.tk % 32 == 0 and (cfg.tj * cfg.tk) % cfg.threads == 0 and cfg.prefetch >= 1
@@ -769,7 +986,7 @@ def emit_pass(spec: PassSpec) -> str:
     L.append(header)
     L.append(f"#define TJ {cfg.tj}\n#define TK {cfg.tk}\n#define NT {cfg.threads}\n#define RAD {R}"
              f"\n#define NSLOT {nslot}\n#define VPT {vpt}\n#define NSLOTS_RED {max(spec.nslots, 1)}")
-    ntma = sum(1 for f in spec.fields if f.tma)
+    ntma = len(tmap_specs(spec))
     nout = sum(1 for r in spec.roots if r.kind in ("out", "scan"))
     L.append("struct __align__(64) Params {")
     if ntma:
@@ -819,6 +1036,7 @@ def emit_pass(spec: PassSpec) -> str:
     K.append("  const int ib = p.out_lo + (int)blockIdx.y * p.seg_len;")
     K.append("  const int ie = min(ib + p.seg_len, p.out_lo + p.n_out);")
     K.append("  const int cta = p.cta_off + (int)(blockIdx.y * gridDim.x + blockIdx.x);")
+    K.append("  const bool edge_cta = tk0 == 0 || tk0 + TK >= p.n2 || tj0 == 0 || tj0 + TJ >= p.n1;")
     K.append("  FCtx x;")
     K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
              f"x.sc[s] = (s < {spec.n_scalars}) ? (float)p.scal[s] : 0.0f;")
@@ -828,58 +1046,106 @@ def emit_pass(spec: PassSpec) -> str:
         K.append(f"  double sc{si}_acc[VPT * {nc}]; float sc{si}_prev[VPT * {nc}];")
         K.append(f"  #pragma unroll\n  for (int q = 0; q < VPT * {nc}; ++q) {{ sc{si}_acc[q] = 0.0; sc{si}_prev[q] = 0.0f; }}")
     staged = tma_fields or lsu_fields
+    tmaps = tmap_specs(spec)
+    tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
     K.append("  const int p_first = ib - RAD;")
     if tma_fields:
         K.append("  if (tid == 0) {")
         K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
         K.append("    fence_mbar_init();")
-        for ti in range(len(tma_fields)):
+        for ti in range(len(tmaps)):
             K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
         K.append("  }")
         K.append("  __syncthreads();")
     if staged:
         K.append("  auto request = [&](int q) {")
         K.append("    const int s = (q - p_first) % NSLOT;")
+        if ghost and spec.i_periodic:
+            K.append("    const int zq = (q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q;")
+        else:
+            K.append("    const int zq = q;")
         if tma_fields:
             K.append("    if (tid == 0) {")
             K.append("      fence_proxy_async();")
-            K.append(f"      mbar_arrive_expect_tx(&bars[s], {tma_bytes}u);")
-            for ti, f in enumerate(tma_fields):
-                K.append(f"      tma_load_3d(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}, &p.tmap[{ti}], &bars[s], "
-                         f"(tk0 - {spec.hk(f)}) * {f.nc}, tj0 - {f.halo}, q);")
+            K.append(f"      unsigned int bytes_ = {tma_bytes}u;")
+            for f in tma_fields:
+                (kw, kh), (jw, jh) = strip_boxes(spec, f)
+                es = ESIZE[f.dtype]
+                if f.wrap_k:
+                    K.append(f"      if (tk0 == 0) bytes_ += {kw * kh * es}u;")
+                    K.append(f"      if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
+                if f.wrap_j:
+                    K.append(f"      if (tj0 == 0) bytes_ += {jw * jh * es}u;")
+                    K.append(f"      if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
+            K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
+            for f in tma_fields:
+                base = f"smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}"
+                lay = slot_layout(spec, f)
+                hk = spec.hk(f)
+                K.append(f"      tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
+                         f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
+                if f.wrap_k:
+                    ti = tidx[(f.slot, "kstrip")]
+                    K.append(f"      if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
+                             f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
+                    K.append(f"      if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
+                             f"0, tj0, zq);")
+                if f.wrap_j:
+                    ti = tidx[(f.slot, "jstrip")]
+                    K.append(f"      if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
+                             f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
+                    K.append(f"      if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
+                             f"(tk0 - {hk}) * {f.nc}, 0, zq);")
             K.append("    }")
         for f in lsu_fields:
             w, h = spec.box(f)
             ct = CTYPE[f.dtype]
+            rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+            rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
             K.append("    {")
             K.append(f"      {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
             K.append(f"      const {ct}* src = (const {ct}*)p.fld[{f.slot}];")
-            K.append(f"      const int x0 = (tk0 - {spec.hk(f)}) * {f.nc};")
-            K.append(f"      const int rowlen = p.n2 * {f.nc};")
             K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
             K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
-            K.append(f"        const int jg = tj0 - {f.halo} + yy, xg = x0 + xx;")
+            K.append(f"        int jg = tj0 - {f.halo} + yy;")
+            K.append(f"        const int xr = xx - {spec.hk(f)} * {f.nc};")
+            K.append(f"        int kg = tk0 + (xr >= 0 ? xr / {f.nc} : -((-xr + {f.nc} - 1) / {f.nc}));")
+            K.append(f"        const int c = xr - (kg - tk0) * {f.nc};")
+            for ax, var, n, rule in ((1, "jg", "p.n1", rj), (2, "kg", "p.n2", rk)):
+                if rule == "periodic":
+                    K.append(f"        {var} = wrap_idx({var}, {n});")
+                elif rule == "replicate":
+                    K.append(f"        {var} = clamp_idx({var}, {n});")
+                elif rule == "reflect":
+                    K.append(f"        if ({n} > 1) {var} = reflect_idx({var}, {n});")
             K.append(f"        {ct} v; v.bits = 0;" if ESIZE[f.dtype] == 2 else f"        {ct} v = ({ct})0;")
-            K.append("        if (q >= 0 && q < p.nl && jg >= 0 && jg < p.n1 && xg >= 0 && xg < rowlen)")
-            K.append("          v = src[((size_t)q * p.n1 + jg) * (size_t)rowlen + xg];")
+            K.append("        if (zq >= 0 && zq < p.nl && jg >= 0 && jg < p.n1 && kg >= 0 && kg < p.n2)")
+            K.append(f"          v = src[(((size_t)zq * p.n1 + jg) * p.n2 + kg) * {f.nc} + c];")
             K.append("        dst[e] = v;")
             K.append("      }")
             K.append("    }")
         K.append("  };")
+        if ghost:
+            K += ["  " + x for x in _ghost_fill(spec, rings)]
         K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
         if lsu_fields:
             K.append("  __syncthreads();")
     K.append("  bool ok = true;")
+    # planes p_first .. ib+RAD must be resident (and ghosted) before the first plane
     if tma_fields:
-        K.append("  for (int q = p_first; q < ib + RAD && q < ie + RAD; ++q) {")
+        K.append("  for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) {")
         K.append("    const int rel = q - p_first;")
         K.append("    ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
         K.append("  }")
+    if ghost and staged:
+        K.append("  if (edge_cta) { for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) ghost_fill(q); }")
+    if staged:
+        K.append("  __syncthreads();")
     # each thread owns column tk of the tile and VPT consecutive rows; everything that
     # does not depend on the plane is computed once, before the march
     K.append("  const int tk = tid % TK, tjb = (tid / TK) * VPT;")
     K.append("  const int k = tk0 + tk;")
-    if split:
+    if split and not ghost:
         K.append("  const bool k_ok = k >= RAD && k < p.n2 - RAD;")
     else:
         K.append("  const bool k_ok = k < p.n2;")
@@ -887,7 +1153,7 @@ def emit_pass(spec: PassSpec) -> str:
     K.append("  #pragma unroll")
     K.append("  for (int m = 0; m < VPT; ++m) {")
     K.append("    const int j = tj0 + tjb + m;")
-    if split:
+    if split and not ghost:
         K.append("    m_ok[m] = k_ok && j >= RAD && j < p.n1 - RAD;")
     else:
         K.append("    m_ok[m] = k_ok && j < p.n1;")
@@ -899,16 +1165,16 @@ def emit_pass(spec: PassSpec) -> str:
     K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
     K.append("  for (int i = ib; i < ie; ++i) {")
     K.append("    const int gi = i + p.i_base;")
-    if tma_fields:
-        K.append("    { const int rel = i + RAD - p_first;")
-        K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS); }")
     for f in spec.fields:
         if f.staged:
             ct = CTYPE[f.dtype]
             K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD + 1; ++d) "
                      f"x.pl{f.slot}[d] = (const {ct}*)(smem + {rings[f.slot]} + "
                      f"((i + d - RAD - p_first) % NSLOT) * {plane_bytes(spec, f)});")
-    K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
+    if ghost and spec.i_periodic:
+        K.append("    const bool i_in = true;")
+    else:
+        K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
     K.append("    const size_t pbase = (size_t)i * plane_n + col;")
     if split:
         K.append("    if (i_in) {")
@@ -933,6 +1199,15 @@ def emit_pass(spec: PassSpec) -> str:
     K.append("    }")
     if split:
         K.append("    }")
+    # the next plane (i+1+RAD) must be resident and ghosted before the barrier
+    if tma_fields or (ghost and staged):
+        K.append("    if (i + 1 < ie) {")
+        if tma_fields:
+            K.append("      const int rel = i + 1 + RAD - p_first;")
+            K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+        if ghost and staged:
+            K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
+        K.append("    }")
     K.append("    ok = __syncthreads_and(ok);")
     K.append("    if (!ok) break;")
     if staged:
@@ -942,7 +1217,7 @@ def emit_pass(spec: PassSpec) -> str:
     K += ["  " + k for k in _red_flush(spec, "cta")]
     K.append("}")
 
-    if split:
+    if regions:
         # shell: voxels within RAD of a face, one per thread, evaluated from global memory
         K.append(f'extern "C" __global__ void __launch_bounds__({SHELL_THREADS}) '
                  f"sten_shell(const __grid_constant__ Params p) {{")
@@ -956,7 +1231,10 @@ def emit_pass(spec: PassSpec) -> str:
         K.append("  const long long hs = max(g_lo, max(n0 - RAD, (long long)RAD));")
         K.append("  const long long c_high = max(0ll, g_hi - hs);")
         K.append("  const long long ii0 = max(g_lo, (long long)RAD), n_int = max(0ll, min(g_hi, n0 - RAD) - ii0);")
-        K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
+        if regions == "A":
+            K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = 0, cC = 0;")
+        else:
+            K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
         K.append("  const long long t = (long long)blockIdx.x * blockDim.x + tid;")
         K.append("  if (t < cA + cB + cC) {")
         K.append("    long long i, j, k;")

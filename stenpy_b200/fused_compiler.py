@@ -33,8 +33,8 @@ from typing import Any, Dict, List, Optional, Sequence, Set, Tuple
 import torch
 
 from . import _native as N
-from .codegen import (ESIZE, SHELL_THREADS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec, emit_pass,
-                      param_layout, shell_count, smem_layout)
+from .codegen import (ESIZE, SHELL_THREADS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec, analyse_ghosts,
+                      emit_pass, param_layout, shell_count, shell_regions, smem_layout, tmap_specs)
 from .graph import Graph
 from .lowering import LoweringError, OpLowerer, dx3
 from .registry import KNOWN_OPS
@@ -134,7 +134,8 @@ class FusedPlan:
 
 class Planner:
     def __init__(self, graph: Graph, wanted: Sequence[str], out_dtype: torch.dtype = torch.float32,
-                 config: Optional[PassConfig] = None):
+                 config: Optional[PassConfig] = None, ghosts: bool = True):
+        self.ghosts = ghosts
         self.g = graph
         self.nodes = graph._nodes
         self.wanted = list(dict.fromkeys(wanted))
@@ -342,6 +343,8 @@ class Planner:
             es = ESIZE[f.dtype]
             f.tma = (n2 * f.nc * es) % 16 == 0 and (w * es) % 16 == 0 and w <= 256 and h <= 256
             f.staged = f.tma or f.slot in offset_read
+        if self.ghosts:
+            analyse_ghosts(spec)
         return PassPlan(spec, field_nodes, out_nodes, reductions)
 
     def _scalar_source(self, sinks: Dict[str, int]) -> str:
@@ -441,7 +444,22 @@ def compile_pass(pp: PassPlan, device: int) -> None:
 
 
 def has_shell(spec: PassSpec) -> bool:
-    return spec.radius > 0 and not spec.has_scan
+    return shell_regions(spec) != ""
+
+
+def encode_tmaps(spec: PassSpec, ptrs: Sequence[int], nl: int, n1: int, n2: int) -> List[bytes]:
+    """TMA descriptors of a pass, in the order the kernel's Params expects: each
+    TMA field's plane box and, for periodic ghosts, its wrap-strip boxes. ``ptrs``
+    are the field base addresses by slot, ``nl`` the planes of the arrays."""
+    out = []
+    for slot, kind, (bw, bh) in tmap_specs(spec):
+        f = spec.fields[slot]
+        es = ESIZE[f.dtype]
+        if ptrs[slot] % 16:
+            raise FusionError("TMA field base address must be 16-byte aligned")
+        out.append(N.encode_tmap_3d(es, ptrs[slot], n2 * f.nc, n1, nl, n2 * f.nc * es,
+                                    n1 * n2 * f.nc * es, (bw, bh, 1)))
+    return out
 
 
 def pack_params(spec: PassSpec, values: Dict[str, Any], tmaps: List[bytes]) -> bytes:
@@ -546,7 +564,6 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
         grid = (tiles_j * tiles_k, nseg, 1)
         ncta = grid[0] * grid[1]
         fptrs: List[int] = []
-        tmaps: List[bytes] = []
         for f, nid in zip(spec.fields, pp.field_nodes):
             t = produced[nid] if nid in produced else values[nid]
             if not isinstance(t, torch.Tensor) or t.device != device:
@@ -556,13 +573,7 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
             if DT_TORCH[f.dtype] != t.dtype:
                 raise FusionError(f"field {nid}: planned {f.dtype}, got {t.dtype}")
             fptrs.append(t.data_ptr())
-            if f.tma:
-                if t.data_ptr() % 16:
-                    raise FusionError(f"field {nid}: base address must be 16-byte aligned")
-                w, h = spec.box(f)
-                es = ESIZE[f.dtype]
-                tmaps.append(N.encode_tmap_3d(es, t.data_ptr(), n2 * f.nc, n1, n0, n2 * f.nc * es,
-                                              n1 * n2 * f.nc * es, (w, h, 1)))
+        tmaps = encode_tmaps(spec, fptrs, n0, n1, n2)
         outs: List[torch.Tensor] = []
         for (nid, okind, nc), r in zip(pp.out_nodes, [r for r in spec.roots if r.kind in ("out", "scan")]):
             o = outputs.get(nid) if (outputs and okind == "out") else None
@@ -572,7 +583,7 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
             produced[nid] = o
             if nid in plan.wanted:
                 results[nid] = o
-        n_shell = shell_count(plan.shape, spec.radius) if has_shell(spec) else 0
+        n_shell = shell_count(plan.shape, spec.radius, regions=shell_regions(spec))
         shell_ctas = -(-n_shell // SHELL_THREADS)
         total_cta = ncta + shell_ctas
         part = plan.buffers.get(f"part{pi}")

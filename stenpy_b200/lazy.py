@@ -32,7 +32,7 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import SHELL_THREADS, PassConfig, shell_count
+from .codegen import SHELL_THREADS, PassConfig, shell_count, shell_regions
 from .graph import Graph
 
 
@@ -171,21 +171,14 @@ class LazyPipeline:
                 nseg = -(-n_out // cfg.seg_len)
                 grid = (tiles_j * tiles_k, nseg, 1)
                 nl = c.hi - c.lo
-                fptrs, tmaps = [], []
-                for f, bufs in zip(spec.fields, slabs):
-                    t = bufs[b]
-                    fptrs.append(t.data_ptr())
-                    if f.tma:
-                        w, h = spec.box(f)
-                        es = FC.ESIZE[f.dtype]
-                        tmaps.append(N.encode_tmap_3d(es, t.data_ptr(), self.n2 * f.nc, self.n1, nl,
-                                                      self.n2 * f.nc * es, self.n1 * self.n2 * f.nc * es, (w, h, 1)))
+                fptrs = [bufs[b].data_ptr() for bufs in slabs]
+                tmaps = FC.encode_tmaps(spec, fptrs, nl, self.n1, self.n2)
                 vals = dict(fld=fptrs, out=[o[b].data_ptr() for o in outs], scal=self.table.data_ptr(), part=0,
                             hist=0, err=self.err.data_ptr(), n0g=self.n0, n1=self.n1, n2=self.n2, nl=nl,
                             i_base=c.lo, out_lo=c.s - c.lo, n_out=n_out, seg_len=cfg.seg_len,
                             tiles_k=tiles_k, cta_off=cta_off)
                 ncta = grid[0] * grid[1]
-                n_shell = shell_count(plan.shape, spec.radius, c.s, c.e) if split else 0
+                n_shell = shell_count(plan.shape, spec.radius, c.s, c.e, shell_regions(spec)) if split else 0
                 sh = -(-n_shell // SHELL_THREADS)
                 launches.append((c, b, grid, vals, tmaps, cta_off, ncta, sh))
                 cta_off += ncta + sh

@@ -115,3 +115,44 @@ def test_shell_decode_matches_boundary_shell():
 def test_cpu_device_is_rejected():
     with pytest.raises(NotImplementedError):
         S.Runtime(device="cpu")
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16, torch.float16])
+@pytest.mark.parametrize("expr,boundary", [
+    ("divergence(gradient(f)) + l2norm(curl(u))", "periodic"),
+    ("laplacian(f) + gradient(f)*0 + curl(u)", "neumann"),
+    ("laplacian(f)", "periodic"),
+    ("eigenvalues(hessian(f))", "periodic"),
+])
+def test_every_tma_x_coordinate_is_16_byte_aligned(dtype, expr, boundary):
+    """The x coordinate of each tiled TMA load must be a multiple of 16 bytes (an
+    unaligned one faults the GPU). Enumerate the coordinates the generated kernels
+    issue — plane boxes for every tile and the periodic wrap strips — for every
+    candidate schedule, and check them on the host."""
+    from stenpy_b200 import autotune as AT
+    from stenpy_b200.codegen import ESIZE, strip_boxes, tmap_specs
+    import dataclasses
+    shape = (24, 40, 96)
+    fm = {"f": torch.zeros(shape, dtype=dtype), "u": torch.zeros(shape + (3,), dtype=dtype)}
+    try:
+        g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map=fm)
+        plan = FC.Planner(g, [sink]).plan()
+    except FC.FusionError:
+        pytest.skip("graph not fusable")
+    n2 = shape[2]
+    for pp in plan.passes:
+        for cfg in [pp.spec.cfg] + AT.candidates(pp.spec):
+            spec = dataclasses.replace(pp.spec, cfg=cfg)
+            for slot, kind, (bw, bh) in tmap_specs(spec):
+                f = spec.fields[slot]
+                es = ESIZE[f.dtype]
+                hk = spec.hk(f)
+                assert (bw * es) % 16 == 0 and bw <= 256 and bh <= 256
+                assert (n2 * f.nc * es) % 16 == 0
+                xs = []
+                if kind in ("box", "jstrip"):
+                    xs = [(tk0 - hk) * f.nc for tk0 in range(0, n2, cfg.tk)]
+                else:
+                    xs = [(n2 - hk) * f.nc, 0]
+                for x in xs:
+                    assert (x * es) % 16 == 0, (kind, x, es, cfg)

@@ -120,6 +120,29 @@ int stenpy_finalize(const double* partials, int ncta, int nslots,
                     const StenReduceDesc* descs, int nred, double* scalars,
                     void* stream);
 
+/* ---- schedule cost model (MLP) -----------------------------------------------
+ * No counterpart in the reference, whose only schedule model is an analytic
+ * arithmetic-intensity / register estimate (fused_compiler.py:20-43). A 2-hidden-
+ * layer ReLU perceptron (hidden = 64) predicts a pass's log run time under a
+ * schedule; it is trained on the autotuner's timings with these kernels and only
+ * ranks candidate schedules. Parameters: one FP32 device buffer laid out
+ * W1[in][h], b1[h], W2[h][h], b2[h], w3[h], b3. All buffers are caller-owned
+ * device memory; `workspace` holds stenpy_mlp_workspace_floats(n, hidden) floats. */
+int stenpy_mlp_param_count(int in_dim, int hidden);
+int stenpy_mlp_workspace_floats(int n, int hidden);
+/* out[n] = MLP(X[n][in_dim]). */
+int stenpy_mlp_forward(const float* params, int in_dim, int hidden, const float* X, int n,
+                       float* out, float* workspace, void* stream);
+/* Mean squared error against target[n]: *loss (device scalar) and grad (same
+ * layout as params) of the mean loss, by explicit backpropagation. */
+int stenpy_mlp_loss_grad(const float* params, int in_dim, int hidden, const float* X,
+                         const float* target, int n, float* grad, float* loss,
+                         float* workspace, void* stream);
+/* One Adam update (bias-corrected, decoupled weight decay added to the gradient). */
+int stenpy_adam_step(float* params, const float* grad, float* m, float* v, int n_params,
+                     float lr, float beta1, float beta2, float eps, int step,
+                     float weight_decay, void* stream);
+
 /* ---- allocation-free variant ------------------------------------------------
  * No counterpart in the reference. For hosts that cannot allocate device memory
  * (an application that owns a fixed arena and forbids further cudaMalloc, code

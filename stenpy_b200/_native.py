@@ -22,6 +22,8 @@ ABI_SYMBOLS = (
     "stenpy_abi_version", "stenpy_last_error", "stenpy_nvrtc_version", "stenpy_device_props",
     "stenpy_nvrtc_compile", "stenpy_free", "stenpy_module_load", "stenpy_module_free",
     "stenpy_launch", "stenpy_encode_tmap_3d", "stenpy_finalize", "stenpy_pass_noalloc",
+    "stenpy_mlp_param_count", "stenpy_mlp_workspace_floats", "stenpy_mlp_forward", "stenpy_mlp_loss_grad",
+    "stenpy_adam_step",
 )
 
 
@@ -86,6 +88,14 @@ def lib() -> ctypes.CDLL:
                                       c.c_void_p, c.c_void_p]
         L.stenpy_pass_noalloc.argtypes = [c.POINTER(LaunchDesc), c.c_int, c.c_int, c.c_int,
                                           c.POINTER(ReduceDesc), c.c_int, c.c_void_p, c.c_void_p]
+        L.stenpy_mlp_param_count.argtypes = [c.c_int, c.c_int]
+        L.stenpy_mlp_workspace_floats.argtypes = [c.c_int, c.c_int]
+        L.stenpy_mlp_forward.argtypes = [c.c_void_p, c.c_int, c.c_int, c.c_void_p, c.c_int, c.c_void_p,
+                                         c.c_void_p, c.c_void_p]
+        L.stenpy_mlp_loss_grad.argtypes = [c.c_void_p, c.c_int, c.c_int, c.c_void_p, c.c_void_p, c.c_int,
+                                           c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p]
+        L.stenpy_adam_step.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int, c.c_float,
+                                       c.c_float, c.c_float, c.c_float, c.c_int, c.c_float, c.c_void_p]
         for name in ABI_SYMBOLS:
             if not hasattr(L, name):
                 raise NativeUnavailable(f"{LIB_PATH} lacks {name}; rebuild it")
@@ -198,3 +208,30 @@ def pass_noalloc(launches, ncta_total: int, nslots: int, descs: Sequence[ReduceD
     rd = (ReduceDesc * len(descs))(*descs)
     _check(lib().stenpy_pass_noalloc(arr, len(launches), ncta_total, nslots, rd, len(descs),
                                      ctypes.c_void_p(scalars_ptr), ctypes.c_void_p(stream)), "pass_noalloc")
+
+
+def mlp_param_count(in_dim: int, hidden: int) -> int:
+    return int(lib().stenpy_mlp_param_count(in_dim, hidden))
+
+
+def mlp_workspace_floats(n: int, hidden: int) -> int:
+    return int(lib().stenpy_mlp_workspace_floats(n, hidden))
+
+
+def mlp_forward(params: int, in_dim: int, hidden: int, X: int, n: int, out: int, ws: int, stream: int) -> None:
+    v = ctypes.c_void_p
+    _check(lib().stenpy_mlp_forward(v(params), in_dim, hidden, v(X), n, v(out), v(ws), v(stream)), "mlp_forward")
+
+
+def mlp_loss_grad(params: int, in_dim: int, hidden: int, X: int, target: int, n: int, grad: int, loss: int,
+                  ws: int, stream: int) -> None:
+    v = ctypes.c_void_p
+    _check(lib().stenpy_mlp_loss_grad(v(params), in_dim, hidden, v(X), v(target), n, v(grad), v(loss), v(ws),
+                                      v(stream)), "mlp_loss_grad")
+
+
+def adam_step(params: int, grad: int, m: int, vv: int, n: int, lr: float, b1: float, b2: float, eps: float,
+              step: int, wd: float, stream: int) -> None:
+    v = ctypes.c_void_p
+    _check(lib().stenpy_adam_step(v(params), v(grad), v(m), v(vv), n, lr, b1, b2, eps, step, wd, v(stream)),
+           "adam_step")

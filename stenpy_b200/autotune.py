@@ -29,7 +29,7 @@ import torch
 from . import _native as N
 from . import fused_compiler as FC
 from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, plane_bytes, shell_count,
-                      shell_regions, smem_layout)
+                      shell_regions, smem_layout, with_config)
 
 LOG_PATH = os.environ.get("STENPY_TUNE_LOG", os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                                           "_tune", "timings.jsonl"))
@@ -37,16 +37,16 @@ _BEST_PATH = os.path.join(os.path.dirname(LOG_PATH), "best.json")
 _lock = threading.Lock()
 SMEM_LIMIT = 227 * 1024
 
-# (TK, threads, rows per thread) x segment lengths: 12 x 2 = 24 schedules
-_SHAPES = [(32, 64, 4), (32, 128, 2), (32, 128, 4), (64, 64, 2), (64, 128, 2), (64, 128, 4),
-           (64, 256, 2), (64, 256, 4), (128, 128, 2), (128, 128, 4), (128, 256, 2), (128, 256, 4)]
+# (TK, threads, rows per thread) x segment lengths x boundary strategy = 6 x 2 x 2 = 24
+_SHAPES = [(32, 128, 4), (32, 128, 8), (64, 128, 2), (64, 128, 4), (64, 256, 4), (64, 256, 8)]
 _SEGS = (32, 128)
+_GHOST = (True, False)
 
 
 def _valid(spec: PassSpec, cfg: PassConfig) -> bool:
     if cfg.threads % cfg.tk or cfg.tk % 32 or (cfg.tj * cfg.tk) % cfg.threads:
         return False
-    trial = dataclasses.replace(spec, cfg=cfg)
+    trial = with_config(spec, cfg)
     for f in spec.fields:
         w, h = trial.box(f)
         if f.tma and (w > 256 or h > 256 or (w * ESIZE[f.dtype]) % 16):
@@ -57,17 +57,19 @@ def _valid(spec: PassSpec, cfg: PassConfig) -> bool:
 
 def candidates(spec: PassSpec) -> List[PassConfig]:
     out = []
+    uses_ghost = with_config(spec, dataclasses.replace(spec.cfg, ghost=True)).ghosts is not None
     for tk, nt, vpt in _SHAPES:
         for seg in _SEGS:
-            cfg = PassConfig(tj=(nt // tk) * vpt, tk=tk, threads=nt, prefetch=2, seg_len=seg)
-            if spec.has_scan:
-                cfg.seg_len = spec.cfg.seg_len
-            if _valid(spec, cfg):
-                out.append(cfg)
+            for gh in (_GHOST if uses_ghost else (True,)):
+                cfg = PassConfig(tj=(nt // tk) * vpt, tk=tk, threads=nt, prefetch=2, seg_len=seg, ghost=gh)
+                if spec.has_scan:
+                    cfg.seg_len = spec.cfg.seg_len
+                if _valid(spec, cfg):
+                    out.append(cfg)
     # keep distinct schedules only (scan passes collapse the segment axis)
     seen, uniq = set(), []
     for c in out:
-        k = (c.tj, c.tk, c.threads, c.seg_len, c.prefetch)
+        k = (c.tj, c.tk, c.threads, c.seg_len, c.prefetch, c.ghost)
         if k not in seen:
             seen.add(k)
             uniq.append(c)
@@ -97,14 +99,15 @@ def features(spec: PassSpec, shape: Sequence[int]) -> Dict[str, float]:
 
 
 def schedule_features(spec: PassSpec, cfg: PassConfig) -> Dict[str, float]:
-    trial = dataclasses.replace(spec, cfg=cfg)
+    trial = with_config(spec, cfg)
     smem, _, _ = smem_layout(trial)
     return {"tj": cfg.tj, "tk": cfg.tk, "threads": cfg.threads, "vpt": cfg.tj * cfg.tk // cfg.threads,
-            "seg_len": cfg.seg_len, "prefetch": cfg.prefetch, "smem": smem}
+            "seg_len": cfg.seg_len, "prefetch": cfg.prefetch, "smem": smem, "ghost": float(cfg.ghost),
+            "shell": float(shell_regions(trial) != "")}
 
 
 def pass_key(spec: PassSpec, shape: Sequence[int]) -> str:
-    src = emit_pass(dataclasses.replace(spec, cfg=PassConfig()))
+    src = emit_pass(with_config(spec, PassConfig()))
     return hashlib.sha256((src + repr(tuple(shape))).encode()).hexdigest()[:24]
 
 
@@ -135,7 +138,7 @@ def time_schedule(pp: FC.PassPlan, cfg: PassConfig, values: Dict[str, Any], shap
                   reps: int = 5) -> float:
     """Median milliseconds of one pass (main + shell kernel) under ``cfg``."""
     dev_idx = device.index if device.index is not None else torch.cuda.current_device()
-    spec = dataclasses.replace(pp.spec, cfg=cfg)
+    spec = with_config(pp.spec, cfg)
     src = emit_pass(spec)
     smem, _, _ = smem_layout(spec)
     key, cubin = N.compile_cached(src, FC.NVRTC_OPTS)
@@ -230,7 +233,7 @@ def tune_plan(plan: FC.FusedPlan, values: Dict[str, Any], device, tag: str = "",
             cands = chooser(pp, candidates(pp.spec), plan.shape)
         cfg, res = tune_pass(pp, values, plan.shape, device, cands, tag=tag, reuse=reuse)
         if vars(cfg) != vars(pp.spec.cfg):
-            pp.spec = dataclasses.replace(pp.spec, cfg=cfg)
+            pp.spec = with_config(pp.spec, cfg)
             pp.module = None
             pp.shell_module = None
         out.append((cfg, min([m for _, m in res]) if res else float("nan")))

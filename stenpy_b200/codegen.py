@@ -114,6 +114,7 @@ class PassConfig:
     prefetch: int = 2
     seg_len: int = 64
     min_blocks: int = 1
+    ghost: bool = True   # evaluate dim-1/dim-2 faces in the z-march (else in the shell kernel)
 
 
 @dataclass
@@ -160,7 +161,9 @@ def analyse_ghosts(spec: "PassSpec") -> None:
     g = spec.graph
     spec.ghosts = None
     spec.i_periodic = False
-    if spec.radius == 0 or spec.has_scan:
+    for f in spec.fields:
+        f.wrap_k = f.wrap_j = False
+    if spec.radius == 0 or spec.has_scan or not spec.cfg.ghost:
         return
 
     def subtree(nid, acc):
@@ -201,6 +204,14 @@ def analyse_ghosts(spec: "PassSpec") -> None:
     for f in spec.fields:
         f.wrap_k = f.tma and f.halo > 0 and rules.get((f.slot, 2)) == "periodic"
         f.wrap_j = f.tma and f.halo > 0 and rules.get((f.slot, 1)) == "periodic"
+
+
+def with_config(spec: "PassSpec", cfg: "PassConfig") -> "PassSpec":
+    """Copy of ``spec`` under another schedule (fields copied, ghost plan redone)."""
+    import dataclasses
+    out = dataclasses.replace(spec, cfg=cfg, fields=[dataclasses.replace(f) for f in spec.fields])
+    analyse_ghosts(out)
+    return out
 
 
 def shell_regions(spec: "PassSpec") -> str:
@@ -339,7 +350,7 @@ class _Emitter:
         if f.staged:
             w = self.s.box(f)[0]
             for c in range(n.nc):
-                body.append(f"{arr}[{c}] = ld_as_f32(x.pl{f.slot}[({di}) + {self.R}] + x.o{f.slot}"
+                body.append(f"{arr}[{c}] = ld_as_f32((const {CTYPE[f.dtype]}*)sten_smem + x.so{f.slot}[({di}) + {self.R}] + x.o{f.slot}"
                             f" + ({dj}) * {w} + ({dk}) * {f.nc} + {c});")
         elif di != "0" or dj != "0" or dk != "0":
             raise AssertionError("unstaged field read at an offset")
@@ -750,7 +761,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
         nc = e.g.nodes[r.node].nc
         if r.kind == "out":
             ct = CTYPE[r.out_dtype]
-            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - (size_t)p.out_lo * p.n1 * p.n2) * {nc};")
+            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
             for c in range(nc):
                 K.append(f"  st_from_f32(o_ + {c}, rv[{off + c}]);")
             K.append("}")
@@ -758,7 +769,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
             assert scan_ok
             ct = CTYPE[r.out_dtype]
             half = repr(0.5 * float(r.dx[0]))
-            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - (size_t)p.out_lo * p.n1 * p.n2) * {nc};")
+            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
             for c in range(nc):
                 q = f"m * {nc} + {c}"
                 K.append(f"  if (gi > 0) sc{si}_acc[{q}] += ((double)sc{si}_prev[{q}] + (double)rv[{off + c}]) * {half};")
@@ -784,7 +795,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
                 elif r.red == "var":
                     K.append(f"{{ const double t_ = {val}; rv{ri_here}_piv = rv{ri_here}_h ? rv{ri_here}_piv : t_; rv{ri_here}_h = true;"
                              f" const double d_ = t_ - rv{ri_here}_piv; rv{ri_here}_s1 += d_; rv{ri_here}_s2 = fma(d_, d_, rv{ri_here}_s2);"
-                             f" rv{ri_here}_n += 1.0; }}")
+                             f" ++rv{ri_here}_n; }}")
                 elif r.red == "entropy":
                     K.append(f"{{ const double a_ = fabs({val}); rv{ri_here}_a += a_; if (a_ > 0.0) rv{ri_here}_b += a_ * log(a_); }}")
                 elif r.red == "minmax":
@@ -804,7 +815,7 @@ def _red_decls(spec: PassSpec) -> List[str]:
     K: List[str] = []
     for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
         if r.red == "var":
-            K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0, rv{ri}_n = 0.0; bool rv{ri}_h = false;")
+            K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
         elif r.red in ("entropy",):
             K.append(f"double rv{ri}_a = 0.0, rv{ri}_b = 0.0;")
         elif r.red == "minmax":
@@ -833,7 +844,7 @@ def _red_flush(spec: PassSpec, cta: str) -> List[str]:
     for ri, r in enumerate(reds):
         base = f"p.part[(size_t)({cta}) * NSLOTS_RED + {r.slot}"
         if r.red == "var":
-            K.append(f"{{ double n_ = rv{ri}_n, mu_ = 0.0, q_ = 0.0;")
+            K.append(f"{{ double n_ = (double)rv{ri}_n, mu_ = 0.0, q_ = 0.0;")
             K.append(f"  if (n_ > 0.0) {{ mu_ = rv{ri}_piv + rv{ri}_s1 / n_; q_ = rv{ri}_s2 - rv{ri}_s1 * rv{ri}_s1 / n_; if (q_ < 0.0) q_ = 0.0; }}")
             K.append("  block_chan(n_, mu_, q_, red_scratch);")
             K.append(f"  if (tid == 0) {{ {base}] = n_; {base} + 1] = mu_; {base} + 2] = q_;")
@@ -1002,11 +1013,12 @@ def emit_pass(spec: PassSpec) -> str:
     L.append("  if (l < 0) l += p.n0g; else if (l >= p.nl) l -= p.n0g;")
     L.append("  return l;")
     L.append("}")
+    L.append("extern __shared__ __align__(128) unsigned char sten_smem[];")
     L.append("struct FCtx {")
     for f in spec.fields:
         ct = CTYPE[f.dtype]
         if f.staged:
-            L.append(f"  const {ct}* pl{f.slot}[2 * RAD + 1]; int o{f.slot};")
+            L.append(f"  unsigned int so{f.slot}[2 * RAD + 1]; unsigned int o{f.slot};")
         else:
             L.append(f"  const {ct}* gp{f.slot};")
     L.append(f"  float sc[{max(spec.n_scalars, 1)}];")
@@ -1026,7 +1038,7 @@ def emit_pass(spec: PassSpec) -> str:
     K: List[str] = []
     K.append(f'extern "C" __global__ void __launch_bounds__(NT, {cfg.min_blocks}) '
              f"sten_kernel(const __grid_constant__ Params p) {{")
-    K.append("  extern __shared__ __align__(128) unsigned char smem[];")
+    K.append("  unsigned char* smem = sten_smem;")
     K.append("  u64* bars = (u64*)smem;")
     K.append(f"  double* red_scratch = (double*)(smem + {red_off});")
     K.append("  const int tid = threadIdx.x;")
@@ -1160,17 +1172,21 @@ def emit_pass(spec: PassSpec) -> str:
     K.append("  }")
     for f in spec.fields:
         if f.staged:
-            K.append(f"  const int ob{f.slot} = (tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc};")
+            K.append(f"  const unsigned int ob{f.slot} = (tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc};")
     K.append("  const size_t col = (size_t)(tj0 + tjb) * p.n2 + k;")
     K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
+    K.append("  const size_t out_base = (size_t)p.out_lo * plane_n;")
+    K.append("  int sb = 0;  // ring slot of plane i - RAD, rotated each plane")
     K.append("  for (int i = ib; i < ie; ++i) {")
     K.append("    const int gi = i + p.i_base;")
+    K.append("    int sslot[2 * RAD + 1];")
+    K.append("    #pragma unroll")
+    K.append("    for (int d = 0; d < 2 * RAD + 1; ++d) { const int t_ = sb + d; sslot[d] = t_ >= NSLOT ? t_ - NSLOT : t_; }")
     for f in spec.fields:
         if f.staged:
             ct = CTYPE[f.dtype]
             K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD + 1; ++d) "
-                     f"x.pl{f.slot}[d] = (const {ct}*)(smem + {rings[f.slot]} + "
-                     f"((i + d - RAD - p_first) % NSLOT) * {plane_bytes(spec, f)});")
+                     f"x.so{f.slot}[d] = ({rings[f.slot]}u + (unsigned)sslot[d] * {plane_bytes(spec, f)}u) / {ESIZE[f.dtype]}u;")
     if ghost and spec.i_periodic:
         K.append("    const bool i_in = true;")
     else:
@@ -1185,7 +1201,7 @@ def emit_pass(spec: PassSpec) -> str:
     K.append("      const size_t vox = pbase + (size_t)m * p.n2;")
     for f in spec.fields:
         if f.staged:
-            K.append(f"      x.o{f.slot} = ob{f.slot} + m * {spec.box(f)[0]};")
+            K.append(f"      x.o{f.slot} = ob{f.slot} + m * {spec.box(f)[0]}u;")
         else:
             ct = CTYPE[f.dtype]
             K.append(f"      x.gp{f.slot} = (const {ct}*)p.fld[{f.slot}] + vox * {f.nc};")
@@ -1210,6 +1226,7 @@ def emit_pass(spec: PassSpec) -> str:
         K.append("    }")
     K.append("    ok = __syncthreads_and(ok);")
     K.append("    if (!ok) break;")
+    K.append("    sb = (sb + 1 == NSLOT) ? 0 : sb + 1;")
     if staged:
         K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
     K.append("  }")
@@ -1255,6 +1272,7 @@ def emit_pass(spec: PassSpec) -> str:
         K.append("    }")
         K.append("    const int gi = (int)i;")
         K.append("    const size_t vox = ((size_t)(sten_plane(p, gi)) * p.n1 + j) * p.n2 + k;")
+        K.append("    const size_t out_base = (size_t)p.out_lo * p.n1 * p.n2;")
         K.append(f"    float rv[{nroot}];")
         K.append("    eval_slow(p, gi, (int)j, (int)k, rv);")
         K += ["    " + k for k in _epilogue(spec, e, scan_ok=False)]

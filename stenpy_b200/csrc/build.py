@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 REPO = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libstenpy_b200.so")
-SOURCES = ["stenpy_abi.cu", "noalloc.cu"]
+SOURCES = ["stenpy_abi.cu", "noalloc.cu", "mlp_kernels.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -130,7 +130,7 @@ def test_every_tma_x_coordinate_is_16_byte_aligned(dtype, expr, boundary):
     issue — plane boxes for every tile and the periodic wrap strips — for every
     candidate schedule, and check them on the host."""
     from stenpy_b200 import autotune as AT
-    from stenpy_b200.codegen import ESIZE, strip_boxes, tmap_specs
+    from stenpy_b200.codegen import ESIZE, strip_boxes, tmap_specs, with_config
     import dataclasses
     shape = (24, 40, 96)
     fm = {"f": torch.zeros(shape, dtype=dtype), "u": torch.zeros(shape + (3,), dtype=dtype)}
@@ -142,7 +142,7 @@ def test_every_tma_x_coordinate_is_16_byte_aligned(dtype, expr, boundary):
     n2 = shape[2]
     for pp in plan.passes:
         for cfg in [pp.spec.cfg] + AT.candidates(pp.spec):
-            spec = dataclasses.replace(pp.spec, cfg=cfg)
+            spec = with_config(pp.spec, cfg)
             for slot, kind, (bw, bh) in tmap_specs(spec):
                 f = spec.fields[slot]
                 es = ESIZE[f.dtype]

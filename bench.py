@@ -404,6 +404,216 @@ def run_lazy(args):
     print(json.dumps(line), flush=True)
 
 
+def run_costmodel(args):
+    """Config 4: random expression DAGs timed by the autotuner, an MLP (the library's
+    CUDA forward/backward/Adam kernels) trained on the timings, top-3 regret on
+    held-out DAGs whose every candidate was timed."""
+    import numpy as np
+    from stenpy_b200 import autotune as AT
+    from stenpy_b200 import costmodel as CM
+    from stenpy_b200 import fused_compiler as FC
+    rng = np.random.default_rng(args.seed)
+    n_dag, n_hold, n_sub = args.dags, args.heldout, args.train_cands
+    dags = []
+    sources = []
+    for d in range(n_dag):
+        g, wanted, shape, dtype = CM.random_dag(rng)
+        try:
+            plan = FC.Planner(CM.placeholder_graph(g), wanted, dtype).plan()
+        except FC.FusionError:
+            continue
+        held = d >= n_dag - n_hold
+        picks = []
+        for pp in plan.passes:
+            cands = AT.candidates(pp.spec)
+            if not held:
+                idx = rng.choice(len(cands), size=min(n_sub, len(cands)), replace=False)
+                cands = [cands[i] for i in sorted(idx)]
+            picks.append(cands)
+            sources += [FC.emit_pass(AT.with_config(pp.spec, c)) for c in cands]
+        dags.append((d, g, wanted, shape, dtype, held, picks))
+    t0 = time.time()
+    n_comp = CM.precompile(sources)          # spawn pool, before the first CUDA call
+    compile_s = time.time() - t0
+    dev = torch.device("cuda", 0)
+    t0 = time.time()
+    tune_s_total = 0.0
+    for d, g, wanted, shape, dtype, held, picks in dags:
+        gd = CM.materialize(g, dev, seed=d * 10)
+        plan = FC.Planner(gd, wanted, dtype).plan()
+        values, _ = FC.bind(plan, gd, wanted)
+        for pp, cands in zip(plan.passes, picks):
+            t1 = time.time()
+            AT.tune_pass(pp, values, plan.shape, dev, cands=[AT.with_config(pp.spec, c).cfg for c in cands],
+                         tag=f"cm-{'hold' if held else 'train'}-{d}", reuse=False)
+            tune_s_total += time.time() - t1
+        del gd, values
+        torch.cuda.empty_cache()
+    collect_s = time.time() - t0
+    recs = CM.load_records(AT.LOG_PATH, tags=["cm-"])
+    train = [r for r in recs if r["tag"].startswith("cm-train")]
+    hold = [r for r in recs if r["tag"].startswith("cm-hold")]
+    X, y = CM.records_to_xy(train)
+    model = CM.CostModel(X.shape[1], dev, seed=args.seed)
+    t0 = time.time()
+    hist = model.fit(X, y, steps=args.train_steps)
+    torch.cuda.synchronize()
+    fit_s = time.time() - t0
+    model.save(os.path.join(os.path.dirname(AT.LOG_PATH), "costmodel.npz"))
+    ev = CM.evaluate(model, hold, k=3, seed=args.seed)
+    Xh, yh = CM.records_to_xy(hold)
+    rmse = float(((model.predict(Xh) - yh.double()) ** 2).mean().sqrt())
+    line = {"metric": "cost-model top-3 schedule regret vs exhaustive autotuning", "value": (ev["model_topk"] or {}).get("mean"),
+            "unit": "fraction", "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+            "config": {"workload": f"{len(dags)} random DAGs of 3-20 ops, grids 64..512 per dim (multiples of 32), "
+                                   f"FP32/BF16; {n_hold} held out with every candidate timed, training DAGs "
+                                   f"with {n_sub} random candidates each",
+                       "candidates_per_pass": ev["candidates_per_pass"]},
+            "regret": ev, "train_records": len(train), "heldout_records": len(hold),
+            "heldout_rmse_log_ns_per_voxel": rmse, "loss_history": hist[::5] + hist[-1:],
+            "seconds": {"compile": compile_s, "collect": collect_s, "fit": fit_s, "kernels_compiled": n_comp}}
+    print(json.dumps(line), flush=True)
+
+
+def make_batch_jobs(n, seed, lo, hi, dev):
+    """The batched workload: ``n`` independent fields (dims uniform in [lo, hi],
+    60% FP32 / 40% BF16), field i with expression i mod 8, periodic boundaries."""
+    import stenpy_b200 as S
+    from stenpy_b200.batch import BatchJob
+    from stenpy_b200.synth import batch_field, batch_specs
+    specs = batch_specs(n, seed=seed, lo=lo, hi=hi)
+    jobs, fields = [], []
+    for expr, dt, shape, fseed in specs:
+        f = batch_field(expr, dt, shape, fseed, device=dev)
+        g, sink, *_ = S.compile_expression(expr, boundary="periodic", field_map={"f": f})
+        jobs.append(BatchJob(g, [sink]))
+        fields.append(f)
+    return specs, jobs, fields
+
+
+def run_batch(args):
+    """Config 3: 256 uneven fields x 8 expressions in ONE persistent launch per step,
+    replayed from a CUDA graph, schedules from the batch autotuner."""
+    from stenpy_b200 import batch as B
+    world, rank, local = _dist()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    peak, peak_kind = _peaks()
+    specs, jobs, fields = make_batch_jobs(args.batch_fields, args.seed + rank, args.batch_lo, args.batch_hi, dev)
+    t0 = time.time()
+    tune_log = []
+    if args.no_tune:
+        threads, configs = 128, None
+    else:
+        threads, configs = B.tune_batch(jobs, dev, log=tune_log)
+    tune_s = time.time() - t0
+    prog = B.build(jobs, dev, configs, threads)
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):
+        prog.enqueue(stream)
+    torch.cuda.synchronize()
+    prog.check()
+    cg = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(cg, stream=stream):
+        prog.enqueue(stream)
+
+    def replay():
+        with torch.cuda.stream(stream):
+            cg.replay()
+
+    with ClockSampler(local) as cs:
+        ms, per = time_graph(replay, stream, args.steps, args.warmup, world, dev)
+        n_more = max(1, int(1500.0 / max(ms, 1e-3)))
+        for _ in range(n_more):
+            replay()
+        torch.cuda.synchronize()
+    prog.check()
+    vox = prog.voxels()
+    alg = prog.algorithmic_bytes()
+    line = {"metric": "batched fused-expr throughput (Gvoxel/s), HBM roofline fraction",
+            "value": vox * world / (ms * 1e-3) / 1e9, "unit": "Gvoxel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "storage": "60% fp32 / 40% bf16 fields and outputs",
+            "data": "synthetic",
+            "config": {"workload": f"{len(jobs)} independent fields, dims uniform in [{args.batch_lo}, "
+                                   f"{args.batch_hi}], field i gets expression i mod 8 of laplacian, grad_mag, "
+                                   "curl (3-component field), f**2+tanh(f)*exp(f), clamp(log(abs(f)+1),0,2), "
+                                   "trace(hessian), integrate, 256-bin entropy_hist; periodic",
+                       "voxels": vox, "algorithmic_bytes": alg,
+                       "l2": f"inputs ({alg / 1e9:.1f} GB per step) larger than L2 (126 MB)",
+                       "step": "one CUDA-graph replay of one persistent launch", "parallelism": f"replicas x{world}",
+                       "threads": threads, "ctas": prog.n_ctas, "work_items": prog.n_items,
+                       "programs": len(prog.mod.specs), "blocks_per_sm": prog.mod.blocks_per_sm,
+                       "registers": prog.mod.regs, "local_bytes": prog.mod.local_bytes,
+                       "tma_jobs": sum(1 for p in prog.plans if any(f.tma for pp in p.passes for f in pp.spec.fields))},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms * 1e-3) / 1e9 / peak, "peak_kind": peak_kind, "traffic": None,
+                         "kernel": "sten_batch (the only launch of a step)"},
+            "gpu_launches": args.steps, "clocks": cs.summary(),
+            "tuning": {"seconds": tune_s, "timed": len(tune_log),
+                       "schedules": sorted({json.dumps(vars(c), sort_keys=True) for c in (configs or {}).values()})}}
+    if not args.no_e2e:
+        host_in = [f.cpu().pin_memory() for f in fields]
+        outs = [o for job in jobs for o in job.outputs.values()]
+        host_out = [torch.empty(o.shape, dtype=o.dtype, pin_memory=True) for o in outs]
+        host_tab = torch.empty(prog.table.numel(), dtype=torch.float64, pin_memory=True)
+
+        def e2e_step():
+            with torch.cuda.stream(stream):
+                for d, h in zip(fields, host_in):
+                    d.copy_(h, non_blocking=True)
+                prog.enqueue(stream)
+                for h, o in zip(host_out, outs):
+                    h.copy_(o, non_blocking=True)
+                host_tab.copy_(prog.table, non_blocking=True)
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        _barrier(world)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n = max(2, min(args.steps, 5))
+        a.record(stream)
+        for _ in range(n):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ems = _max_over_ranks(a.elapsed_time(b) / n, world, dev)
+        prog.check()
+        line["e2e"] = {"value": vox * world / (ems * 1e-3) / 1e9, "unit": "Gvoxel/s", "ms_per_step": ems,
+                       "h2d_bytes_per_step": sum(h.numel() * h.element_size() for h in host_in),
+                       "d2h_bytes_per_step": sum(h.numel() * h.element_size() for h in host_out) + 8 * host_tab.numel()}
+    if rank == 0 and not args.no_cpu:
+        # the reference algorithm (CPU FP64 oracle) on one field of each expression, cropped
+        from oracle import stenpy_oracle as O
+        import stenpy_b200 as S
+        torch.set_num_threads(os.cpu_count() or 1)
+        sample = []
+        for (expr, dt, shape, fseed), f in list(zip(specs, fields))[:8]:
+            fc = f[:32].double().cpu()
+            g, sink, *_ = S.compile_expression(expr, boundary="periodic", field_map={"f": fc})
+            sample.append((g, sink, fc[..., 0].numel() if expr.startswith("curl") else fc.numel()))
+        ts = []
+        for rep in range(2):
+            t = time.perf_counter()
+            for g, sink, _ in sample:
+                O.evaluate(g, [sink])
+            ts.append(time.perf_counter() - t)
+        nv = sum(n for _, _, n in sample)
+        line["cpu_baseline"] = {"value": nv / min(ts) / 1e9, "unit": "Gvoxel/s", "cores": torch.get_num_threads(),
+                                "kind": "port", "sample": "one field per expression, first 32 planes, FP64 torch "
+                                                          "CPU oracle, best of 2"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+        if tune_log and args.tune_log:
+            with open(args.tune_log, "w") as fh:
+                for r in tune_log:
+                    fh.write(json.dumps(r) + "\n")
+    del cg
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def FC_check(dev):
     from stenpy_b200 import fused_compiler as FC
     FC.ErrorFlag.check(dev)
@@ -420,8 +630,19 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default schedules instead of autotuned ones")
-    ap.add_argument("--workload", default="fields", choices=["fields", "lazy"],
-                    help="fields: the 512^3 fused step (default); lazy: the out-of-core run")
+    ap.add_argument("--workload", default="fields", choices=["fields", "lazy", "costmodel", "batch"],
+                    help="fields: the 512^3 fused step (default); lazy: the out-of-core run; "
+                         "costmodel: the learned schedule-ranking study; batch: 256 uneven fields in one "
+                         "persistent launch")
+    ap.add_argument("--batch-fields", type=int, default=256)
+    ap.add_argument("--batch-lo", type=int, default=32)
+    ap.add_argument("--batch-hi", type=int, default=320)
+    ap.add_argument("--tune-log", default="")
+    ap.add_argument("--dags", type=int, default=300)
+    ap.add_argument("--heldout", type=int, default=60)
+    ap.add_argument("--train-cands", type=int, default=6)
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lazy-shape", default="1536x1536x1024")
     ap.add_argument("--budget-gb", type=float, default=8.0)
     args = ap.parse_args()
@@ -431,6 +652,12 @@ def main():
         return
     if args.workload == "lazy":
         run_lazy(args)
+        return
+    if args.workload == "costmodel":
+        run_costmodel(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
     world, rank, local = _dist()
     dev = torch.device("cuda", local)

@@ -68,6 +68,14 @@ void stenpy_free(void* p);
 int stenpy_module_load(const void* cubin, size_t cubin_size, const char* kernel_name,
                        int dyn_smem_max, StenModule** out);
 
+/* Resident blocks per SM for `block_threads` threads and `dyn_smem` bytes of
+ * dynamic shared memory, registers per thread and local (spill/stack) bytes per
+ * thread of the module's kernel. Sizes the persistent batch grid. New entry
+ * point: the reference launches Triton kernels with fixed grids
+ * (stenpy_engine.py:1961-1981) and has no persistent kernel. */
+int stenpy_module_info(StenModule* m, int block_threads, int dyn_smem, int* blocks_per_sm, int* regs,
+                       int* local_bytes);
+
 /* Unload a module. */
 void stenpy_module_free(StenModule* m);
 

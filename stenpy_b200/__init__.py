@@ -9,8 +9,10 @@ Public API (same names and contracts as the reference's ``stenpy`` /
 * ``Runtime`` (``run(graph, seed=None)``), ``MemoryManager``
 * ``Pipeline`` / attribute dispatch (``stenpy_b200.laplacian("f")``) and the
   ``stenpy`` command line (``python -m stenpy_b200``)
-* ``LazyRunner`` — out-of-core execution of fields held in pinned host memory
-* ``BatchedExecutor`` — many uneven fields in one persistent launch
+* ``LazyPipeline`` / ``run_chunked`` — out-of-core execution of fields held in
+  pinned host memory
+* ``run_batch`` / ``BatchJob`` — many graphs over uneven fields in one persistent
+  launch (``stenpy_b200.batch``)
 
 Kernels are generated per graph and compiled with NVRTC for sm_100a; the C ABI is
 ``include/stenpy_b200.h`` (``libstenpy_b200.so``). There is no CPU execution path.
@@ -30,6 +32,7 @@ __all__ = [
     "compile_expression", "compile_expressions", "parse_expression",
     "MemoryManager", "Runtime", "run_single_op", "PassConfig",
     "Pipeline", "PerfStats", "load_tensor", "save_tensor", "LazyPipeline", "run_chunked",
+    "run_batch", "BatchJob",
 ]
 
 
@@ -39,6 +42,9 @@ def __getattr__(name: str):
     if name in ("LazyPipeline", "run_chunked"):
         from . import lazy
         return getattr(lazy, name)
+    if name in ("run_batch", "BatchJob"):
+        from . import batch
+        return getattr(batch, name)
     if name in OP_REGISTRY:
         return OperatorDispatch(name)
     raise AttributeError(f"module 'stenpy_b200' has no attribute {name!r}")

@@ -23,7 +23,7 @@ ABI_SYMBOLS = (
     "stenpy_nvrtc_compile", "stenpy_free", "stenpy_module_load", "stenpy_module_free",
     "stenpy_launch", "stenpy_encode_tmap_3d", "stenpy_finalize", "stenpy_pass_noalloc",
     "stenpy_mlp_param_count", "stenpy_mlp_workspace_floats", "stenpy_mlp_forward", "stenpy_mlp_loss_grad",
-    "stenpy_adam_step",
+    "stenpy_adam_step", "stenpy_module_info",
 )
 
 
@@ -79,6 +79,7 @@ def lib() -> ctypes.CDLL:
         L.stenpy_free.restype = None
         L.stenpy_module_load.argtypes = [c.c_void_p, c.c_size_t, c.c_char_p, c.c_int, c.POINTER(c.c_void_p)]
         L.stenpy_module_free.argtypes = [c.c_void_p]
+        L.stenpy_module_info.argtypes = [c.c_void_p, c.c_int, c.c_int] + [c.POINTER(c.c_int)] * 3
         L.stenpy_module_free.restype = None
         L.stenpy_launch.argtypes = [c.c_void_p] + [c.c_uint] * 7 + [c.c_void_p, c.c_void_p, c.c_size_t]
         L.stenpy_encode_tmap_3d.argtypes = [c.c_void_p, c.c_int, c.c_void_p, c.c_uint64, c.c_uint64,
@@ -164,6 +165,14 @@ def load_module(key: str, cubin: bytes, kernel_name: str, dyn_smem_max: int, dev
     with _lock:
         _modules[(key, device)] = out.value
     return out.value
+
+
+def module_info(module: int, block_threads: int, dyn_smem: int) -> Tuple[int, int, int]:
+    """(resident blocks per SM, registers per thread, local bytes per thread)."""
+    b, r, loc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().stenpy_module_info(module, int(block_threads), int(dyn_smem), ctypes.byref(b), ctypes.byref(r),
+                                    ctypes.byref(loc)), "module_info")
+    return b.value, r.value, loc.value
 
 
 def launch(module: int, grid: Tuple[int, int, int], block: Tuple[int, int, int], dyn_smem: int,

@@ -102,6 +102,7 @@ class RootSpec:
     slot: int = -1      # first partial slot (red) / histogram base (hist)
     bins: int = 0
     lohi_index: int = -1  # hist: scalar-table index of (min, max)
+    table_index: int = -1  # hist: scalar-table index of the entropy
     dx: Tuple[float, float, float] = (1.0, 1.0, 1.0)  # integrate / scan spacing
     method: str = "simpson"
 
@@ -423,7 +424,7 @@ class _Emitter:
         if n.op == "field":
             self.field_slow(n, i, j, k, arr, body)
         elif n.op == "scalar":
-            body.append(f"{arr}[0] = (float)p.scal[{n.a('index')}];")
+            body.append(f"{arr}[0] = (float)__ldcg(p.scal + {n.a('index')});")
         elif nid in self.need_fn:
             body.append(f"SS{nid}(p, {i}, {j}, {k}, {arr});")
         else:
@@ -444,7 +445,7 @@ class _Emitter:
             self.field_slow(n, i, j, k, o, body)
             return
         if n.op == "scalar":
-            body.append(f"{o}[0] = (float)p.scal[{n.a('index')}];")
+            body.append(f"{o}[0] = (float)__ldcg(p.scal + {n.a('index')});")
             return
         if n.op == "d1":
             self.slow_d1(n, i, j, k, o, body)
@@ -679,6 +680,7 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
     off = (off + 127) // 128 * 128
     red_off = off
     off += 3 * 32 * 8
+    off += sum(4 * r.bins for r in spec.roots if r.kind == "red" and r.red == "hist")
     return off, rings, red_off
 
 
@@ -800,6 +802,11 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
                     K.append(f"{{ const double a_ = fabs({val}); rv{ri_here}_a += a_; if (a_ > 0.0) rv{ri_here}_b += a_ * log(a_); }}")
                 elif r.red == "minmax":
                     K.append(f"{{ const double t_ = {val}; rv{ri_here}_a = fmin(rv{ri_here}_a, t_); rv{ri_here}_b = fmax(rv{ri_here}_b, t_); }}")
+                elif r.red == "hist":
+                    # bin index as the oracle forms it: floor((x - lo) / (hi - lo) * bins), FP64
+                    K.append(f"if (rv{ri_here}_hh > rv{ri_here}_hl) {{ const double t_ = ({val} - rv{ri_here}_hl)"
+                             f" / (rv{ri_here}_hh - rv{ri_here}_hl) * {float(r.bins)!r}; int b_ = (int)floor(t_);"
+                             f" b_ = b_ < 0 ? 0 : (b_ > {r.bins - 1} ? {r.bins - 1} : b_); sten_hist_add(rv{ri_here}_hs, b_); }}")
                 elif r.red == "integrate":
                     sm = 1 if r.method == "simpson" else 0
                     K.append(f"rv{ri_here}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
@@ -811,10 +818,31 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
     return K
 
 
-def _red_decls(spec: PassSpec) -> List[str]:
-    K: List[str] = []
+def hist_offsets(spec: PassSpec, red_off: int) -> Tuple[Dict[int, int], int]:
+    """Shared-memory byte offsets of the per-CTA histograms (by reduction-root
+    index) placed after the block-reduction scratch, and the end of the region."""
+    off = red_off + 3 * 32 * 8
+    offs: Dict[int, int] = {}
     for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
-        if r.red == "var":
+        if r.red == "hist":
+            offs[ri] = off
+            off += 4 * r.bins
+    return offs, off
+
+
+def _red_decls(spec: PassSpec, where: str = "main") -> List[str]:
+    K: List[str] = []
+    hoffs = hist_offsets(spec, smem_layout(spec)[2])[0] if where == "main" else {}
+    for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
+        if r.red == "hist":
+            K.append(f"const double rv{ri}_hl = __ldcg(p.scal + {r.lohi_index}), "
+                     f"rv{ri}_hh = __ldcg(p.scal + {r.lohi_index + 1});")
+            if where == "main":
+                K.append(f"unsigned int* rv{ri}_hs = (unsigned int*)(smem + {hoffs[ri]});")
+                K.append(f"for (int b_ = tid; b_ < {r.bins}; b_ += NT) rv{ri}_hs[b_] = 0u;")
+            else:
+                K.append(f"unsigned long long* rv{ri}_hs = p.hist + {r.slot};")
+        elif r.red == "var":
             K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
         elif r.red in ("entropy",):
             K.append(f"double rv{ri}_a = 0.0, rv{ri}_b = 0.0;")
@@ -837,13 +865,19 @@ def _sum_from_var(spec: PassSpec, r: RootSpec) -> Optional[int]:
     return None
 
 
-def _red_flush(spec: PassSpec, cta: str) -> List[str]:
-    """Block-reduce each accumulator and write this CTA's partial row."""
+def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
+    """Block-reduce each accumulator and write this CTA's partial row; add the
+    CTA's histogram counts to the global (integer, order-free) histogram."""
     K: List[str] = []
     reds = [r for r in spec.roots if r.kind == "red"]
     for ri, r in enumerate(reds):
         base = f"p.part[(size_t)({cta}) * NSLOTS_RED + {r.slot}"
-        if r.red == "var":
+        if r.red == "hist":
+            if where == "main":
+                K.append("__syncthreads();")
+                K.append(f"for (int b_ = tid; b_ < {r.bins}; b_ += NT) {{ const unsigned int c_ = rv{ri}_hs[b_];"
+                         f" if (c_) atomicAdd(p.hist + {r.slot} + b_, (unsigned long long)c_); }}")
+        elif r.red == "var":
             K.append(f"{{ double n_ = (double)rv{ri}_n, mu_ = 0.0, q_ = 0.0;")
             K.append(f"  if (n_ > 0.0) {{ mu_ = rv{ri}_piv + rv{ri}_s1 / n_; q_ = rv{ri}_s2 - rv{ri}_s1 * rv{ri}_s1 / n_; if (q_ < 0.0) q_ = 0.0; }}")
             K.append("  block_chan(n_, mu_, q_, red_scratch);")
@@ -977,12 +1011,21 @@ def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Option
 SHELL_THREADS = 256
 
 
-def emit_pass(spec: PassSpec) -> str:
+def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int = 0) -> str:
     """Source of the pass: ``sten_kernel`` (z-march over the tile grid) and, when the
     pass has a stencil reach R > 0 and no scan, ``sten_shell`` (one thread per voxel
-    within R of a face, evaluated from global memory with boundary rules)."""
-    with open(HEADER_PATH) as fh:
-        header = fh.read()
+    within R of a face, evaluated from global memory with boundary rules); with
+    histogram roots also ``sten_hist_final`` (entropy from the counts).
+
+    With ``batch_ns`` the same code is emitted as device functions in that
+    namespace for the persistent batch kernel (``run_item``: one z-march tile or
+    one block of shell voxels per call, parameters read from global memory), without
+    the shared header; ``batch_threads`` is the batch kernel's block size."""
+    batch = batch_ns is not None
+    header = ""
+    if not batch:
+        with open(HEADER_PATH) as fh:
+            header = fh.read()
     e = _Emitter(spec)
     cfg = spec.cfg
     R = spec.radius
@@ -994,9 +1037,15 @@ def emit_pass(spec: PassSpec) -> str:
     assert cfg.tk % 32 == 0 and (cfg.tj * cfg.tk) % cfg.threads == 0 and cfg.prefetch >= 1
     vpt = cfg.tj * cfg.tk // cfg.threads
     L = e.lines
-    L.append(header)
+    if batch:
+        assert cfg.threads == batch_threads, "batch programs share the block size"
+        assert not spec.has_scan, "scans are not batched"
+    else:
+        L.append(header)
     L.append(f"#define TJ {cfg.tj}\n#define TK {cfg.tk}\n#define NT {cfg.threads}\n#define RAD {R}"
              f"\n#define NSLOT {nslot}\n#define VPT {vpt}\n#define NSLOTS_RED {max(spec.nslots, 1)}")
+    if batch:
+        L.append(f"namespace {batch_ns} {{")
     ntma = len(tmap_specs(spec))
     nout = sum(1 for r in spec.roots if r.kind in ("out", "scan"))
     L.append("struct __align__(64) Params {")
@@ -1004,16 +1053,38 @@ def emit_pass(spec: PassSpec) -> str:
         L.append(f"  TmaDesc tmap[{ntma}];")
     L.append(f"  const void* fld[{max(len(spec.fields), 1)}];")
     L.append(f"  void* out[{max(nout, 1)}];")
-    L.append("  const double* scal; double* part; unsigned int* hist; int* err;")
+    L.append("  const double* scal; double* part; unsigned long long* hist; int* err;")
     L.append("  int n0g, n1, n2, nl, i_base, out_lo, n_out, seg_len, tiles_k, cta_off;")
     L.append("};")
-    L.append("__device__ __forceinline__ int sten_plane(const Params& p, int gi) {")
+    if batch:
+        # register copy of the scalar parameters; TMA descriptors stay in global memory
+        L.append("struct PView {")
+        if ntma:
+            L.append("  const TmaDesc* tmap;")
+        L.append(f"  const void* fld[{max(len(spec.fields), 1)}];")
+        L.append(f"  void* out[{max(nout, 1)}];")
+        L.append("  const double* scal; double* part; unsigned long long* hist; int* err;")
+        L.append("  int n0g, n1, n2, nl, i_base, out_lo, n_out, seg_len, tiles_k, cta_off;")
+        L.append("};")
+        L.append("__device__ __forceinline__ PView make_view(const Params& g) {")
+        L.append("  PView v;")
+        if ntma:
+            L.append("  v.tmap = g.tmap;")
+        L.append(f"  #pragma unroll\n  for (int i = 0; i < {max(len(spec.fields), 1)}; ++i) v.fld[i] = g.fld[i];")
+        L.append(f"  #pragma unroll\n  for (int i = 0; i < {max(nout, 1)}; ++i) v.out[i] = g.out[i];")
+        L.append("  v.scal = g.scal; v.part = g.part; v.hist = g.hist; v.err = g.err;")
+        L.append("  v.n0g = g.n0g; v.n1 = g.n1; v.n2 = g.n2; v.nl = g.nl; v.i_base = g.i_base; v.out_lo = g.out_lo;")
+        L.append("  v.n_out = g.n_out; v.seg_len = g.seg_len; v.tiles_k = g.tiles_k; v.cta_off = g.cta_off;")
+        L.append("  return v;")
+        L.append("}")
+    L.append("template <class P> __device__ __forceinline__ int sten_plane(const P& p, int gi) {")
     L.append("  // global plane index -> plane of the (possibly chunked) arrays")
     L.append("  int l = gi - p.i_base;")
     L.append("  if (l < 0) l += p.n0g; else if (l >= p.nl) l -= p.n0g;")
     L.append("  return l;")
     L.append("}")
-    L.append("extern __shared__ __align__(128) unsigned char sten_smem[];")
+    if not batch:
+        L.append("extern __shared__ __align__(128) unsigned char sten_smem[];")
     L.append("struct FCtx {")
     for f in spec.fields:
         ct = CTYPE[f.dtype]
@@ -1036,23 +1107,30 @@ def emit_pass(spec: PassSpec) -> str:
     scans = [r for r in spec.roots if r.kind == "scan"]
 
     K: List[str] = []
-    K.append(f'extern "C" __global__ void __launch_bounds__(NT, {cfg.min_blocks}) '
-             f"sten_kernel(const __grid_constant__ Params p) {{")
+    if batch:
+        K.append("__device__ __forceinline__ bool run_tile(const PView& p, const Params& pg, int bx, int by, int gdx) {")
+    else:
+        K.append(f'extern "C" __global__ void __launch_bounds__(NT, {cfg.min_blocks}) '
+                 f"sten_kernel(const __grid_constant__ Params p) {{")
+        K.append("  const Params& pg = p;")
+        K.append("  const int bx = blockIdx.x, by = blockIdx.y, gdx = gridDim.x;")
     K.append("  unsigned char* smem = sten_smem;")
     K.append("  u64* bars = (u64*)smem;")
     K.append(f"  double* red_scratch = (double*)(smem + {red_off});")
     K.append("  const int tid = threadIdx.x;")
-    K.append("  const int tile = blockIdx.x;")
+    K.append("  const int tile = bx;")
     K.append("  const int tk0 = (tile % p.tiles_k) * TK;")
     K.append("  const int tj0 = (tile / p.tiles_k) * TJ;")
-    K.append("  const int ib = p.out_lo + (int)blockIdx.y * p.seg_len;")
+    K.append("  const int ib = p.out_lo + by * p.seg_len;")
     K.append("  const int ie = min(ib + p.seg_len, p.out_lo + p.n_out);")
-    K.append("  const int cta = p.cta_off + (int)(blockIdx.y * gridDim.x + blockIdx.x);")
+    K.append("  const int cta = p.cta_off + by * gdx + bx;")
     K.append("  const bool edge_cta = tk0 == 0 || tk0 + TK >= p.n2 || tj0 == 0 || tj0 + TJ >= p.n1;")
     K.append("  FCtx x;")
     K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
-             f"x.sc[s] = (s < {spec.n_scalars}) ? (float)p.scal[s] : 0.0f;")
+             f"x.sc[s] = (s < {spec.n_scalars}) ? (float)__ldcg(p.scal + s) : 0.0f;")
     K += ["  " + k for k in _red_decls(spec)]
+    if any(r.red == "hist" for r in reds):
+        K.append("  __syncthreads();  // histogram cleared")
     for si, r in enumerate(scans):
         nc = e.g.nodes[r.node].nc
         K.append(f"  double sc{si}_acc[VPT * {nc}]; float sc{si}_prev[VPT * {nc}];")
@@ -1210,7 +1288,7 @@ def emit_pass(spec: PassSpec) -> str:
         K.append("      eval_fast(x, rv);")
     else:
         K.append("      const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-        K.append("      if (inter) eval_fast(x, rv); else eval_slow(p, gi, j, k, rv);")
+        K.append("      if (inter) eval_fast(x, rv); else eval_slow(pg, gi, j, k, rv);")
     K += ["      " + k for k in _epilogue(spec, e, scan_ok=True)]
     K.append("    }")
     if split:
@@ -1230,17 +1308,32 @@ def emit_pass(spec: PassSpec) -> str:
     if staged:
         K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
     K.append("  }")
-    K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return; }")
+    K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
+    K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
+             % (" false" if batch else ""))
     K += ["  " + k for k in _red_flush(spec, "cta")]
+    if batch:
+        if tma_fields:
+            # every requested plane was waited on: retire the barriers before the
+            # next item re-initialises this shared memory
+            K.append("  __syncthreads();")
+            K.append("  if (tid == 0) { for (int s = 0; s < NSLOT; ++s) mbar_inval(&bars[s]); }")
+        K.append("  return true;")
     K.append("}")
 
     if regions:
         # shell: voxels within RAD of a face, one per thread, evaluated from global memory
-        K.append(f'extern "C" __global__ void __launch_bounds__({SHELL_THREADS}) '
-                 f"sten_shell(const __grid_constant__ Params p) {{")
-        K.append(f"  __shared__ double red_scratch[96];")
+        if batch:
+            K.append("__device__ __forceinline__ void run_shell(const PView& p, const Params& pg, int bx) {")
+            K.append("  double* red_scratch = (double*)(sten_smem + 128);")
+        else:
+            K.append(f'extern "C" __global__ void __launch_bounds__({SHELL_THREADS}) '
+                     f"sten_shell(const __grid_constant__ Params p) {{")
+            K.append("  const Params& pg = p;")
+            K.append("  const int bx = blockIdx.x;")
+            K.append(f"  __shared__ double red_scratch[96];")
         K.append("  const int tid = threadIdx.x;")
-        K += ["  " + k for k in _red_decls(spec)]
+        K += ["  " + k for k in _red_decls(spec, "shell")]
         K.append("  const long long n0 = p.n0g, n1 = p.n1, n2 = p.n2;")
         K.append("  const long long g_lo = (long long)p.out_lo + p.i_base, g_hi = g_lo + p.n_out;")
         K.append("  const long long a1 = max(n1 - 2 * RAD, 0ll), a2 = max(n2 - 2 * RAD, 0ll);")
@@ -1252,7 +1345,7 @@ def emit_pass(spec: PassSpec) -> str:
             K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = 0, cC = 0;")
         else:
             K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
-        K.append("  const long long t = (long long)blockIdx.x * blockDim.x + tid;")
+        K.append("  const long long t = (long long)bx * blockDim.x + tid;")
         K.append("  if (t < cA + cB + cC) {")
         K.append("    long long i, j, k;")
         K.append("    if (t < cA) {            // planes within RAD of a dim-0 face")
@@ -1274,9 +1367,140 @@ def emit_pass(spec: PassSpec) -> str:
         K.append("    const size_t vox = ((size_t)(sten_plane(p, gi)) * p.n1 + j) * p.n2 + k;")
         K.append("    const size_t out_base = (size_t)p.out_lo * p.n1 * p.n2;")
         K.append(f"    float rv[{nroot}];")
-        K.append("    eval_slow(p, gi, (int)j, (int)k, rv);")
+        K.append("    eval_slow(pg, gi, (int)j, (int)k, rv);")
         K += ["    " + k for k in _epilogue(spec, e, scan_ok=False)]
         K.append("  }")
-        K += ["  " + k for k in _red_flush(spec, "p.cta_off + blockIdx.x")]
+        K += ["  " + k for k in _red_flush(spec, "p.cta_off + bx", "shell")]
         K.append("}")
+    hists = [r for r in reds if r.red == "hist"]
+    if hists and not batch:
+        K.append('extern "C" __global__ void __launch_bounds__(256) sten_hist_final(const __grid_constant__ Params p) {')
+        K.append("  __shared__ double red_scratch[96];")
+        K.append("  const double nvox = (double)p.n0g * (double)p.n1 * (double)p.n2;")
+        for r in hists:
+            nc = e.g.nodes[r.node].nc
+            K.append(f"  {{ const double s_ = sten_hist_qlogq(p.hist + {r.slot}, {r.bins}, nvox * {nc}, red_scratch);")
+            K.append(f"    if (threadIdx.x == 0) {{ const double lo_ = __ldcg(p.scal + {r.lohi_index}), "
+                     f"hi_ = __ldcg(p.scal + {r.lohi_index + 1});")
+            K.append(f"      ((double*)p.scal)[{r.table_index}] = hi_ > lo_ ? -s_ : 0.0; }} }}")
+        K.append("}")
+    if batch:
+        K.append("__device__ __noinline__ bool run_item(const Params& pg, int kind, int bx, int by, int gdx, int shell_cta0) {")
+        K.append("  PView p = make_view(pg);")
+        if regions:
+            K.append("  if (kind == 1) { p.cta_off = shell_cta0; run_shell(p, pg, bx); return true; }")
+        K.append("  return run_tile(p, pg, bx, by, gdx);")
+        K.append("}")
+        K.append(f"}}  // namespace {batch_ns}")
+        K.append("#undef TJ\n#undef TK\n#undef NT\n#undef RAD\n#undef NSLOT\n#undef VPT\n#undef NSLOTS_RED")
+    return "\n".join(L) + "\n" + "\n".join(K) + "\n"
+
+
+# ----------------------------------------------------------------------------- batch module
+BATCH_STRUCTS = r"""
+struct BPhase {            // one pass of one job (80 bytes)
+  unsigned long long params, part, table, hist;  // its Params; partial rows; scalar table; histograms
+  int prog, n_items, dep, gdx;                    // program; work items; phase to wait for (-1); tiles per plane row
+  int shell_cta0, ncta, nslots, red0;             // first shell partial row; partial rows; slots per row; first BRed
+  int nred, hist0, nhist, pad;                    // reductions; first BHist; histograms
+};
+struct BRed { int kind, slot, out_index, unbiased; double count, eps; };
+struct BHist { int base, bins, lohi, out_index; double count; };
+struct BatchArgs {
+  const int4* items;        // (phase, kind 0 tile | 1 shell, bx, by), in queue order
+  const BPhase* phases; const BRed* reds; const BHist* hists;
+  unsigned int* ctl;        // [0] queue head, [1] CTAs done, then done items and ready flag per phase
+  int* err;
+  int n_items, n_phases;
+};
+// the host packs these records with fixed layouts
+static_assert(sizeof(BPhase) == 80 && sizeof(BRed) == 32 && sizeof(BHist) == 24 && sizeof(BatchArgs) == 56,
+              "batch record layout");
+"""
+
+
+def emit_batch_module(specs: List[PassSpec], threads: int, min_blocks: int = 1) -> str:
+    """One module holding every program of a batch (``specs[i]`` in namespace
+    ``p<i>``) and ``sten_batch``, a persistent kernel whose CTAs take work items
+    from a queue in order. An item is one z-march tile or one block of shell voxels
+    of one pass of one job. The CTA completing the last item of a pass combines its
+    partial rows and histograms into the job's scalar table (same fixed-order
+    reduction as the standalone finalize) and sets the pass's ready flag; items of a
+    pass that reads those scalars wait for the flag (bounded). Items are queued so a
+    pass's prerequisites come first, so every wait is on items already taken by
+    running CTAs. The last CTA to finish resets the queue for the next launch."""
+    with open(HEADER_PATH) as fh:
+        header = fh.read()
+    L = [header, "extern __shared__ __align__(128) unsigned char sten_smem[];"]
+    for i, sp_ in enumerate(specs):
+        L.append(emit_pass(sp_, batch_ns=f"p{i}", batch_threads=threads))
+    L.append(BATCH_STRUCTS)
+    L.append(r"""
+__device__ __noinline__ void sten_batch_finalize(const BatchArgs& a, const BPhase& ph) {
+  double* scratch = (double*)(sten_smem + 128);
+  double* table = (double*)ph.table;
+  for (int r = 0; r < ph.nred; ++r) {
+    const BRed d = a.reds[ph.red0 + r];
+    sten_reduce_rows(d.kind, (const double*)ph.part, ph.ncta, ph.nslots, d.slot, d.unbiased, d.count, d.eps,
+                     table + d.out_index, scratch);
+  }
+  for (int h = 0; h < ph.nhist; ++h) {
+    const BHist d = a.hists[ph.hist0 + h];
+    const double s = sten_hist_qlogq((unsigned long long*)ph.hist + d.base, d.bins, d.count, scratch);
+    if (threadIdx.x == 0) {
+      const double lo = __ldcg(table + d.lohi), hi = __ldcg(table + d.lohi + 1);
+      table[d.out_index] = hi > lo ? -s : 0.0;
+    }
+  }
+}
+""")
+    K = [f'extern "C" __global__ void __launch_bounds__({threads}, {min_blocks}) '
+         "sten_batch(const __grid_constant__ BatchArgs a) {",
+         "  __shared__ int s_item, s_last;",
+         "  const int tid = threadIdx.x;",
+         "  unsigned int* done = a.ctl + 2;",
+         "  unsigned int* ready = a.ctl + 2 + a.n_phases;",
+         "  bool ok = true;",
+         "  for (;;) {",
+         "    // a CTA that hit an error stops the others at their next item",
+         "    if (tid == 0) s_item = *(volatile int*)a.err ? 0x7fffffff : (int)atomicAdd(a.ctl, 1u);",
+         "    __syncthreads();",
+         "    const int it = s_item;",
+         "    if (it >= a.n_items) break;",
+         "    const int4 w = a.items[it];",
+         "    const BPhase& ph = a.phases[w.x];",
+         "    if (ph.dep >= 0) {",
+         "      bool got = true;",
+         "      if (tid == 0) got = flag_wait_bounded(ready + ph.dep, STEN_WAIT_LIMIT_NS);",
+         "      if (!__syncthreads_and(got)) { ok = false; break; }",
+         "    }",
+         "    const void* prm = (const void*)ph.params;",
+         "    switch (ph.prog) {"]
+    for i in range(len(specs)):
+        K.append(f"      case {i}: ok = p{i}::run_item(*(const p{i}::Params*)prm, w.y, w.z, w.w, ph.gdx, "
+                 "ph.shell_cta0); break;")
+    K += ["      default: ok = false; break;",
+          "    }",
+          "    if (!ok) break;",
+          "    __threadfence();  // this item's partials and histogram counts, before it is counted done",
+          "    __syncthreads();",
+          "    if (tid == 0) { __threadfence(); s_last = atomicAdd(done + w.x, 1u) == (unsigned)ph.n_items - 1u; }",
+          "    __syncthreads();",
+          "    if (s_last) {",
+          "      __threadfence();",
+          "      sten_batch_finalize(a, ph);",
+          "      __syncthreads();",
+          "      if (tid == 0) { __threadfence(); atomicExch(ready + w.x, 1u); }",
+          "    }",
+          "  }",
+          "  if (!ok && tid == 0) atomicExch(a.err, STEN_ERR_TMA_TIMEOUT);",
+          "  __syncthreads();",
+          "  if (tid == 0) {",
+          "    __threadfence();",
+          "    if (atomicAdd(a.ctl + 1, 1u) == gridDim.x - 1) {",
+          "      for (int i = 0; i < 2 + 2 * a.n_phases; ++i) a.ctl[i] = 0u;",
+          "      __threadfence();",
+          "    }",
+          "  }",
+          "}"]
     return "\n".join(L) + "\n" + "\n".join(K) + "\n"

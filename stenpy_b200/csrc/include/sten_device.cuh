@@ -85,6 +85,9 @@ STEN_DEV u32 smem_u32(const void* p) {
 STEN_DEV void mbar_init(u64* bar, u32 count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
 }
+STEN_DEV void mbar_inval(u64* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
 STEN_DEV void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -114,6 +117,20 @@ STEN_DEV bool mbar_wait_bounded(u64* bar, u32 parity, u64 limit_ns) {
     if (global_ns() - t0 > limit_ns) return false;
   }
   return true;
+}
+// Bounded wait for a flag that another CTA of this launch sets to non-zero (after a
+// __threadfence); acquire loads with a short back-off. False after limit_ns.
+STEN_DEV bool flag_wait_bounded(const unsigned int* f, u64 limit_ns) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+  if (v) return true;
+  const u64 t0 = global_ns();
+  for (;;) {
+    __nanosleep(200);
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(f) : "memory");
+    if (v) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
 }
 // 3-D tiled TMA load of one box into shared memory; completion counted on `bar`.
 // Coordinates: x innermost (elements), y, z. x * elem_size must be a multiple of 16.
@@ -212,6 +229,67 @@ STEN_DEV void block_chan(double& n, double& mean, double& m2, double* scratch) {
     if (lane < nw) { a = scratch[lane]; b = scratch[32 + lane]; c = scratch[64 + lane]; }
     warp_chan(a, b, c);
     n = a; mean = b; m2 = c;
+  }
+}
+
+// ------------------------------------------------------------------ histograms
+STEN_DEV void sten_hist_add(unsigned int* h, int b) { atomicAdd(h + b, 1u); }
+STEN_DEV void sten_hist_add(unsigned long long* h, int b) { atomicAdd(h + b, 1ull); }
+// sum over non-empty bins of q log q, q = count / n (the entropy is its negation),
+// clearing the counts for the next run. Fixed bins per thread and a fixed
+// reduction tree: deterministic. Whole block; the result is valid in thread 0.
+STEN_DEV double sten_hist_qlogq(unsigned long long* h, int bins, double n, double* scratch) {
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < bins; b += blockDim.x) {
+    const unsigned long long c = __ldcg(h + b);
+    if (c) { const double q = (double)c / n; acc += q * log(q); }
+    h[b] = 0ull;
+  }
+  return block_sum(acc, scratch);
+}
+
+// ------------------------------------------------------------------ in-kernel finalize
+// Kinds of per-CTA partial rows (same numbering as the library's STENPY_RED_*).
+#define STEN_RED_SUM 0
+#define STEN_RED_MEAN 1
+#define STEN_RED_NORM_L2 2
+#define STEN_RED_VARIANCE 3
+#define STEN_RED_ENTROPY 4
+#define STEN_RED_INTEGRATE 5
+#define STEN_RED_MIN_MAX 6
+// Combine rows part[c * nslots + slot], c < ncta, into the final value(s) at out[0]
+// (out[1] for min/max). Each thread folds rows t, t + blockDim, ... in order and a
+// fixed warp/block tree combines them: deterministic for a given block size.
+// Whole block; partials are read through L2 (written by other CTAs of this launch).
+STEN_DEV void sten_reduce_rows(int kind, const double* part, int ncta, int nslots, int slot, int unbiased,
+                               double count, double eps, double* out, double* scratch) {
+  const int t = threadIdx.x;
+  double x0 = 0.0, x1 = 0.0, x2 = 0.0;
+  if (kind == STEN_RED_MIN_MAX) { x0 = __longlong_as_double(0x7ff0000000000000ll); x1 = -x0; }
+  for (int c = t; c < ncta; c += blockDim.x) {
+    const double* row = part + (size_t)c * nslots + slot;
+    if (kind == STEN_RED_VARIANCE) chan_merge(x0, x1, x2, __ldcg(row), __ldcg(row + 1), __ldcg(row + 2));
+    else if (kind == STEN_RED_ENTROPY) { x0 += __ldcg(row); x1 += __ldcg(row + 1); }
+    else if (kind == STEN_RED_MIN_MAX) { x0 = fmin(x0, __ldcg(row)); x1 = fmax(x1, __ldcg(row + 1)); }
+    else x0 += __ldcg(row);
+  }
+  double r0, r1 = 0.0, r2 = 0.0;
+  if (kind == STEN_RED_VARIANCE) { block_chan(x0, x1, x2, scratch); r0 = x0; r2 = x2; }
+  else if (kind == STEN_RED_MIN_MAX) { r0 = block_min(x0, scratch); r1 = block_max(x1, scratch); }
+  else if (kind == STEN_RED_ENTROPY) { r0 = block_sum(x0, scratch); r1 = block_sum(x1, scratch); }
+  else r0 = block_sum(x0, scratch);
+  if (t != 0) return;
+  switch (kind) {
+    case STEN_RED_MEAN: out[0] = r0 / count; break;
+    case STEN_RED_NORM_L2: out[0] = sqrt(r0); break;
+    case STEN_RED_VARIANCE: {
+      const double den = unbiased ? (r0 - 1.0 > 1.0 ? r0 - 1.0 : 1.0) : (r0 > 1.0 ? r0 : 1.0);
+      out[0] = r2 / den;
+      break;
+    }
+    case STEN_RED_ENTROPY: { const double Z = r0 + eps; out[0] = (r0 * log(Z) - r1) / Z; break; }
+    case STEN_RED_MIN_MAX: out[0] = r0; out[1] = r1; break;
+    default: out[0] = r0; break;
   }
 }
 

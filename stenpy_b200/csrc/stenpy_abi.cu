@@ -49,6 +49,8 @@ struct Driver {
   CUresult (*ModuleGetFunction)(CUfunction*, CUmodule, const char*) = nullptr;
   CUresult (*ModuleUnload)(CUmodule) = nullptr;
   CUresult (*FuncSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
+  CUresult (*FuncGetAttribute)(int*, CUfunction_attribute, CUfunction) = nullptr;
+  CUresult (*OccupancyMaxActiveBlocksPerMultiprocessor)(int*, CUfunction, int, size_t) = nullptr;
   CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned,
                            unsigned, unsigned, CUstream, void**, void**) = nullptr;
   CUresult (*TensorMapEncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
@@ -79,6 +81,8 @@ void load_driver() {
             bind(h, "cuModuleGetFunction", g_drv.ModuleGetFunction) &&
             bind(h, "cuModuleUnload", g_drv.ModuleUnload) &&
             bind(h, "cuFuncSetAttribute", g_drv.FuncSetAttribute) &&
+            bind(h, "cuFuncGetAttribute", g_drv.FuncGetAttribute) &&
+            bind(h, "cuOccupancyMaxActiveBlocksPerMultiprocessor", g_drv.OccupancyMaxActiveBlocksPerMultiprocessor) &&
             bind(h, "cuLaunchKernel", g_drv.LaunchKernel) &&
             bind(h, "cuTensorMapEncodeTiled", g_drv.TensorMapEncodeTiled) &&
             bind(h, "cuGetErrorString", g_drv.GetErrorString);
@@ -218,6 +222,21 @@ int stenpy_module_load(const void* cubin, size_t cubin_size, const char* kernel_
     if (r != CUDA_SUCCESS) { g_drv.ModuleUnload(m->mod); delete m; return drv_fail(r, "cuFuncSetAttribute"); }
   }
   *out = m;
+  return STENPY_OK;
+}
+
+int stenpy_module_info(StenModule* m, int block_threads, int dyn_smem, int* blocks_per_sm, int* regs,
+                       int* local_bytes) {
+  if (!m || !m->fn || !blocks_per_sm || !regs || !local_bytes) return fail(STENPY_E_INVALID, "module_info: null argument");
+  if (block_threads <= 0 || block_threads > 1024 || dyn_smem < 0) return fail(STENPY_E_INVALID, "module_info: bad block");
+  int rc = ensure_context();
+  if (rc) return rc;
+  CUresult r = g_drv.OccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, m->fn, block_threads, (size_t)dyn_smem);
+  if (r != CUDA_SUCCESS) return drv_fail(r, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+  if ((r = g_drv.FuncGetAttribute(regs, CU_FUNC_ATTRIBUTE_NUM_REGS, m->fn)) != CUDA_SUCCESS)
+    return drv_fail(r, "cuFuncGetAttribute");
+  if ((r = g_drv.FuncGetAttribute(local_bytes, CU_FUNC_ATTRIBUTE_LOCAL_SIZE_BYTES, m->fn)) != CUDA_SUCCESS)
+    return drv_fail(r, "cuFuncGetAttribute");
   return STENPY_OK;
 }
 

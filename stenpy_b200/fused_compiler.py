@@ -104,8 +104,10 @@ class PassPlan:
     field_nodes: List[str]                 # graph node read by each Params::fld slot
     out_nodes: List[Tuple[str, str, int]]  # (graph node, "out" | "scan", components) per Params::out slot
     reductions: List[RedPlan]
+    hists: List[RootSpec] = dc_field(default_factory=list)  # histogram-entropy roots
     module: Optional[int] = None
     shell_module: Optional[int] = None
+    hist_module: Optional[int] = None
     smem: int = 0
     source: str = ""
     key: str = ""
@@ -127,6 +129,7 @@ class FusedPlan:
     live: List[str] = dc_field(default_factory=list)
     buffers: Dict[str, torch.Tensor] = dc_field(default_factory=dict)
     scalar_module: Optional[int] = None
+    hist_size: int = 0
 
     def kernel_sources(self) -> List[str]:
         return [emit_pass(p.spec) for p in self.passes]
@@ -142,6 +145,8 @@ class Planner:
         self.out_dtype = out_dtype
         self.cfg = config or PassConfig()
         self.live = graph.live_nodes(self.wanted)
+        self.hist_mm: Dict[str, int] = {}   # entropy_hist node -> pass of its min/max phase
+        self.hist_base = 0                   # histogram bins allocated so far
 
     def analyse(self) -> None:
         infos: Dict[str, _Info] = {}
@@ -171,11 +176,14 @@ class Planner:
                 raise FusionError(f"operator '{op}' is not known to the fused executor")
             ins = [infos[i] for i in node.input_ids]
             if spec.kind == "reduction":
-                if op == "entropy_hist":
-                    raise FusionError("entropy_hist runs in the batched executor only")
                 if not ins or ins[0].kind in ("scalar", "red"):
                     raise FusionError(f"{op} needs a per-voxel input")
                 p = ins[0].avail
+                if op == "entropy_hist":
+                    # two phases: min/max of the value, then its histogram over [min, max]
+                    self.hist_mm[nid] = p
+                    infos[nid] = _Info("red", p + 2, 1, compute_pass=p + 1)
+                    continue
                 infos[nid] = _Info("red", p + 1, 2 if op == "min_max" else 1, compute_pass=p)
             elif spec.kind == "scan":
                 if int(node.params.get("dim", 0)) != 0:
@@ -210,7 +218,8 @@ class Planner:
         for nid in self.live:
             if infos[nid].kind == "red":
                 self.red_index[nid] = t
-                t += 2 if self.nodes[nid].op_name == "min_max" else 1
+                # min_max: (min, max); entropy_hist: (entropy, min, max)
+                t += {"min_max": 2, "entropy_hist": 3}.get(self.nodes[nid].op_name, 1)
         for nid in self.wanted:
             if infos[nid].kind == "scalar" and self.nodes[nid].op_name != "_constant":
                 scalar_sinks[nid] = t
@@ -226,11 +235,14 @@ class Planner:
                     roots.append(("out", nid))
                 elif inf.kind in ("red", "scan") and inf.compute_pass == p:
                     roots.append((inf.kind, nid))
+                if self.hist_mm.get(nid) == p:
+                    roots.append(("hist_mm", nid))
             if roots:
                 passes.append(self._build_pass(roots))
         scalar_source = self._scalar_source(scalar_sinks) if scalar_sinks else None
         return FusedPlan(key, self.shape, infos, passes, self.table_size, self.const_index, self.red_index,
-                         scalar_sinks, scalar_source, self.wanted, self.out_dtype, list(self.live))
+                         scalar_sinks, scalar_source, self.wanted, self.out_dtype, list(self.live),
+                         hist_size=self.hist_base)
 
     def _build_pass(self, roots: List[Tuple[str, str]]) -> PassPlan:
         pg = PGraph()
@@ -276,6 +288,7 @@ class Planner:
         reductions: List[RedPlan] = []
         nslots = 0
         has_scan = False
+        hists: List[RootSpec] = []
         n_vox = self.shape[0] * self.shape[1] * self.shape[2]
         for kind, nid in roots:
             node = self.nodes[nid]
@@ -292,6 +305,26 @@ class Planner:
                 h = float(node.params.get("dx", 1.0))
                 rspecs.append(RootSpec("scan", pn, out_slot=len(out_nodes), out_dtype="f32", dx=(h, h, h)))
                 out_nodes.append((nid, "scan", nc))
+            elif kind == "hist_mm":
+                pn = lower(node.input_ids[0])
+                nc = pg.nodes[pn].nc
+                rspecs.append(RootSpec("red", pn, red="minmax", slot=nslots))
+                reductions.append(RedPlan(nid, nslots, self.red_index[nid] + 1, N.RED_MIN_MAX,
+                                          float(n_vox * nc), 0, 0.0))
+                nslots += RED_SLOTS["minmax"]
+            elif node.op_name == "entropy_hist":
+                extra = set(node.params) - {"bins", "alloc", "mm"}
+                if extra:
+                    raise FusionError(f"entropy_hist: unexpected parameters {sorted(extra)}")
+                bins = int(node.params.get("bins", 256))
+                if not 1 <= bins <= 4096:
+                    raise FusionError(f"entropy_hist: bins={bins} outside [1, 4096]")
+                pn = lower(node.input_ids[0])
+                r = RootSpec("red", pn, red="hist", slot=self.hist_base, bins=bins,
+                             lohi_index=self.red_index[nid] + 1, table_index=self.red_index[nid])
+                self.hist_base += bins
+                rspecs.append(r)
+                hists.append(r)
             else:
                 op = node.op_name
                 extra = set(node.params) - {"dim", "keepdim", "unbiased", "eps", "dx", "dims", "method",
@@ -345,7 +378,7 @@ class Planner:
             f.staged = f.tma or f.slot in offset_read
         if self.ghosts:
             analyse_ghosts(spec)
-        return PassPlan(spec, field_nodes, out_nodes, reductions)
+        return PassPlan(spec, field_nodes, out_nodes, reductions, hists)
 
     def _scalar_source(self, sinks: Dict[str, int]) -> str:
         """One-thread FP64 kernel for sinks that are expressions of scalars only."""
@@ -440,6 +473,8 @@ def compile_pass(pp: PassPlan, device: int) -> None:
     pp.module = N.load_module(key, cubin, "sten_kernel", smem, device)
     if has_shell(pp.spec):
         pp.shell_module = N.load_module(key + ":shell", cubin, "sten_shell", 0, device)
+    if pp.hists:
+        pp.hist_module = N.load_module(key + ":hist", cubin, "sten_hist_final", 0, device)
     pp.smem, pp.source, pp.key = smem, src, key
 
 
@@ -554,6 +589,14 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
     ops: List[Any] = []
     results: Dict[str, Any] = {}
     produced: Dict[str, torch.Tensor] = {}
+    hist_ptr = 0
+    if plan.hist_size:
+        hist = plan.buffers.get("hist")
+        if hist is None:
+            # zeroed once; the entropy kernel clears the counts after reading them
+            hist = torch.zeros(plan.hist_size, dtype=torch.int64, device=device)
+            plan.buffers["hist"] = hist
+        hist_ptr = hist.data_ptr()
     for pi, pp in enumerate(plan.passes):
         compile_pass(pp, dev_idx)
         spec = pp.spec
@@ -592,13 +635,13 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
             part = torch.zeros(max(need, 1), dtype=torch.float64, device=device)
             plan.buffers[f"part{pi}"] = part
         params = pack_params(spec, dict(fld=fptrs, out=[o.data_ptr() for o in outs], scal=table.data_ptr(),
-                                        part=part.data_ptr(), hist=0, err=err.data_ptr(), n0g=n0, n1=n1,
+                                        part=part.data_ptr(), hist=hist_ptr, err=err.data_ptr(), n0g=n0, n1=n1,
                                         n2=n2, nl=n0, i_base=0, out_lo=0, n_out=n0, seg_len=cfg.seg_len,
                                         tiles_k=tiles_k, cta_off=0), tmaps)
         ops.append(Launch(pp.module, grid, (cfg.threads, 1, 1), pp.smem, params))
         if shell_ctas:
             shell_params = pack_params(spec, dict(fld=fptrs, out=[o.data_ptr() for o in outs],
-                                                  scal=table.data_ptr(), part=part.data_ptr(), hist=0,
+                                                  scal=table.data_ptr(), part=part.data_ptr(), hist=hist_ptr,
                                                   err=err.data_ptr(), n0g=n0, n1=n1, n2=n2, nl=n0, i_base=0,
                                                   out_lo=0, n_out=n0, seg_len=cfg.seg_len, tiles_k=tiles_k,
                                                   cta_off=ncta), tmaps)
@@ -607,6 +650,8 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
             descs = [N.ReduceDesc(r.kind, r.slot, r.table_index, r.unbiased, r.count, r.eps)
                      for r in pp.reductions]
             ops.append(Finalize(part, total_cta, spec.nslots, descs, table))
+        if pp.hists:
+            ops.append(Launch(pp.hist_module, (1, 1, 1), (256, 1, 1), 0, params))
     if plan.scalar_source:
         if plan.scalar_module is None:
             key, cubin = N.compile_cached(plan.scalar_source, NVRTC_OPTS)

@@ -92,6 +92,8 @@ class LazyPipeline:
         self.plan = FC.Planner(graph, self.wanted, out_dtype, config).plan()
         if any(pp.spec.has_scan for pp in self.plan.passes):
             raise FC.FusionError("cumulative_integral is not supported in lazy mode")
+        if self.plan.hist_size:
+            raise FC.FusionError("entropy_hist is not supported in lazy mode")
         self.values = {nid: graph._nodes[nid].params["value"] for nid in self.plan.live
                        if graph._nodes[nid].op_name == "_constant"}
         self.n0, self.n1, self.n2 = self.plan.shape

@@ -8,6 +8,10 @@ reference's benchmark configurations (the reference ships no datasets).
 * ``smoothed_vector``: 3 components, each N(0, 1) smoothed by a 5-point box filter
   (a 5-tap mean along each axis in turn, periodic wrap), stored channels-last
   ``(*shape, 3)`` as the reference's vector layout.
+* ``batch_specs`` / ``batch_fields``: the batched workload — independent fields,
+  each dimension uniform in [lo, hi], a seeded 60/40 FP32/BF16 split, each field
+  with one of eight expressions (field i gets expression i mod 8); the curl
+  expression takes a 3-component field whose components are sinusoid fields.
 
 Generation runs with torch on the requested device (FP64 on the CPU, FP32 on a
 GPU, where 512³ fields would take minutes with numpy); parameters come from
@@ -75,3 +79,33 @@ def smoothed_vector(shape: Sequence[int], seed: int = 2, device="cpu",
         out[..., c] = comp.to(dtype)
         del comp
     return out
+
+
+BATCH_EXPRESSIONS = (
+    "laplacian(f)", "grad_mag(f)", "curl(f)", "f**2 + tanh(f)*exp(f)", "clamp(log(abs(f) + 1), 0, 2)",
+    "trace(hessian(f))", "integrate(f)", "entropy_hist(f, bins=256)",
+)
+
+
+def batch_specs(n: int = 256, seed: int = 0, lo: int = 32, hi: int = 320,
+                bf16_frac: float = 0.4) -> list:
+    """[(expression, storage dtype, shape, field seed)] for ``n`` independent fields."""
+    rng = np.random.default_rng(seed)
+    dims = rng.integers(lo, hi + 1, size=(n, 3))
+    n_bf16 = int(round(bf16_frac * n))
+    is_bf16 = np.zeros(n, dtype=bool)
+    is_bf16[rng.permutation(n)[:n_bf16]] = True
+    out = []
+    for i in range(n):
+        dt = torch.bfloat16 if is_bf16[i] else torch.float32
+        out.append((BATCH_EXPRESSIONS[i % len(BATCH_EXPRESSIONS)], dt, tuple(int(d) for d in dims[i]),
+                    int(seed) * 100003 + i))
+    return out
+
+
+def batch_field(expr: str, dtype: torch.dtype, shape: Sequence[int], seed: int, device="cpu") -> torch.Tensor:
+    """The input field of one batched job (3 components for the curl expression)."""
+    if expr.startswith("curl"):
+        comps = [sinusoid_field(shape, seed=seed * 3 + c, device=device, dtype=torch.float32) for c in range(3)]
+        return torch.stack(comps, dim=-1).to(dtype).contiguous()
+    return sinusoid_field(shape, seed=seed, device=device, dtype=dtype)

@@ -156,3 +156,71 @@ def test_every_tma_x_coordinate_is_16_byte_aligned(dtype, expr, boundary):
                     xs = [(n2 - hk) * f.nc, 0]
                 for x in xs:
                     assert (x * es) % 16 == 0, (kind, x, es, cfg)
+
+
+def test_entropy_hist_plans_minmax_then_histogram():
+    f = torch.zeros(10, 12, 16)
+    g, sink, *_ = S.compile_expression("entropy_hist(f, bins=64)", field_map={"f": f})
+    plan = FC.Planner(g, [sink]).plan()
+    assert len(plan.passes) == 2 and plan.hist_size == 64
+    assert [r.red for r in plan.passes[0].spec.roots] == ["minmax"] and not plan.passes[0].hists
+    h = plan.passes[1].hists
+    assert len(h) == 1 and h[0].bins == 64 and h[0].table_index == plan.red_index[sink]
+    assert h[0].lohi_index == plan.red_index[sink] + 1
+    assert plan.passes[0].reductions[0].table_index == h[0].lohi_index
+
+
+def _batch_jobs_cpu():
+    from stenpy_b200 import batch as B
+    from stenpy_b200.synth import BATCH_EXPRESSIONS
+    jobs = []
+    for e in BATCH_EXPRESSIONS:
+        for dt, shape in ((torch.float32, (20, 24, 64)), (torch.bfloat16, (17, 20, 51))):
+            f = torch.zeros(shape + ((3,) if e.startswith("curl") else ()), dtype=dt)
+            g, sink, *_ = S.compile_expression(e, boundary="periodic", field_map={"f": f})
+            jobs.append(B.BatchJob(g, [sink]))
+    return jobs
+
+
+@pytest.mark.parametrize("threads", [128, 256])
+def test_batch_module_compiles_for_sm100a(threads):
+    from stenpy_b200 import batch as B
+    from stenpy_b200.codegen import emit_batch_module
+    jobs = _batch_jobs_cpu()
+    cfg = B.batch_candidates(threads)[0]
+    specs, seen = [], set()
+    for j in jobs:
+        for pp in B.plan_job(j, cfg).passes:
+            k = B.program_key(pp.spec)
+            if k not in seen:
+                seen.add(k)
+                specs.append(pp.spec)
+    assert len(specs) >= 16          # 8 expressions x 2 dtypes (+ the entropy min/max passes)
+    key, cubin = N.compile_cached(emit_batch_module(specs, threads), FC.NVRTC_OPTS)
+    assert len(cubin) > 10000
+    # job outputs follow the storage dtype of the job's field
+    assert {j.out_dtype for j in jobs} == {torch.float32, torch.bfloat16}
+
+
+def test_batch_queue_orders_prerequisites_first():
+    from stenpy_b200.batch import _Phase, build_queue
+    # job 0: one pass; job 1: min/max pass then a dependent histogram pass; job 2 larger
+    ph = [_Phase(0, 0, 0, 4, 2, 1, 9, 1, -1, 100.0),
+          _Phase(1, 0, 1, 2, 1, 0, 2, 2, -1, 50.0),
+          _Phase(1, 1, 2, 2, 1, 0, 2, 1, 1, 50.0),
+          _Phase(2, 0, 0, 3, 3, 2, 11, 1, -1, 900.0)]
+    items = build_queue(ph)
+    quads = [tuple(items[i:i + 4]) for i in range(0, len(items), 4)]
+    assert len(quads) == sum(p.ncta for p in ph)
+    order = [q[0] for q in quads]
+    # the pass with a dependent comes first, the dependent pass last, larger jobs before smaller
+    assert order[0] == 1 and order[-1] == 2
+    assert order.index(3) < order.index(0)
+    assert max(i for i, p in enumerate(order) if p == 1) < min(i for i, p in enumerate(order) if p == 2)
+    # every tile of every pass appears exactly once, shell blocks after the pass's tiles
+    for pi, p in enumerate(ph):
+        tiles = [(q[2], q[3]) for q in quads if q[0] == pi and q[1] == 0]
+        assert sorted(tiles) == sorted((bx, by) for by in range(p.nseg) for bx in range(p.gdx))
+        assert sum(1 for q in quads if q[0] == pi and q[1] == 1) == p.shell_items
+    with pytest.raises(ValueError):
+        build_queue([_Phase(0, 0, 0, 1, 1, 0, 1, 1, 0, 1.0)])

@@ -1,0 +1,66 @@
+"""Cost-model MLP kernels: the library's forward / backward / Adam kernels against
+a CPU FP64 reference (torch autograd on the same parameters and data)."""
+import math
+
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def _reference(params, X, y, din, h):
+    """Same network in float64 with autograd: loss and d loss / d params."""
+    p = params.double().clone().requires_grad_(True)
+    o = 0
+    W1 = p[o:o + din * h].view(din, h); o += din * h
+    b1 = p[o:o + h]; o += h
+    W2 = p[o:o + h * h].view(h, h); o += h * h
+    b2 = p[o:o + h]; o += h
+    w3 = p[o:o + h]; o += h
+    b3 = p[o]
+    a1 = torch.relu(X.double() @ W1 + b1)
+    a2 = torch.relu(a1 @ W2 + b2)
+    pred = a2 @ w3 + b3
+    loss = ((pred - y.double()) ** 2).mean()
+    loss.backward()
+    return pred.detach(), float(loss), p.grad
+
+
+@pytest.mark.parametrize("n,din", [(37, 11), (256, 31)])
+def test_mlp_forward_and_gradient_match_fp64_autograd(n, din):
+    from stenpy_b200 import costmodel as CM
+    dev = _dev()
+    torch.manual_seed(n)
+    m = CM.CostModel(din, dev, seed=n)
+    X = torch.randn(n, din)
+    y = torch.randn(n)
+    pred_ref, loss_ref, grad_ref = _reference(m.params.cpu(), X, y, din, m.hidden)
+    Xd, yd = X.to(dev).contiguous(), y.to(dev).contiguous()
+    loss, grad = m.loss_grad(Xd, yd)
+    assert abs(float(loss) - loss_ref) <= 1e-4 * max(1.0, loss_ref)
+    g = grad.cpu().double()
+    rel = (g - grad_ref).abs().max().item() / grad_ref.abs().max().item()
+    assert rel <= 1e-4, rel
+    m.mu, m.sd, m.y_mu = torch.zeros(din), torch.ones(din), 0.0
+    p = m.predict(X)
+    assert (p - pred_ref).abs().max().item() <= 1e-4 * max(1.0, pred_ref.abs().max().item())
+
+
+def test_adam_training_fits_a_smooth_function():
+    """A few hundred Adam steps with the library's kernels fit y = sum(sin(x))."""
+    from stenpy_b200 import costmodel as CM
+    dev = _dev()
+    torch.manual_seed(0)
+    X = torch.rand(2048, 8) * 2 - 1
+    y = torch.sin(2 * X).sum(1)
+    m = CM.CostModel(8, dev, seed=1)
+    hist = m.fit(X, y, steps=800, batch=256, lr=3e-3)
+    var = float(y.var())
+    assert hist[-1] < 0.1 * var, (hist[0], hist[-1], var)
+    assert math.isfinite(hist[-1])

@@ -148,9 +148,10 @@ def make_fields(size, device):
     return f, u
 
 
-def build(form, f, u, device, tune=True):
+def build(form, f, u, device, tune=True, schedule=None):
     """Plan the step for one storage form; with ``tune`` every pass gets the schedule
-    the autotuner measured fastest (exhaustive over its candidates, cached)."""
+    the autotuner measured fastest (exhaustive over its candidates, cached); a fixed
+    ``schedule`` (PassConfig) applies to every pass instead."""
     import stenpy_b200 as S
     from stenpy_b200 import autotune as AT
     from stenpy_b200 import fused_compiler as FC
@@ -158,7 +159,9 @@ def build(form, f, u, device, tune=True):
     g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
                                        field_map={"f": f.to(dt), "u": u.to(dt)})
     wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
-    plan = FC.get_plan(g, wanted, out_dtype=dt)
+    if schedule is not None:
+        tune = False
+    plan = FC.get_plan(g, wanted, out_dtype=dt, config=schedule)
     values, back = FC.bind(plan, g, wanted)
     tuned = AT.tune_plan(plan, values, device, tag=f"bench-{form}") if tune else []
     prog = FC.build_program(plan, values, device)
@@ -638,6 +641,8 @@ def main():
     ap.add_argument("--batch-lo", type=int, default=32)
     ap.add_argument("--batch-hi", type=int, default=320)
     ap.add_argument("--tune-log", default="")
+    ap.add_argument("--schedule", default="", help="JSON PassConfig for every pass (no autotuning), "
+                                                    "e.g. '{\"tj\": 16, \"tk\": 32, \"seg_len\": 32}'")
     ap.add_argument("--dags", type=int, default=300)
     ap.add_argument("--heldout", type=int, default=60)
     ap.add_argument("--train-cands", type=int, default=6)
@@ -664,6 +669,10 @@ def main():
     torch.cuda.set_device(dev)
     from stenpy_b200 import fused_compiler as FC
     forms = [x for x in args.forms.split(",") if x]
+    schedule = None
+    if args.schedule:
+        from stenpy_b200.codegen import PassConfig
+        schedule = PassConfig(**json.loads(args.schedule))
     f, u = make_fields(args.size, dev)
     n_vox = args.size ** 3
     stream = torch.cuda.Stream(dev)
@@ -671,7 +680,7 @@ def main():
     results = {}
     clocks = None
     for form in forms:
-        g, wanted, plan, prog, tuned = build(form, f, u, dev, tune=not args.no_tune)
+        g, wanted, plan, prog, tuned = build(form, f, u, dev, tune=not args.no_tune, schedule=schedule)
         with torch.cuda.stream(stream):
             FC.enqueue(prog, stream)
         torch.cuda.synchronize()

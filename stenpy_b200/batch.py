@@ -176,6 +176,27 @@ def build_queue(phases: Sequence[_Phase]) -> List[int]:
     return items
 
 
+def check_queue(items: torch.Tensor, phases: Sequence[_Phase]) -> None:
+    """Every item names an existing pass and a tile / shell block inside it, each
+    exactly once (the kernel trusts these indices)."""
+    if items.ndim != 2 or items.shape[1] != 4:
+        raise ValueError("work items must be (n, 4)")
+    ph = items[:, 0].long()
+    if len(phases) == 0 or int(ph.min()) < 0 or int(ph.max()) >= len(phases):
+        raise ValueError("work item names a missing pass")
+    gdx = torch.tensor([p.gdx for p in phases])[ph]
+    nseg = torch.tensor([p.nseg for p in phases])[ph]
+    nsh = torch.tensor([p.shell_items for p in phases])[ph]
+    kind, bx, by = items[:, 1].long(), items[:, 2].long(), items[:, 3].long()
+    tile_ok = (kind == 0) & (bx >= 0) & (bx < gdx) & (by >= 0) & (by < nseg)
+    shell_ok = (kind == 1) & (bx >= 0) & (bx < nsh) & (by == 0)
+    if not bool((tile_ok | shell_ok).all()):
+        raise ValueError("work item outside its pass")
+    if items.shape[0] != sum(p.ncta for p in phases) or \
+            torch.unique(items, dim=0).shape[0] != items.shape[0]:
+        raise ValueError("work items must cover every tile and shell block exactly once")
+
+
 class BatchProgram:
     """A batch resolved against its tensors: per-job plans, the work queue, scalar
     tables, partial rows, histograms and outputs, and the packed kernel arguments.
@@ -295,9 +316,10 @@ class BatchProgram:
         self.phase_buf = torch.frombuffer(bytearray(prec), dtype=torch.uint8).to(dev)
         self.red_buf = torch.frombuffer(bytearray(b"".join(red_recs) or bytes(32)), dtype=torch.uint8).to(dev)
         self.hist_buf = torch.frombuffer(bytearray(b"".join(hist_recs) or bytes(24)), dtype=torch.uint8).to(dev)
-        items = build_queue(self.phases)
-        self.n_items = len(items)
-        self.items = torch.tensor(items, dtype=torch.int32).reshape(-1, 4).to(dev)
+        items = torch.tensor(build_queue(self.phases), dtype=torch.int32).reshape(-1, 4)
+        check_queue(items, self.phases)
+        self.n_items = int(items.shape[0])
+        self.items = items.to(dev)
         self.ctl = torch.zeros(2 + 2 * len(phases), dtype=torch.int32, device=dev)
         self.n_ctas = max(1, min(self.n_items, module.sm_count * module.blocks_per_sm))
         self.args = struct.pack(ARGS_FMT, self.items.data_ptr(), self.phase_buf.data_ptr(), self.red_buf.data_ptr(),

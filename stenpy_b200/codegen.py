@@ -1468,6 +1468,7 @@ __device__ __noinline__ void sten_batch_finalize(const BatchArgs& a, const BPhas
          "    const int it = s_item;",
          "    if (it >= a.n_items) break;",
          "    const int4 w = a.items[it];",
+         "    if ((unsigned)w.x >= (unsigned)a.n_phases) { ok = false; break; }  // corrupt queue: stop",
          "    const BPhase& ph = a.phases[w.x];",
          "    if (ph.dep >= 0) {",
          "      bool got = true;",

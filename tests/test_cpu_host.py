@@ -224,3 +224,17 @@ def test_batch_queue_orders_prerequisites_first():
         assert sum(1 for q in quads if q[0] == pi and q[1] == 1) == p.shell_items
     with pytest.raises(ValueError):
         build_queue([_Phase(0, 0, 0, 1, 1, 0, 1, 1, 0, 1.0)])
+
+
+def test_batch_queue_check_rejects_bad_items():
+    from stenpy_b200.batch import _Phase, build_queue, check_queue
+    ph = [_Phase(0, 0, 0, 3, 2, 1, 7, 1, -1, 10.0), _Phase(1, 0, 1, 2, 1, 0, 2, 1, 0, 5.0)]
+    items = torch.tensor(build_queue(ph), dtype=torch.int32).reshape(-1, 4)
+    check_queue(items, ph)
+    assert items.shape[0] == sum(p.ncta for p in ph)
+    for bad in (items[:-1], torch.cat([items, items[:1]]),
+                torch.cat([items[:-1], torch.tensor([[2, 0, 0, 0]], dtype=torch.int32)]),
+                torch.cat([items[:-1], torch.tensor([[0, 0, 3, 0]], dtype=torch.int32)]),
+                torch.cat([items[:-1], torch.tensor([[0, 1, 0, 1]], dtype=torch.int32)])):
+        with pytest.raises(ValueError):
+            check_queue(bad, ph)

@@ -28,7 +28,7 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, plane_bytes, shell_count,
+from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, plane_bytes, shell_count, valid_shape,
                       shell_regions, smem_layout, with_config)
 
 LOG_PATH = os.environ.get("STENPY_TUNE_LOG", os.path.join(os.path.dirname(os.path.abspath(__file__)),
@@ -44,7 +44,7 @@ _GHOST = (True, False)
 
 
 def _valid(spec: PassSpec, cfg: PassConfig) -> bool:
-    if cfg.threads % cfg.tk or cfg.tk % 32 or (cfg.tj * cfg.tk) % cfg.threads:
+    if not valid_shape(cfg):
         return False
     trial = with_config(spec, cfg)
     for f in spec.fields:

@@ -116,6 +116,7 @@ class PassConfig:
     seg_len: int = 64
     min_blocks: int = 1
     ghost: bool = True   # evaluate dim-1/dim-2 faces in the z-march (else in the shell kernel)
+    kv: int = 1          # k-adjacent voxels per thread (one vector chunk per row in shared memory)
 
 
 @dataclass
@@ -205,6 +206,18 @@ def analyse_ghosts(spec: "PassSpec") -> None:
     for f in spec.fields:
         f.wrap_k = f.tma and f.halo > 0 and rules.get((f.slot, 2)) == "periodic"
         f.wrap_j = f.tma and f.halo > 0 and rules.get((f.slot, 1)) == "periodic"
+
+
+def valid_shape(cfg: "PassConfig") -> bool:
+    """Thread mapping: TK/KV threads along k (each KV adjacent voxels), the block's
+    other threads along j, VPT = TJ / (threads / (TK/KV)) rows each."""
+    if cfg.kv not in (1, 2, 4) or cfg.tk % 32 or cfg.tk % cfg.kv or cfg.prefetch < 1:
+        return False
+    tkt = cfg.tk // cfg.kv
+    if cfg.threads % tkt:
+        return False
+    rows = cfg.threads // tkt
+    return cfg.tj % rows == 0 and cfg.tj // rows >= 1
 
 
 def with_config(spec: "PassSpec", cfg: "PassConfig") -> "PassSpec":
@@ -349,11 +362,9 @@ class _Emitter:
     def field_fast(self, n: PNode, di, dj, dk, arr, body):
         f = self.s.fields[n.a("field")]
         if f.staged:
-            w = self.s.box(f)[0]
             for c in range(n.nc):
-                body.append(f"{arr}[{c}] = ld_as_f32((const {CTYPE[f.dtype]}*)sten_smem + x.so{f.slot}[({di}) + {self.R}] + x.o{f.slot}"
-                            f" + ({dj}) * {w} + ({dk}) * {f.nc} + {c});")
-        elif di != "0" or dj != "0" or dk != "0":
+                body.append(f"{arr}[{c}] = LDF{f.slot}<{di}, {dj}, ({dk}) * {f.nc} + {c}>(x);")
+        elif di != "0" or dj not in ("0", "M") or dk not in ("0", "KK"):
             raise AssertionError("unstaged field read at an offset")
         else:
             for c in range(n.nc):
@@ -586,7 +597,7 @@ class _Emitter:
             if n.op in ("d1", "lap") or n.op == "field" or n.op == "scalar":
                 arr = self.t()
                 body.append(f"float {arr}[{n.nc}];")
-                self.fast_value(n, "0", "0", "0", arr, body)
+                self.fast_value(n, "0", "M", "KK", arr, body)
             else:
                 ins = [point(i) for i in n.ins]
                 arr = self.t()
@@ -599,7 +610,7 @@ class _Emitter:
             arr = point(r.node)
             for c in range(self.g.nodes[r.node].nc):
                 body.append(f"rv[{off + c}] = {arr}[{c}];")
-        self.lines.append("__device__ __forceinline__ void eval_fast(const FCtx& x, float* rv) {")
+        self.lines.append("template <int M, int KK> __device__ __forceinline__ void eval_fast(const FCtx& x, float* rv) {")
         self.lines += ["  " + b for b in body]
         self.lines.append("}")
         # slow
@@ -753,14 +764,17 @@ __device__ __forceinline__ double sten_simpson_w(int idx, int n, double h, int s
 """
 
 
-def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
+def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootSpec] = (),
+              where: str = "main", m: int = 0, kk: int = 0) -> List[str]:
     """Per-voxel root handling (stores, reduction accumulation, scans). Expects
     ``rv`` (root values), ``vox`` (linear voxel index), ``gi, j, k`` and, for scans,
-    the register slot ``m``."""
+    the register slot ``mq``. Roots in ``skip`` are stored by the caller."""
     K: List[str] = []
     ri = si = 0
     for r, off in zip(spec.roots, e.offsets):  # noqa: C901
         nc = e.g.nodes[r.node].nc
+        if any(r is x for x in skip):
+            continue
         if r.kind == "out":
             ct = CTYPE[r.out_dtype]
             K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
@@ -773,7 +787,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
             half = repr(0.5 * float(r.dx[0]))
             K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
             for c in range(nc):
-                q = f"m * {nc} + {c}"
+                q = f"mq * {nc} + {c}"
                 K.append(f"  if (gi > 0) sc{si}_acc[{q}] += ((double)sc{si}_prev[{q}] + (double)rv[{off + c}]) * {half};")
                 K.append(f"  sc{si}_prev[{q}] = rv[{off + c}];")
                 K.append(f"  st_from_f64(o_ + {c}, sc{si}_acc[{q}]);")
@@ -804,18 +818,26 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool) -> List[str]:
                     K.append(f"{{ const double t_ = {val}; rv{ri_here}_a = fmin(rv{ri_here}_a, t_); rv{ri_here}_b = fmax(rv{ri_here}_b, t_); }}")
                 elif r.red == "hist":
                     # bin index as the oracle forms it: floor((x - lo) / (hi - lo) * bins), FP64
-                    K.append(f"if (rv{ri_here}_hh > rv{ri_here}_hl) {{ const double t_ = ({val} - rv{ri_here}_hl)"
-                             f" / (rv{ri_here}_hh - rv{ri_here}_hl) * {float(r.bins)!r}; int b_ = (int)floor(t_);"
+                    # (the product with a precomputed bins/(hi-lo) rounds differently from the
+                    # quotient only within a few ulps; near a bin edge the quotient is formed)
+                    K.append(f"if (rv{ri_here}_hh > rv{ri_here}_hl) {{ const double d_ = {val} - rv{ri_here}_hl;"
+                             f" double t_ = d_ * rv{ri_here}_hinv;"
+                             f" if (fabs(t_ - rint(t_)) <= 1e-9) t_ = d_ / (rv{ri_here}_hh - rv{ri_here}_hl) * {float(r.bins)!r};"
+                             f" int b_ = (int)floor(t_);"
                              f" b_ = b_ < 0 ? 0 : (b_ > {r.bins - 1} ? {r.bins - 1} : b_); sten_hist_add(rv{ri_here}_hs, b_); }}")
                 elif r.red == "integrate":
                     sm = 1 if r.method == "simpson" else 0
-                    K.append(f"rv{ri_here}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
-                             f" * sten_simpson_w(j, p.n1, {r.dx[1]!r}, {sm}) * sten_simpson_w(k, p.n2, {r.dx[2]!r}, {sm});")
+                    if where == "main":
+                        # per-plane and per-column weights computed outside the voxel loop
+                        K.append(f"rv{ri_here}_a += {val} * rv{ri_here}_wi * rv{ri_here}_wj[{{M}}] * rv{ri_here}_wk[{{KK}}];")
+                    else:
+                        K.append(f"rv{ri_here}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
+                                 f" * sten_simpson_w(j, p.n1, {r.dx[1]!r}, {sm}) * sten_simpson_w(k, p.n2, {r.dx[2]!r}, {sm});")
                 else:
                     raise NotImplementedError(r.red)
         else:
             raise NotImplementedError(r.kind)
-    return K
+    return [k.replace("{M}", str(m)).replace("{KK}", str(kk)) for k in K]
 
 
 def hist_offsets(spec: PassSpec, red_off: int) -> Tuple[Dict[int, int], int]:
@@ -837,6 +859,7 @@ def _red_decls(spec: PassSpec, where: str = "main") -> List[str]:
         if r.red == "hist":
             K.append(f"const double rv{ri}_hl = __ldcg(p.scal + {r.lohi_index}), "
                      f"rv{ri}_hh = __ldcg(p.scal + {r.lohi_index + 1});")
+            K.append(f"const double rv{ri}_hinv = rv{ri}_hh > rv{ri}_hl ? {float(r.bins)!r} / (rv{ri}_hh - rv{ri}_hl) : 0.0;")
             if where == "main":
                 K.append(f"unsigned int* rv{ri}_hs = (unsigned int*)(smem + {hoffs[ri]});")
                 K.append(f"for (int b_ = tid; b_ < {r.bins}; b_ += NT) rv{ri}_hs[b_] = 0u;")
@@ -1034,8 +1057,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     split = R > 0 and not spec.has_scan          # main kernel never takes the slow path
     nslot = 2 * R + 1 + cfg.prefetch
     assert nslot <= 16, "too many ring slots"
-    assert cfg.tk % 32 == 0 and (cfg.tj * cfg.tk) % cfg.threads == 0 and cfg.prefetch >= 1
-    vpt = cfg.tj * cfg.tk // cfg.threads
+    assert valid_shape(cfg), f"invalid tile shape {cfg}"
+    vpt = cfg.tj * cfg.tk // (cfg.threads * cfg.kv)
     L = e.lines
     if batch:
         assert cfg.threads == batch_threads, "batch programs share the block size"
@@ -1043,7 +1066,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     else:
         L.append(header)
     L.append(f"#define TJ {cfg.tj}\n#define TK {cfg.tk}\n#define NT {cfg.threads}\n#define RAD {R}"
-             f"\n#define NSLOT {nslot}\n#define VPT {vpt}\n#define NSLOTS_RED {max(spec.nslots, 1)}")
+             f"\n#define NSLOT {nslot}\n#define VPT {vpt}\n#define NSLOTS_RED {max(spec.nslots, 1)}"
+             f"\n#define KV {cfg.kv}\n#define TKT {cfg.tk // cfg.kv}")
     if batch:
         L.append(f"namespace {batch_ns} {{")
     ntma = len(tmap_specs(spec))
@@ -1089,11 +1113,27 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     for f in spec.fields:
         ct = CTYPE[f.dtype]
         if f.staged:
-            L.append(f"  unsigned int so{f.slot}[2 * RAD + 1]; unsigned int o{f.slot};")
+            # byte offset of this thread's chunk (row 0, first k) in each ring slot in use
+            L.append(f"  unsigned int sb{f.slot}[2 * RAD + 1];")
         else:
             L.append(f"  const {ct}* gp{f.slot};")
     L.append(f"  float sc[{max(spec.n_scalars, 1)}];")
     L.append("};")
+    for f in spec.fields:
+        if not f.staged:
+            continue
+        ct, es = CTYPE[f.dtype], ESIZE[f.dtype]
+        cw = cfg.kv * f.nc * es
+        chunk = es in (2, 4) and cw % 4 == 0
+        L.append(f"template <int DI, int DJ, int E> __device__ __forceinline__ float LDF{f.slot}(const FCtx& x) {{")
+        L.append(f"  // element E of row DJ (relative to the thread's chunk) in the plane at offset DI")
+        L.append(f"  const unsigned char* row_ = sten_smem + x.sb{f.slot}[DI + RAD] + DJ * {spec.box(f)[0] * es};")
+        if chunk:
+            L.append(f"  if constexpr (E >= 0 && E < {cfg.kv * f.nc}) return chunk_elem<{ct}, {cw}, E * {es}>(row_);")
+            L.append(f"  else return ld_as_f32((const {ct}*)row_ + E);")
+        else:
+            L.append(f"  return ld_as_f32((const {ct}*)row_ + E);")
+        L.append("}")
     e.emit_fast_fns()
     e.emit_slow_fns()
     e.emit_eval()
@@ -1133,8 +1173,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  __syncthreads();  // histogram cleared")
     for si, r in enumerate(scans):
         nc = e.g.nodes[r.node].nc
-        K.append(f"  double sc{si}_acc[VPT * {nc}]; float sc{si}_prev[VPT * {nc}];")
-        K.append(f"  #pragma unroll\n  for (int q = 0; q < VPT * {nc}; ++q) {{ sc{si}_acc[q] = 0.0; sc{si}_prev[q] = 0.0f; }}")
+        K.append(f"  double sc{si}_acc[VPT * KV * {nc}]; float sc{si}_prev[VPT * KV * {nc}];")
+        K.append(f"  #pragma unroll\n  for (int q = 0; q < VPT * KV * {nc}; ++q) {{ sc{si}_acc[q] = 0.0; sc{si}_prev[q] = 0.0f; }}")
     staged = tma_fields or lsu_fields
     tmaps = tmap_specs(spec)
     tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
@@ -1192,9 +1232,26 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             ct = CTYPE[f.dtype]
             rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
             rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
+            hk = spec.hk(f)
+            et = -(-(w * h) // cfg.threads)
             K.append("    {")
             K.append(f"      {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
             K.append(f"      const {ct}* src = (const {ct}*)p.fld[{f.slot}];")
+            # tile box inside the field: plain row-offset loads, issued in groups of 8
+            # before their shared-memory stores (one memory latency per group)
+            K.append(f"      if (zq >= 0 && zq < p.nl && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && "
+                     f"tk0 >= {hk} && tk0 + TK + {hk} <= p.n2) {{")
+            K.append(f"        const {ct}* rowp = src + (((size_t)zq * p.n1 + (tj0 - {f.halo})) * p.n2 + (tk0 - {hk})) * {f.nc};")
+            K.append(f"        const int pitch = p.n2 * {f.nc};")
+            for g0 in range(0, et, 8):
+                g1 = min(et, g0 + 8)
+                K.append(f"        {{ {ct} v_[{g1 - g0}];")
+                K.append(f"          #pragma unroll\n          for (int t = 0; t < {g1 - g0}; ++t) {{ const int e = tid + (t + {g0}) * NT;"
+                         f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (size_t)yy * pitch + (e - yy * {w})); }} }}")
+                K.append(f"          #pragma unroll\n          for (int t = 0; t < {g1 - g0}; ++t) {{ const int e = tid + (t + {g0}) * NT;"
+                         f" if (e < {w * h}) dst[e] = v_[t]; }}")
+                K.append("        }")
+            K.append("      } else")
             K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
             K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
             K.append(f"        int jg = tj0 - {f.halo} + yy;")
@@ -1231,27 +1288,38 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  if (edge_cta) { for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) ghost_fill(q); }")
     if staged:
         K.append("  __syncthreads();")
-    # each thread owns column tk of the tile and VPT consecutive rows; everything that
-    # does not depend on the plane is computed once, before the march
-    K.append("  const int tk = tid % TK, tjb = (tid / TK) * VPT;")
-    K.append("  const int k = tk0 + tk;")
+    # each thread owns KV adjacent columns (kt0 ..) of the tile and VPT consecutive rows;
+    # everything that does not depend on the plane is computed once, before the march
+    kvn = cfg.kv
+    K.append("  const int tk = (tid % TKT) * KV, tjb = (tid / TKT) * VPT;")
+    K.append("  const int kt0 = tk0 + tk;")
+    K.append("  bool k_ok[KV];")
+    K.append("  #pragma unroll")
     if split and not ghost:
-        K.append("  const bool k_ok = k >= RAD && k < p.n2 - RAD;")
+        K.append("  for (int q = 0; q < KV; ++q) k_ok[q] = kt0 + q >= RAD && kt0 + q < p.n2 - RAD;")
     else:
-        K.append("  const bool k_ok = k < p.n2;")
+        K.append("  for (int q = 0; q < KV; ++q) k_ok[q] = kt0 + q < p.n2;")
+    K.append("  const bool k_all = " + " && ".join(f"k_ok[{q}]" for q in range(kvn)) + ";")
     K.append("  bool m_ok[VPT];")
     K.append("  #pragma unroll")
     K.append("  for (int m = 0; m < VPT; ++m) {")
     K.append("    const int j = tj0 + tjb + m;")
     if split and not ghost:
-        K.append("    m_ok[m] = k_ok && j >= RAD && j < p.n1 - RAD;")
+        K.append("    m_ok[m] = j >= RAD && j < p.n1 - RAD;")
     else:
-        K.append("    m_ok[m] = k_ok && j < p.n1;")
+        K.append("    m_ok[m] = j < p.n1;")
     K.append("  }")
     for f in spec.fields:
         if f.staged:
-            K.append(f"  const unsigned int ob{f.slot} = (tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc};")
-    K.append("  const size_t col = (size_t)(tj0 + tjb) * p.n2 + k;")
+            K.append(f"  const unsigned int ob{f.slot} = ((tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc})"
+                     f" * {ESIZE[f.dtype]};")
+    for ri, r in enumerate(reds):
+        if r.red == "integrate":
+            sm = 1 if r.method == "simpson" else 0
+            K.append(f"  double rv{ri}_wj[VPT], rv{ri}_wk[KV];")
+            K.append(f"  #pragma unroll\n  for (int m = 0; m < VPT; ++m) rv{ri}_wj[m] = sten_simpson_w(tj0 + tjb + m, p.n1, {r.dx[1]!r}, {sm});")
+            K.append(f"  #pragma unroll\n  for (int q = 0; q < KV; ++q) rv{ri}_wk[q] = sten_simpson_w(kt0 + q, p.n2, {r.dx[2]!r}, {sm});")
+    K.append("  const size_t col = (size_t)(tj0 + tjb) * p.n2 + kt0;")
     K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
     K.append("  const size_t out_base = (size_t)p.out_lo * plane_n;")
     K.append("  int sb = 0;  // ring slot of plane i - RAD, rotated each plane")
@@ -1262,35 +1330,55 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     K.append("    for (int d = 0; d < 2 * RAD + 1; ++d) { const int t_ = sb + d; sslot[d] = t_ >= NSLOT ? t_ - NSLOT : t_; }")
     for f in spec.fields:
         if f.staged:
-            ct = CTYPE[f.dtype]
             K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD + 1; ++d) "
-                     f"x.so{f.slot}[d] = ({rings[f.slot]}u + (unsigned)sslot[d] * {plane_bytes(spec, f)}u) / {ESIZE[f.dtype]}u;")
+                     f"x.sb{f.slot}[d] = {rings[f.slot]}u + (unsigned)sslot[d] * {plane_bytes(spec, f)}u + ob{f.slot};")
     if ghost and spec.i_periodic:
         K.append("    const bool i_in = true;")
     else:
         K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
     K.append("    const size_t pbase = (size_t)i * plane_n + col;")
+    for ri, r in enumerate(reds):
+        if r.red == "integrate":
+            sm = 1 if r.method == "simpson" else 0
+            K.append(f"    const double rv{ri}_wi = sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm});")
     if split:
         K.append("    if (i_in) {")
-    K.append("    #pragma unroll")
-    K.append("    for (int m = 0; m < VPT; ++m) {")
-    K.append("      if (!m_ok[m]) continue;")
-    K.append("      const int j = tj0 + tjb + m;")
-    K.append("      const size_t vox = pbase + (size_t)m * p.n2;")
-    for f in spec.fields:
-        if f.staged:
-            K.append(f"      x.o{f.slot} = ob{f.slot} + m * {spec.box(f)[0]}u;")
-        else:
-            ct = CTYPE[f.dtype]
-            K.append(f"      x.gp{f.slot} = (const {ct}*)p.fld[{f.slot}] + vox * {f.nc};")
-    K.append(f"      float rv[{nroot}];")
-    if split or R == 0:
-        K.append("      eval_fast(x, rv);")
-    else:
-        K.append("      const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-        K.append("      if (inter) eval_fast(x, rv); else eval_slow(pg, gi, j, k, rv);")
-    K += ["      " + k for k in _epilogue(spec, e, scan_ok=True)]
-    K.append("    }")
+    # KV-wide stores for single-component outputs
+    vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1 and kvn > 1
+                and r.out_dtype in ("f32", "f16", "bf16")]
+    for m in range(vpt):
+        K.append(f"    if (m_ok[{m}]) {{")
+        K.append(f"      const int j = tj0 + tjb + {m};")
+        K.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
+        K.append(f"      float rvk[KV][{nroot}];")
+        for kk in range(kvn):
+            K.append(f"      if (k_ok[{kk}]) {{")
+            K.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
+            K.append(f"        const size_t vox = rowvox + {kk};")
+            K.append(f"        float* rv = rvk[{kk}];")
+            for f in spec.fields:
+                if not f.staged:
+                    ct = CTYPE[f.dtype]
+                    K.append(f"        x.gp{f.slot} = (const {ct}*)p.fld[{f.slot}] + vox * {f.nc};")
+            if split or R == 0:
+                K.append(f"        eval_fast<{m}, {kk}>(x, rv);")
+            else:
+                K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
+                K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
+            K += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk)]
+            K.append("      }")
+        for r in vec_outs:
+            ct = CTYPE[r.out_dtype]
+            off = e.offsets[spec.roots.index(r)]
+            vals = ", ".join(f"rvk[{q}][{off}]" for q in range(kvn))
+            K.append(f"      {{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (rowvox - out_base);")
+            K.append(f"        if (k_all && ((rowvox - out_base) & (KV - 1)) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
+            K.append("        else {")
+            for q in range(kvn):
+                K.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, rvk[{q}][{off}]);")
+            K.append("        }")
+            K.append("      }")
+        K.append("    }")
     if split:
         K.append("    }")
     # the next plane (i+1+RAD) must be resident and ghosted before the barrier
@@ -1302,8 +1390,10 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         if ghost and staged:
             K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
         K.append("    }")
-    K.append("    ok = __syncthreads_and(ok);")
-    K.append("    if (!ok) break;")
+    if staged:
+        # the ring slot of plane i - RAD is refilled next: every thread must be done with it
+        K.append("    ok = __syncthreads_and(ok);")
+        K.append("    if (!ok) break;")
     K.append("    sb = (sb + 1 == NSLOT) ? 0 : sb + 1;")
     if staged:
         K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
@@ -1368,7 +1458,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("    const size_t out_base = (size_t)p.out_lo * p.n1 * p.n2;")
         K.append(f"    float rv[{nroot}];")
         K.append("    eval_slow(pg, gi, (int)j, (int)k, rv);")
-        K += ["    " + k for k in _epilogue(spec, e, scan_ok=False)]
+        K += ["    " + k for k in _epilogue(spec, e, scan_ok=False, where="shell")]
         K.append("  }")
         K += ["  " + k for k in _red_flush(spec, "p.cta_off + bx", "shell")]
         K.append("}")
@@ -1392,7 +1482,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  return run_tile(p, pg, bx, by, gdx);")
         K.append("}")
         K.append(f"}}  // namespace {batch_ns}")
-        K.append("#undef TJ\n#undef TK\n#undef NT\n#undef RAD\n#undef NSLOT\n#undef VPT\n#undef NSLOTS_RED")
+        K.append("#undef TJ\n#undef TK\n#undef NT\n#undef RAD\n#undef NSLOT\n#undef VPT\n#undef NSLOTS_RED"
+                 "\n#undef KV\n#undef TKT")
     return "\n".join(L) + "\n" + "\n".join(K) + "\n"
 
 

@@ -39,6 +39,11 @@ STEN_DEV float ldg_as_f32(const bf16_t* p) {
 STEN_DEV float ldg_as_f32(const f16_t* p) {
   u16 b = __ldg((const u16*)p); float f; asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(b)); return f;
 }
+// raw element loads through the read-only path (no conversion)
+STEN_DEV float ldg_raw(const float* p) { return __ldg(p); }
+STEN_DEV double ldg_raw(const double* p) { return __ldg(p); }
+STEN_DEV bf16_t ldg_raw(const bf16_t* p) { bf16_t v; v.bits = __ldg((const u16*)p); return v; }
+STEN_DEV f16_t ldg_raw(const f16_t* p) { f16_t v; v.bits = __ldg((const u16*)p); return v; }
 STEN_DEV void st_from_f32(float* p, float v) { *p = v; }
 STEN_DEV void st_from_f32(double* p, float v) { *p = (double)v; }
 STEN_DEV void st_from_f32(bf16_t* p, float v) {
@@ -53,6 +58,53 @@ STEN_DEV void st_from_f64(bf16_t* p, double v) { st_from_f32(p, (float)v); }
 STEN_DEV void st_from_f64(f16_t* p, double v) { st_from_f32(p, (float)v); }
 
 // ------------------------------------------------------------------ math helpers
+// ------------------------------------------------------------------ k-vector chunks
+// A thread's KV k-adjacent voxels of one row are one contiguous chunk of CW bytes in
+// shared memory, aligned to 16 (CW % 16 == 0), 8 (CW % 8 == 0) or 4 bytes. Element
+// loads at byte B of the chunk become one wide load per 16/8/4 bytes (identical
+// loads from different taps are merged by the compiler) and a register extract.
+template <typename T> struct is_bf16_t { static constexpr bool value = false; };
+template <> struct is_bf16_t<bf16_t> { static constexpr bool value = true; };
+STEN_DEV float f16_bits_to_f32(u16 b) { float f; asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(b)); return f; }
+template <typename T, int CW, int B>
+STEN_DEV float chunk_elem(const unsigned char* row) {
+  u32 w;
+  if constexpr (CW % 16 == 0) {
+    const uint4 v = *(const uint4*)(row + (B / 16) * 16);
+    constexpr int q = (B % 16) / 4;
+    w = q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+  } else if constexpr (CW % 8 == 0) {
+    const uint2 v = *(const uint2*)(row + (B / 8) * 8);
+    w = ((B % 8) / 4) == 0 ? v.x : v.y;
+  } else {
+    w = *(const u32*)(row + (B / 4) * 4);
+  }
+  if constexpr (sizeof(T) == 4) {
+    return __uint_as_float(w);
+  } else {
+    const u32 h = (B % 4) ? (w >> 16) : (w & 0xffffu);
+    if constexpr (is_bf16_t<T>::value) return __uint_as_float(h << 16);
+    else return f16_bits_to_f32((u16)h);
+  }
+}
+// KV consecutive values to a (KV x element size)-aligned global address.
+STEN_DEV u32 pack2(const f16_t*, float lo, float hi) {
+  u32 w; asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(hi), "f"(lo)); return w;
+}
+STEN_DEV u32 pack2(const bf16_t*, float lo, float hi) {
+  u32 w; asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(hi), "f"(lo)); return w;
+}
+template <int KV> STEN_DEV void st_vec(float* p, const float* v) {
+  if constexpr (KV == 2) *(float2*)p = make_float2(v[0], v[1]);
+  else if constexpr (KV == 4) *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
+  else { for (int q = 0; q < KV; ++q) p[q] = v[q]; }
+}
+template <int KV, typename T> STEN_DEV void st_vec(T* p, const float* v) {
+  if constexpr (KV == 2) *(u32*)p = pack2(p, v[0], v[1]);
+  else if constexpr (KV == 4) *(uint2*)p = make_uint2(pack2(p, v[0], v[1]), pack2(p, v[2], v[3]));
+  else { for (int q = 0; q < KV; ++q) st_from_f32(p + q, v[q]); }
+}
+
 STEN_DEV float sten_clamp(float a, float lo, float hi) {
   // torch.clamp: min(max(a, lo), hi), NaN propagates
   return (a != a) ? a : fminf(fmaxf(a, lo), hi);

@@ -86,3 +86,29 @@ def test_config0_shape_against_oracle():
     g2, sink2, *_ = S.compile_expression(expr, boundary="periodic", field_map={"f": f.double(), "g": gg.double()})
     ref = O.evaluate(g2, [sink2])[sink2]
     assert rel_err(got, ref) <= 1e-5
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
+@pytest.mark.parametrize("boundary", ["periodic", "neumann"])
+def test_kv_chunks_match_one_voxel_per_thread(dtype, boundary):
+    """Several k-adjacent voxels per thread (vector shared-memory chunks, paired
+    stores) compute every voxel exactly as one voxel per thread does."""
+    import stenpy_b200 as S
+    from stenpy_b200.codegen import PassConfig
+    from stenpy_b200.synth import sinusoid_field, smoothed_vector
+    dev = _dev()
+    for shape in [(20, 33, 130), (9, 16, 64), (7, 5, 45)]:
+        f = sinusoid_field(shape, seed=4).to(dtype).to(dev)
+        u = smoothed_vector(shape, seed=5).to(dtype).to(dev)
+        expr = "divergence(gradient(f)) + l2norm(curl(u)) + laplacian(f)*tanh(f)"
+        outs = {}
+        for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8)):
+            cfg = PassConfig(tj=tj, tk=tk, threads=128, seg_len=8, kv=kv)
+            g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map={"f": f, "u": u})
+            w = [sink, g.add("variance", (sink,), {})]
+            res = S.Runtime(device=dev, out_dtype=dtype, config=cfg).run(g, wanted=w)
+            outs[kv, tk] = (res[w[0]], float(res[w[1]]))
+        ref, vref = outs[1, 64]
+        for key, (o, v) in outs.items():
+            assert torch.equal(o, ref), (key, shape, (o.float() - ref.float()).abs().max().item())
+            assert abs(v - vref) <= 1e-12 * abs(vref), (key, v, vref)

@@ -101,9 +101,9 @@ def features(spec: PassSpec, shape: Sequence[int]) -> Dict[str, float]:
 def schedule_features(spec: PassSpec, cfg: PassConfig) -> Dict[str, float]:
     trial = with_config(spec, cfg)
     smem, _, _ = smem_layout(trial)
-    return {"tj": cfg.tj, "tk": cfg.tk, "threads": cfg.threads, "vpt": cfg.tj * cfg.tk // cfg.threads,
+    return {"tj": cfg.tj, "tk": cfg.tk, "threads": cfg.threads, "vpt": cfg.tj * cfg.tk // (cfg.threads * cfg.kv),
             "seg_len": cfg.seg_len, "prefetch": cfg.prefetch, "smem": smem, "ghost": float(cfg.ghost),
-            "shell": float(shell_regions(trial) != "")}
+            "shell": float(shell_regions(trial) != ""), "kv": cfg.kv}
 
 
 def pass_key(spec: PassSpec, shape: Sequence[int]) -> str:

@@ -1243,14 +1243,14 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                      f"tk0 >= {hk} && tk0 + TK + {hk} <= p.n2) {{")
             K.append(f"        const {ct}* rowp = src + (((size_t)zq * p.n1 + (tj0 - {f.halo})) * p.n2 + (tk0 - {hk})) * {f.nc};")
             K.append(f"        const int pitch = p.n2 * {f.nc};")
-            for g0 in range(0, et, 8):
-                g1 = min(et, g0 + 8)
-                K.append(f"        {{ {ct} v_[{g1 - g0}];")
-                K.append(f"          #pragma unroll\n          for (int t = 0; t < {g1 - g0}; ++t) {{ const int e = tid + (t + {g0}) * NT;"
-                         f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (size_t)yy * pitch + (e - yy * {w})); }} }}")
-                K.append(f"          #pragma unroll\n          for (int t = 0; t < {g1 - g0}; ++t) {{ const int e = tid + (t + {g0}) * NT;"
-                         f" if (e < {w * h}) dst[e] = v_[t]; }}")
-                K.append("        }")
+            gsz = 4
+            K.append(f"        #pragma unroll 1\n        for (int t0 = 0; t0 < {et}; t0 += {gsz}) {{")
+            K.append(f"          {ct} v_[{gsz}];")
+            K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
+                     f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (yy * pitch + (e - yy * {w}))); }} }}")
+            K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
+                     f" if (e < {w * h}) dst[e] = v_[t]; }}")
+            K.append("        }")
             K.append("      } else")
             K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
             K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")

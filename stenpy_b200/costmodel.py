@@ -7,9 +7,12 @@ rows per thread, z-segment, boundary strategy, shared memory) so that only the
 top few need timing. It changes which schedule is picked, never any result.
 
 * Network: in -> 64 -> ReLU -> 64 -> ReLU -> 1, trained with mean-squared error on
-  log nanoseconds per voxel, Adam. Forward, backward and the optimizer step are
-  the library's own CUDA kernels (``stenpy_mlp_forward`` / ``stenpy_mlp_loss_grad``
-  / ``stenpy_adam_step``); PyTorch only holds the device buffers.
+  log nanoseconds per voxel centred per pass (only the order of a pass's
+  candidates matters, not the pass's absolute cost), Adam with weight decay; an
+  ensemble of a few seeds is averaged. Forward, backward and the optimizer step
+  are the library's own CUDA kernels (``stenpy_mlp_forward`` /
+  ``stenpy_mlp_loss_grad`` / ``stenpy_adam_step``); PyTorch only holds the device
+  buffers.
 * Data: the autotuner's JSON-lines log (``autotune.LOG_PATH``).
 * ``random_dag`` generates the cost-model workload: random expression DAGs of
   3-20 ops over the operator list, stencil reach 1-2, FP32 or BF16 fields, grids
@@ -32,8 +35,8 @@ from . import _native as N
 HIDDEN = 64
 GRAPH_KEYS = ["radius", "n_fields", "in_bytes", "out_bytes", "n_d1", "n_lap", "n_trans", "n_arith", "n_eig",
               "n_out", "n_red", "n_slots", "narrow", "max_nc"]
-SCHED_KEYS = ["tj", "tk", "threads", "vpt", "seg_len", "prefetch", "smem", "ghost", "shell"]
-_LOG_KEYS = {"tj", "tk", "threads", "vpt", "seg_len"}
+SCHED_KEYS = ["tj", "tk", "threads", "vpt", "seg_len", "prefetch", "smem", "ghost", "shell", "kv"]
+_LOG_KEYS = {"tj", "tk", "threads", "vpt", "seg_len", "kv"}
 
 
 def vectorize(feat: Dict[str, float], sched: Dict[str, float]) -> List[float]:
@@ -43,7 +46,7 @@ def vectorize(feat: Dict[str, float], sched: Dict[str, float]) -> List[float]:
     n0, n1, n2 = float(feat["n0"]), float(feat["n1"]), float(feat["n2"])
     x += [math.log2(n0), math.log2(n1), math.log2(n2), math.log2(max(feat["voxels"], 1.0))]
     for k in SCHED_KEYS:
-        v = float(sched.get(k, 0.0))
+        v = float(sched.get(k, 1.0 if k == "kv" else 0.0))
         x.append(math.log2(v) if k in _LOG_KEYS and v > 0 else (v / 1e5 if k == "smem" else v))
     tj, tk, seg = float(sched["tj"]), float(sched["tk"]), float(sched["seg_len"])
     ctas = math.ceil(n1 / tj) * math.ceil(n2 / tk) * math.ceil(n0 / seg)
@@ -112,7 +115,7 @@ class CostModel:
         return loss, self.grad
 
     def fit(self, X: torch.Tensor, y: torch.Tensor, steps: int = 3000, batch: int = 256, lr: float = 2e-3,
-            weight_decay: float = 1e-5, seed: int = 0) -> List[float]:
+            weight_decay: float = 1e-3, seed: int = 0) -> List[float]:
         self.mu = X.mean(0)
         self.sd = X.std(0).clamp(min=1e-6)
         self.y_mu = float(y.mean())
@@ -145,6 +148,72 @@ class CostModel:
         m.params = torch.from_numpy(z["params"]).to(m.device)
         m.mu, m.sd, m.y_mu = torch.from_numpy(z["mu"]), torch.from_numpy(z["sd"]), float(z["y_mu"])
         return m
+
+
+class Ensemble:
+    """Average of several independently seeded models (lower-variance ranking)."""
+
+    def __init__(self, models: Sequence[CostModel]):
+        self.models = list(models)
+
+    def predict(self, X: torch.Tensor) -> torch.Tensor:
+        return sum(m.predict(X) for m in self.models) / len(self.models)
+
+    @classmethod
+    def train(cls, X: torch.Tensor, y: torch.Tensor, device: Any = "cuda", n: int = 5, seed: int = 0,
+              **fit_kw) -> Tuple["Ensemble", List[List[float]]]:
+        models, hists = [], []
+        for i in range(n):
+            m = CostModel(X.shape[1], device, seed=seed * 1000 + i)
+            hists.append(m.fit(X, y, seed=seed * 1000 + i, **fit_kw))
+            models.append(m)
+        return cls(models), hists
+
+    def save(self, path: str) -> None:
+        np.savez(path, n=len(self.models), **{f"m{i}_{k}": v for i, m in enumerate(self.models)
+                                              for k, v in (("in_dim", m.in_dim), ("hidden", m.hidden),
+                                                           ("params", m.params.cpu().numpy()),
+                                                           ("mu", m.mu.numpy()), ("sd", m.sd.numpy()),
+                                                           ("y_mu", m.y_mu))})
+
+    @classmethod
+    def load(cls, path: str, device: Any = "cuda") -> "Ensemble":
+        z = np.load(path)
+        models = []
+        for i in range(int(z["n"])):
+            m = CostModel(int(z[f"m{i}_in_dim"]), device, int(z[f"m{i}_hidden"]))
+            m.params = torch.from_numpy(z[f"m{i}_params"]).to(m.device)
+            m.mu, m.sd = torch.from_numpy(z[f"m{i}_mu"]), torch.from_numpy(z[f"m{i}_sd"])
+            m.y_mu = float(z[f"m{i}_y_mu"])
+            models.append(m)
+        return cls(models)
+
+
+def centred_targets(recs: Sequence[Dict[str, Any]]) -> torch.Tensor:
+    """log ns/voxel minus its mean over the timed candidates of the same pass."""
+    _, y = records_to_xy(recs)
+    groups: Dict[str, List[int]] = {}
+    for i, r in enumerate(recs):
+        groups.setdefault(r["tag"] + ":" + r["key"], []).append(i)
+    for idx in groups.values():
+        y[idx] -= y[idx].mean()
+    return y
+
+
+def analytic_cost(feat: Dict[str, float], sched: Dict[str, float]) -> float:
+    """A roofline-style estimate without learning: bytes moved (staged halo and
+    z-segment overlap included) times the wave-quantisation loss of the grid."""
+    n0, n1, n2 = float(feat["n0"]), float(feat["n1"]), float(feat["n2"])
+    tj, tk, seg, nt = float(sched["tj"]), float(sched["tk"]), float(sched["seg_len"]), float(sched["threads"])
+    r = float(feat.get("radius", 0))
+    halo = (tj + 2 * r) * (tk + (8 if r > 0 else 0)) / (tj * tk)
+    zf = (min(seg, n0) + 2 * r) / min(seg, n0)
+    ctas = math.ceil(n1 / tj) * math.ceil(n2 / tk) * math.ceil(n0 / seg)
+    per_sm = max(1, min(2048 // int(nt), 32, int(227e3 // max(float(sched.get("smem", 1.0)), 1.0))))
+    waves = ctas / (148.0 * per_sm)
+    tail = math.ceil(waves) / waves if waves > 0 else 1.0
+    cover = (math.ceil(n1 / tj) * tj * math.ceil(n2 / tk) * tk) / (n1 * n2)
+    return (feat["in_bytes"] * halo * zf + feat["out_bytes"]) * cover * tail
 
 
 def load_records(path: str, tags: Optional[Sequence[str]] = None) -> List[Dict[str, Any]]:
@@ -183,10 +252,10 @@ def evaluate(model: CostModel, heldout: Sequence[Dict[str, Any]], k: int = 3, se
     the model ranks fastest, keep the measured best of those, compare with the
     measured best of all candidates. Baselines without the model: the default
     schedule alone, and k schedules picked at random."""
-    from .codegen import PassConfig
     rng = np.random.default_rng(seed)
-    default = vars(PassConfig())
-    reg_model, reg_rand, reg_def, reg_top1, n_cands = [], [], [], [], []
+    # the fixed schedule closest to the executor's default (64 x 8 tiles, 128 threads)
+    default = {"tj": 8, "tk": 64, "threads": 128, "seg_len": 32}
+    reg_model, reg_rand, reg_def, reg_top1, reg_an, n_cands = [], [], [], [], [], []
     for key, rs in group_by_pass(heldout).items():
         if len(rs) < 8:
             continue
@@ -199,14 +268,17 @@ def evaluate(model: CostModel, heldout: Sequence[Dict[str, Any]], k: int = 3, se
         reg_model.append(ms[order[:k]].min() / best - 1.0)
         reg_top1.append(ms[order[0]] / best - 1.0)
         reg_rand.append(ms[rng.choice(len(rs), size=min(k, len(rs)), replace=False)].min() / best - 1.0)
-        d = [r["ms"] for r in rs if all(r["cfg"].get(a) == default[a] for a in ("tj", "tk", "threads", "seg_len"))
-             and r["cfg"].get("ghost", True)]
+        an = np.array([analytic_cost(r["features"], r["schedule"]) for r in rs])
+        reg_an.append(ms[np.argsort(an, kind="stable")[:k]].min() / best - 1.0)
+        d = [r["ms"] for r in rs if all(r["cfg"].get(a) == default[a] for a in default)
+             and r["cfg"].get("ghost", True) and r["cfg"].get("kv", 1) == 1]
         if d:
             reg_def.append(d[0] / best - 1.0)
     mean_c = float(np.mean(n_cands)) if n_cands else 0.0
     return {"top_k": k, "passes": len(reg_model), "candidates_per_pass": mean_c,
             "model_topk": _stats(reg_model), "model_top1": _stats(reg_top1),
-            "random_topk": _stats(reg_rand), "default_schedule": _stats(reg_def),
+            "random_topk": _stats(reg_rand), "analytic_topk": _stats(reg_an),
+            "default_schedule": _stats(reg_def),
             "timing_runs_saved_frac": (1.0 - k / mean_c) if mean_c else None}
 
 

@@ -79,7 +79,26 @@ class OpLowerer:
     def r(self, *nids: int) -> int:
         return max([self.pg.nodes[n].radius for n in nids] + [0])
 
+    def component(self, x: int, c: int) -> Optional[int]:
+        """The scalar node holding component ``c`` of ``x`` when ``x`` is built by
+        stacking (so a consumer of one component does not evaluate the others)."""
+        n = self.pg.nodes[x]
+        if n.nc == 1 and c == 0:
+            return x
+        if n.op != "stack":
+            return None
+        for y in n.ins:
+            k = self.nc(y)
+            if c < k:
+                return self.component(y, c)
+            c -= k
+        return None
+
     def d1(self, x: int, axis: int, mode: str, h: float, comp: Optional[int] = None) -> int:
+        if comp is not None:
+            y = self.component(x, comp)
+            if y is not None:          # derivative of one stacked component: that component alone
+                x, comp = y, None
         nc = 1 if comp is not None else self.nc(x)
         rad = self.r(x) + (0 if mode == "zero" else 1)
         return self.pg.add("d1", (x,), nc, rad, axis=axis, mode=mode, comp=comp,
@@ -148,6 +167,9 @@ class OpLowerer:
             need(1); no_extra()
             if self.nc(ins[0]) != 9:
                 raise LoweringError("trace: needs (*, 3, 3) input")
+            diag = [self.component(ins[0], c) for c in (0, 4, 8)]
+            if all(d is not None for d in diag):   # only the diagonal is evaluated
+                return self.binop("add", self.binop("add", diag[0], diag[1]), diag[2])
             return self.pg.add("trace", (ins[0],), 1, self.r(ins[0]))
         if op == "eigenvalues":
             need(1); no_extra()
@@ -159,8 +181,14 @@ class OpLowerer:
             nc = self.nc(ins[0])
             idx = int(p["index"])
             if nc == 3 and 0 <= idx < 3:
+                y = self.component(ins[0], idx)
+                if y is not None:
+                    return y
                 return self.pg.add("select", (ins[0],), 1, self.r(ins[0]), index=idx)
             if nc == 9 and 0 <= idx < 3:
+                row = [self.component(ins[0], 3 * idx + c) for c in range(3)]
+                if all(y is not None for y in row):
+                    return self.stack(row)
                 return self.pg.add("select", (ins[0],), 3, self.r(ins[0]), index=idx)
             raise LoweringError("select_component: index out of range")
 

@@ -28,8 +28,8 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, plane_bytes, shell_count, valid_shape,
-                      shell_regions, smem_layout, with_config)
+from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, is_flat, pass_grid, plane_bytes,
+                      shell_count, shell_regions, smem_layout, valid_shape, with_config)
 
 LOG_PATH = os.environ.get("STENPY_TUNE_LOG", os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                                           "_tune", "timings.jsonl"))
@@ -69,7 +69,8 @@ def candidates(spec: PassSpec) -> List[PassConfig]:
     # keep distinct schedules only (scan passes collapse the segment axis)
     seen, uniq = set(), []
     for c in out:
-        k = (c.tj, c.tk, c.threads, c.seg_len, c.prefetch, c.ghost)
+        # a flat pass only uses the block size
+        k = (c.threads,) if is_flat(spec) else (c.tj, c.tk, c.threads, c.seg_len, c.prefetch, c.ghost, c.kv)
         if k not in seen:
             seen.add(k)
             uniq.append(c)
@@ -116,8 +117,8 @@ def _launches(pp: FC.PassPlan, spec: PassSpec, values: Dict[str, Any], shape, de
     n0, n1, n2 = shape
     cfg = spec.cfg
     tiles_k = -(-n2 // cfg.tk)
-    tiles_j = -(-n1 // cfg.tj)
-    grid = (tiles_j * tiles_k, -(-n0 // cfg.seg_len), 1)
+    gx, gy = pass_grid(spec, n1, n2, n0)
+    grid = (gx, gy, 1)
     ncta = grid[0] * grid[1]
     fptrs = [values[nid].data_ptr() for nid in pp.field_nodes]
     tmaps = FC.encode_tmaps(spec, fptrs, n0, n1, n2)
@@ -145,7 +146,8 @@ def time_schedule(pp: FC.PassPlan, cfg: PassConfig, values: Dict[str, Any], shap
     mod = N.load_module(key, cubin, "sten_kernel", smem, dev_idx)
     shell_mod = N.load_module(key + ":shell", cubin, "sten_shell", 0, dev_idx) if FC.has_shell(spec) else None
     n_shell = -(-shell_count(shape, spec.radius, regions=shell_regions(spec)) // SHELL_THREADS)
-    tiles = (-(-shape[1] // cfg.tj)) * (-(-shape[2] // cfg.tk)) * (-(-shape[0] // cfg.seg_len))
+    gx, gy = pass_grid(spec, shape[1], shape[2], shape[0])
+    tiles = gx * gy
     part = torch.empty(max((tiles + n_shell) * spec.nslots, 1), dtype=torch.float64, device=device)
     table = torch.zeros(max(spec.n_scalars, 1) + 8, dtype=torch.float64, device=device)
     err = FC.ErrorFlag.get(device)

@@ -36,7 +36,8 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import PassConfig, PassSpec, emit_batch_module, emit_pass, shell_count, shell_regions, smem_layout
+from .codegen import (PassConfig, PassSpec, emit_batch_module, emit_pass, pass_grid, shell_count, shell_regions,
+                      smem_layout)
 from .graph import Graph
 from .runtime import default_wanted
 
@@ -223,8 +224,7 @@ class BatchProgram:
                 prog = module.index.get(program_key(spec))
                 if prog is None:
                     raise FC.FusionError("batch: pass program missing from the module")
-                gdx = -(-n2 // spec.cfg.tk) * -(-n1 // spec.cfg.tj)
-                nseg = -(-n0 // spec.cfg.seg_len)
+                gdx, nseg = pass_grid(spec, n1, n2, n0)
                 n_shell = shell_count(plan.shape, spec.radius, regions=shell_regions(spec))
                 shell_items = -(-n_shell // nt)
                 phases.append(_Phase(ji, pi, prog, gdx, nseg, shell_items, gdx * nseg + shell_items,

@@ -220,6 +220,25 @@ def valid_shape(cfg: "PassConfig") -> bool:
     return cfg.tj % rows == 0 and cfg.tj // rows >= 1
 
 
+FLAT_V = 4       # voxels per thread per step of a flat (stencil-free) pass
+FLAT_ITER = 8    # steps per work item: an item covers threads x FLAT_V x FLAT_ITER voxels
+
+
+def is_flat(spec: "PassSpec") -> bool:
+    """A pass without stencils or scans runs flat: its voxels as one linear range,
+    each thread FLAT_V consecutive voxels per step with vector loads, no staging."""
+    return spec.radius == 0 and not spec.has_scan
+
+
+def pass_grid(spec: "PassSpec", n1: int, n2: int, n_out: int) -> Tuple[int, int]:
+    """(tiles or chunks, z-segments) of one launch covering ``n_out`` planes."""
+    cfg = spec.cfg
+    if is_flat(spec):
+        ch = cfg.threads * FLAT_V * FLAT_ITER
+        return max(1, -(-(n_out * n1 * n2) // ch)), 1
+    return -(-n1 // cfg.tj) * -(-n2 // cfg.tk), max(1, -(-n_out // cfg.seg_len))
+
+
 def with_config(spec: "PassSpec", cfg: "PassConfig") -> "PassSpec":
     """Copy of ``spec`` under another schedule (fields copied, ghost plan redone)."""
     import dataclasses
@@ -250,6 +269,7 @@ def _lit(x: float) -> str:
 class _Emitter:
     def __init__(self, spec: PassSpec):
         self.s = spec
+        self.flat = is_flat(spec)
         self.g = spec.graph
         self.R = spec.radius
         self.lines: List[str] = []
@@ -366,6 +386,9 @@ class _Emitter:
                 body.append(f"{arr}[{c}] = LDF{f.slot}<{di}, {dj}, ({dk}) * {f.nc} + {c}>(x);")
         elif di != "0" or dj not in ("0", "M") or dk not in ("0", "KK"):
             raise AssertionError("unstaged field read at an offset")
+        elif self.flat:
+            for c in range(n.nc):
+                body.append(f"{arr}[{c}] = x.fv{f.slot}[({dk}) * {f.nc} + {c}];")
         else:
             for c in range(n.nc):
                 body.append(f"{arr}[{c}] = ldg_as_f32(x.gp{f.slot} + {c});")
@@ -775,9 +798,14 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
         nc = e.g.nodes[r.node].nc
         if any(r is x for x in skip):
             continue
+        # z-march: per-plane row pointers advanced by the march (no 64-bit index math per voxel)
+        tile_ptr = where == "main" and not is_flat(spec)
         if r.kind == "out":
             ct = CTYPE[r.out_dtype]
-            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
+            if tile_ptr:
+                K.append(f"{{ {ct}* o_ = orow{r.out_slot} + ro_[{{M}}] * {nc} + {{KK}} * {nc};")
+            else:
+                K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
             for c in range(nc):
                 K.append(f"  st_from_f32(o_ + {c}, rv[{off + c}]);")
             K.append("}")
@@ -785,7 +813,10 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
             assert scan_ok
             ct = CTYPE[r.out_dtype]
             half = repr(0.5 * float(r.dx[0]))
-            K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
+            if tile_ptr:
+                K.append(f"{{ {ct}* o_ = orow{r.out_slot} + ro_[{{M}}] * {nc} + {{KK}} * {nc};")
+            else:
+                K.append(f"{{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (vox - out_base) * {nc};")
             for c in range(nc):
                 q = f"mq * {nc} + {c}"
                 K.append(f"  if (gi > 0) sc{si}_acc[{q}] += ((double)sc{si}_prev[{q}] + (double)rv[{off + c}]) * {half};")
@@ -827,7 +858,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
                              f" b_ = b_ < 0 ? 0 : (b_ > {r.bins - 1} ? {r.bins - 1} : b_); sten_hist_add(rv{ri_here}_hs, b_); }}")
                 elif r.red == "integrate":
                     sm = 1 if r.method == "simpson" else 0
-                    if where == "main":
+                    if where == "main" and not is_flat(spec):
                         # per-plane and per-column weights computed outside the voxel loop
                         K.append(f"rv{ri_here}_a += {val} * rv{ri_here}_wi * rv{ri_here}_wj[{{M}}] * rv{ri_here}_wk[{{KK}}];")
                     else:
@@ -1034,6 +1065,79 @@ def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Option
 SHELL_THREADS = 256
 
 
+def _flat_body(spec: PassSpec, e: "_Emitter", red_off: int, batch: bool) -> List[str]:
+    """Kernel body of a flat pass: work item ``bx`` covers voxels
+    [out_base + bx*CH, out_base + (bx+1)*CH) of the planes [out_lo, out_lo + n_out)."""
+    K: List[str] = []
+    nroot = e.nroot
+    reds = [r for r in spec.roots if r.kind == "red"]
+    K.append("  unsigned char* smem = sten_smem;")
+    K.append(f"  double* red_scratch = (double*)(smem + {red_off});")
+    K.append("  const int tid = threadIdx.x;")
+    K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
+    K.append("  const size_t out_base = (size_t)p.out_lo * plane_n;")
+    K.append("  const size_t vhi = out_base + (size_t)p.n_out * plane_n;")
+    K.append("  const size_t c0 = out_base + (size_t)bx * (NT * FV * FITER);")
+    K.append("  const int cta = p.cta_off + bx;")
+    K.append("  FCtx x;")
+    K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
+             f"x.sc[s] = (s < {spec.n_scalars}) ? (float)__ldcg(p.scal + s) : 0.0f;")
+    K += ["  " + k for k in _red_decls(spec)]
+    if any(r.red == "hist" for r in reds):
+        K.append("  __syncthreads();  // histogram cleared")
+    need_idx = any(r.red == "integrate" for r in reds)
+    vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1
+                and r.out_dtype in ("f32", "f16", "bf16")]
+    K.append("  #pragma unroll 1")
+    K.append("  for (int it = 0; it < FITER; ++it) {")
+    K.append("    const size_t base = c0 + ((size_t)it * NT + tid) * FV;")
+    K.append("    if (base >= vhi) break;")
+    K.append("    const int nv = (int)min((size_t)FV, vhi - base);")
+    K.append("    const bool full = nv == FV;")
+    for f in spec.fields:
+        ct, es = CTYPE[f.dtype], ESIZE[f.dtype]
+        nb = FLAT_V * f.nc * es
+        va = 16 if nb % 16 == 0 else (8 if nb % 8 == 0 else (4 if nb % 4 == 0 else 0))
+        K.append(f"    {{ const {ct}* fp_ = (const {ct}*)p.fld[{f.slot}] + base * {f.nc};")
+        if va and es in (2, 4):
+            K.append(f"      if (full && (((size_t)fp_) & {va - 1}) == 0) ld_vec_f32<{ct}, FV * {f.nc}>(fp_, x.fv{f.slot});")
+            K.append(f"      else ld_part_f32<{ct}, FV * {f.nc}>(fp_, nv * {f.nc}, x.fv{f.slot}); }}")
+        else:
+            K.append(f"      ld_part_f32<{ct}, FV * {f.nc}>(fp_, nv * {f.nc}, x.fv{f.slot}); }}")
+    if need_idx:
+        K.append("    size_t i_ = base / plane_n; const size_t r_ = base - i_ * plane_n;")
+        K.append("    int jq = (int)(r_ / (size_t)p.n2), kq = (int)(r_ - (size_t)jq * p.n2);")
+    K.append(f"    float rvk[FV][{nroot}];")
+    for v in range(FLAT_V):
+        K.append(f"    if ({v} < nv) {{")
+        if need_idx:
+            K.append("      const int gi = (int)i_ + p.i_base, j = jq, k = kq;")
+        K.append(f"      const size_t vox = base + {v};")
+        K.append(f"      float* rv = rvk[{v}];")
+        K.append(f"      eval_fast<0, {v}>(x, rv);")
+        K += ["      " + k for k in _epilogue(spec, e, scan_ok=False, skip=vec_outs, where="flat", m=0, kk=v)]
+        K.append("    }")
+        if need_idx and v + 1 < FLAT_V:
+            K.append("    if (++kq == p.n2) { kq = 0; if (++jq == p.n1) { jq = 0; ++i_; } }")
+    for r in vec_outs:
+        ct = CTYPE[r.out_dtype]
+        off = e.offsets[spec.roots.index(r)]
+        sa = FLAT_V * ESIZE[r.out_dtype]
+        vals = ", ".join(f"rvk[{q}][{off}]" for q in range(FLAT_V))
+        K.append(f"    {{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (base - out_base);")
+        K.append(f"      if (full && (((size_t)o_) & {sa - 1}) == 0) {{ const float v_[FV] = {{{vals}}}; st_vec<FV>(o_, v_); }}")
+        K.append("      else {")
+        for q in range(FLAT_V):
+            K.append(f"        if ({q} < nv) st_from_f32(o_ + {q}, rvk[{q}][{off}]);")
+        K.append("      }")
+        K.append("    }")
+    K.append("  }")
+    K += ["  " + k for k in _red_flush(spec, "cta")]
+    if batch:
+        K.append("  return true;")
+    return K
+
+
 def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int = 0) -> str:
     """Source of the pass: ``sten_kernel`` (z-march over the tile grid) and, when the
     pass has a stencil reach R > 0 and no scan, ``sten_shell`` (one thread per voxel
@@ -1045,6 +1149,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     one block of shell voxels per call, parameters read from global memory), without
     the shared header; ``batch_threads`` is the batch kernel's block size."""
     batch = batch_ns is not None
+    flat = is_flat(spec)
     header = ""
     if not batch:
         with open(HEADER_PATH) as fh:
@@ -1067,7 +1172,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         L.append(header)
     L.append(f"#define TJ {cfg.tj}\n#define TK {cfg.tk}\n#define NT {cfg.threads}\n#define RAD {R}"
              f"\n#define NSLOT {nslot}\n#define VPT {vpt}\n#define NSLOTS_RED {max(spec.nslots, 1)}"
-             f"\n#define KV {cfg.kv}\n#define TKT {cfg.tk // cfg.kv}")
+             f"\n#define KV {cfg.kv}\n#define TKT {cfg.tk // cfg.kv}\n#define FV {FLAT_V}\n#define FITER {FLAT_ITER}")
     if batch:
         L.append(f"namespace {batch_ns} {{")
     ntma = len(tmap_specs(spec))
@@ -1115,6 +1220,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         if f.staged:
             # byte offset of this thread's chunk (row 0, first k) in each ring slot in use
             L.append(f"  unsigned int sb{f.slot}[2 * RAD + 1];")
+        elif is_flat(spec):
+            L.append(f"  float fv{f.slot}[FV * {f.nc}];")
         else:
             L.append(f"  const {ct}* gp{f.slot};")
     L.append(f"  float sc[{max(spec.n_scalars, 1)}];")
@@ -1154,261 +1261,282 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                  f"sten_kernel(const __grid_constant__ Params p) {{")
         K.append("  const Params& pg = p;")
         K.append("  const int bx = blockIdx.x, by = blockIdx.y, gdx = gridDim.x;")
-    K.append("  unsigned char* smem = sten_smem;")
-    K.append("  u64* bars = (u64*)smem;")
-    K.append(f"  double* red_scratch = (double*)(smem + {red_off});")
-    K.append("  const int tid = threadIdx.x;")
-    K.append("  const int tile = bx;")
-    K.append("  const int tk0 = (tile % p.tiles_k) * TK;")
-    K.append("  const int tj0 = (tile / p.tiles_k) * TJ;")
-    K.append("  const int ib = p.out_lo + by * p.seg_len;")
-    K.append("  const int ie = min(ib + p.seg_len, p.out_lo + p.n_out);")
-    K.append("  const int cta = p.cta_off + by * gdx + bx;")
-    K.append("  const bool edge_cta = tk0 == 0 || tk0 + TK >= p.n2 || tj0 == 0 || tj0 + TJ >= p.n1;")
-    K.append("  FCtx x;")
-    K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
-             f"x.sc[s] = (s < {spec.n_scalars}) ? (float)__ldcg(p.scal + s) : 0.0f;")
-    K += ["  " + k for k in _red_decls(spec)]
-    if any(r.red == "hist" for r in reds):
-        K.append("  __syncthreads();  // histogram cleared")
-    for si, r in enumerate(scans):
-        nc = e.g.nodes[r.node].nc
-        K.append(f"  double sc{si}_acc[VPT * KV * {nc}]; float sc{si}_prev[VPT * KV * {nc}];")
-        K.append(f"  #pragma unroll\n  for (int q = 0; q < VPT * KV * {nc}; ++q) {{ sc{si}_acc[q] = 0.0; sc{si}_prev[q] = 0.0f; }}")
-    staged = tma_fields or lsu_fields
-    tmaps = tmap_specs(spec)
-    tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
-    K.append("  const int p_first = ib - RAD;")
-    if tma_fields:
-        K.append("  if (tid == 0) {")
-        K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
-        K.append("    fence_mbar_init();")
-        for ti in range(len(tmaps)):
-            K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
-        K.append("  }")
-        K.append("  __syncthreads();")
-    if staged:
-        K.append("  auto request = [&](int q) {")
-        K.append("    const int s = (q - p_first) % NSLOT;")
-        if ghost and spec.i_periodic:
-            K.append("    const int zq = (q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q;")
-        else:
-            K.append("    const int zq = q;")
+    if flat:
+        K += _flat_body(spec, e, red_off, batch)
+    else:
+        K.append("  unsigned char* smem = sten_smem;")
+        K.append("  u64* bars = (u64*)smem;")
+        K.append(f"  double* red_scratch = (double*)(smem + {red_off});")
+        K.append("  const int tid = threadIdx.x;")
+        K.append("  const int tile = bx;")
+        K.append("  const int tk0 = (tile % p.tiles_k) * TK;")
+        K.append("  const int tj0 = (tile / p.tiles_k) * TJ;")
+        K.append("  const int ib = p.out_lo + by * p.seg_len;")
+        K.append("  const int ie = min(ib + p.seg_len, p.out_lo + p.n_out);")
+        K.append("  const int cta = p.cta_off + by * gdx + bx;")
+        K.append("  const bool edge_cta = tk0 == 0 || tk0 + TK >= p.n2 || tj0 == 0 || tj0 + TJ >= p.n1;")
+        K.append("  FCtx x;")
+        K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
+                 f"x.sc[s] = (s < {spec.n_scalars}) ? (float)__ldcg(p.scal + s) : 0.0f;")
+        K += ["  " + k for k in _red_decls(spec)]
+        if any(r.red == "hist" for r in reds):
+            K.append("  __syncthreads();  // histogram cleared")
+        for si, r in enumerate(scans):
+            nc = e.g.nodes[r.node].nc
+            K.append(f"  double sc{si}_acc[VPT * KV * {nc}]; float sc{si}_prev[VPT * KV * {nc}];")
+            K.append(f"  #pragma unroll\n  for (int q = 0; q < VPT * KV * {nc}; ++q) {{ sc{si}_acc[q] = 0.0; sc{si}_prev[q] = 0.0f; }}")
+        staged = tma_fields or lsu_fields
+        tmaps = tmap_specs(spec)
+        tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
+        K.append("  const int p_first = ib - RAD;")
         if tma_fields:
-            K.append("    if (tid == 0) {")
-            K.append("      fence_proxy_async();")
-            K.append(f"      unsigned int bytes_ = {tma_bytes}u;")
-            for f in tma_fields:
-                (kw, kh), (jw, jh) = strip_boxes(spec, f)
-                es = ESIZE[f.dtype]
-                if f.wrap_k:
-                    K.append(f"      if (tk0 == 0) bytes_ += {kw * kh * es}u;")
-                    K.append(f"      if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
-                if f.wrap_j:
-                    K.append(f"      if (tj0 == 0) bytes_ += {jw * jh * es}u;")
-                    K.append(f"      if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
-            K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
-            for f in tma_fields:
-                base = f"smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}"
-                lay = slot_layout(spec, f)
-                hk = spec.hk(f)
-                K.append(f"      tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
-                         f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
-                if f.wrap_k:
-                    ti = tidx[(f.slot, "kstrip")]
-                    K.append(f"      if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
-                             f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
-                    K.append(f"      if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
-                             f"0, tj0, zq);")
-                if f.wrap_j:
-                    ti = tidx[(f.slot, "jstrip")]
-                    K.append(f"      if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
-                             f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
-                    K.append(f"      if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
-                             f"(tk0 - {hk}) * {f.nc}, 0, zq);")
-            K.append("    }")
-        for f in lsu_fields:
-            w, h = spec.box(f)
-            ct = CTYPE[f.dtype]
-            rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
-            rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-            hk = spec.hk(f)
-            et = -(-(w * h) // cfg.threads)
-            K.append("    {")
-            K.append(f"      {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
-            K.append(f"      const {ct}* src = (const {ct}*)p.fld[{f.slot}];")
-            # tile box inside the field: plain row-offset loads, issued in groups of 8
-            # before their shared-memory stores (one memory latency per group)
-            K.append(f"      if (zq >= 0 && zq < p.nl && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && "
-                     f"tk0 >= {hk} && tk0 + TK + {hk} <= p.n2) {{")
-            K.append(f"        const {ct}* rowp = src + (((size_t)zq * p.n1 + (tj0 - {f.halo})) * p.n2 + (tk0 - {hk})) * {f.nc};")
-            K.append(f"        const int pitch = p.n2 * {f.nc};")
-            gsz = 4
-            K.append(f"        #pragma unroll 1\n        for (int t0 = 0; t0 < {et}; t0 += {gsz}) {{")
-            K.append(f"          {ct} v_[{gsz}];")
-            K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
-                     f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (yy * pitch + (e - yy * {w}))); }} }}")
-            K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
-                     f" if (e < {w * h}) dst[e] = v_[t]; }}")
-            K.append("        }")
-            K.append("      } else")
-            K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
-            K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
-            K.append(f"        int jg = tj0 - {f.halo} + yy;")
-            K.append(f"        const int xr = xx - {spec.hk(f)} * {f.nc};")
-            K.append(f"        int kg = tk0 + (xr >= 0 ? xr / {f.nc} : -((-xr + {f.nc} - 1) / {f.nc}));")
-            K.append(f"        const int c = xr - (kg - tk0) * {f.nc};")
-            for ax, var, n, rule in ((1, "jg", "p.n1", rj), (2, "kg", "p.n2", rk)):
-                if rule == "periodic":
-                    K.append(f"        {var} = wrap_idx({var}, {n});")
-                elif rule == "replicate":
-                    K.append(f"        {var} = clamp_idx({var}, {n});")
-                elif rule == "reflect":
-                    K.append(f"        if ({n} > 1) {var} = reflect_idx({var}, {n});")
-            K.append(f"        {ct} v; v.bits = 0;" if ESIZE[f.dtype] == 2 else f"        {ct} v = ({ct})0;")
-            K.append("        if (zq >= 0 && zq < p.nl && jg >= 0 && jg < p.n1 && kg >= 0 && kg < p.n2)")
-            K.append(f"          v = src[(((size_t)zq * p.n1 + jg) * p.n2 + kg) * {f.nc} + c];")
-            K.append("        dst[e] = v;")
-            K.append("      }")
-            K.append("    }")
-        K.append("  };")
-        if ghost:
-            K += ["  " + x for x in _ghost_fill(spec, rings)]
-        K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
-        if lsu_fields:
+            K.append("  if (tid == 0) {")
+            K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
+            K.append("    fence_mbar_init();")
+            for ti in range(len(tmaps)):
+                K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
+            K.append("  }")
             K.append("  __syncthreads();")
-    K.append("  bool ok = true;")
-    # planes p_first .. ib+RAD must be resident (and ghosted) before the first plane
-    if tma_fields:
-        K.append("  for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) {")
-        K.append("    const int rel = q - p_first;")
-        K.append("    ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-        K.append("  }")
-    if ghost and staged:
-        K.append("  if (edge_cta) { for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) ghost_fill(q); }")
-    if staged:
-        K.append("  __syncthreads();")
-    # each thread owns KV adjacent columns (kt0 ..) of the tile and VPT consecutive rows;
-    # everything that does not depend on the plane is computed once, before the march
-    kvn = cfg.kv
-    K.append("  const int tk = (tid % TKT) * KV, tjb = (tid / TKT) * VPT;")
-    K.append("  const int kt0 = tk0 + tk;")
-    K.append("  bool k_ok[KV];")
-    K.append("  #pragma unroll")
-    if split and not ghost:
-        K.append("  for (int q = 0; q < KV; ++q) k_ok[q] = kt0 + q >= RAD && kt0 + q < p.n2 - RAD;")
-    else:
-        K.append("  for (int q = 0; q < KV; ++q) k_ok[q] = kt0 + q < p.n2;")
-    K.append("  const bool k_all = " + " && ".join(f"k_ok[{q}]" for q in range(kvn)) + ";")
-    K.append("  bool m_ok[VPT];")
-    K.append("  #pragma unroll")
-    K.append("  for (int m = 0; m < VPT; ++m) {")
-    K.append("    const int j = tj0 + tjb + m;")
-    if split and not ghost:
-        K.append("    m_ok[m] = j >= RAD && j < p.n1 - RAD;")
-    else:
-        K.append("    m_ok[m] = j < p.n1;")
-    K.append("  }")
-    for f in spec.fields:
-        if f.staged:
-            K.append(f"  const unsigned int ob{f.slot} = ((tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc})"
-                     f" * {ESIZE[f.dtype]};")
-    for ri, r in enumerate(reds):
-        if r.red == "integrate":
-            sm = 1 if r.method == "simpson" else 0
-            K.append(f"  double rv{ri}_wj[VPT], rv{ri}_wk[KV];")
-            K.append(f"  #pragma unroll\n  for (int m = 0; m < VPT; ++m) rv{ri}_wj[m] = sten_simpson_w(tj0 + tjb + m, p.n1, {r.dx[1]!r}, {sm});")
-            K.append(f"  #pragma unroll\n  for (int q = 0; q < KV; ++q) rv{ri}_wk[q] = sten_simpson_w(kt0 + q, p.n2, {r.dx[2]!r}, {sm});")
-    K.append("  const size_t col = (size_t)(tj0 + tjb) * p.n2 + kt0;")
-    K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
-    K.append("  const size_t out_base = (size_t)p.out_lo * plane_n;")
-    K.append("  int sb = 0;  // ring slot of plane i - RAD, rotated each plane")
-    K.append("  for (int i = ib; i < ie; ++i) {")
-    K.append("    const int gi = i + p.i_base;")
-    K.append("    int sslot[2 * RAD + 1];")
-    K.append("    #pragma unroll")
-    K.append("    for (int d = 0; d < 2 * RAD + 1; ++d) { const int t_ = sb + d; sslot[d] = t_ >= NSLOT ? t_ - NSLOT : t_; }")
-    for f in spec.fields:
-        if f.staged:
-            K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD + 1; ++d) "
-                     f"x.sb{f.slot}[d] = {rings[f.slot]}u + (unsigned)sslot[d] * {plane_bytes(spec, f)}u + ob{f.slot};")
-    if ghost and spec.i_periodic:
-        K.append("    const bool i_in = true;")
-    else:
-        K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
-    K.append("    const size_t pbase = (size_t)i * plane_n + col;")
-    for ri, r in enumerate(reds):
-        if r.red == "integrate":
-            sm = 1 if r.method == "simpson" else 0
-            K.append(f"    const double rv{ri}_wi = sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm});")
-    if split:
-        K.append("    if (i_in) {")
-    # KV-wide stores for single-component outputs
-    vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1 and kvn > 1
-                and r.out_dtype in ("f32", "f16", "bf16")]
-    for m in range(vpt):
-        K.append(f"    if (m_ok[{m}]) {{")
-        K.append(f"      const int j = tj0 + tjb + {m};")
-        K.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
-        K.append(f"      float rvk[KV][{nroot}];")
-        for kk in range(kvn):
-            K.append(f"      if (k_ok[{kk}]) {{")
-            K.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
-            K.append(f"        const size_t vox = rowvox + {kk};")
-            K.append(f"        float* rv = rvk[{kk}];")
-            for f in spec.fields:
-                if not f.staged:
-                    ct = CTYPE[f.dtype]
-                    K.append(f"        x.gp{f.slot} = (const {ct}*)p.fld[{f.slot}] + vox * {f.nc};")
-            if split or R == 0:
-                K.append(f"        eval_fast<{m}, {kk}>(x, rv);")
+        if staged:
+            K.append("  auto request = [&](int q) {")
+            K.append("    const int s = (q - p_first) % NSLOT;")
+            if ghost and spec.i_periodic:
+                K.append("    const int zq = (q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q;")
             else:
-                K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-                K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
-            K += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk)]
-            K.append("      }")
-        for r in vec_outs:
-            ct = CTYPE[r.out_dtype]
-            off = e.offsets[spec.roots.index(r)]
-            vals = ", ".join(f"rvk[{q}][{off}]" for q in range(kvn))
-            K.append(f"      {{ {ct}* o_ = ({ct}*)p.out[{r.out_slot}] + (rowvox - out_base);")
-            K.append(f"        if (k_all && ((rowvox - out_base) & (KV - 1)) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
-            K.append("        else {")
-            for q in range(kvn):
-                K.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, rvk[{q}][{off}]);")
-            K.append("        }")
-            K.append("      }")
-        K.append("    }")
-    if split:
-        K.append("    }")
-    # the next plane (i+1+RAD) must be resident and ghosted before the barrier
-    if tma_fields or (ghost and staged):
-        K.append("    if (i + 1 < ie) {")
+                K.append("    const int zq = q;")
+            if tma_fields:
+                K.append("    if (tid == 0) {")
+                K.append("      fence_proxy_async();")
+                K.append(f"      unsigned int bytes_ = {tma_bytes}u;")
+                for f in tma_fields:
+                    (kw, kh), (jw, jh) = strip_boxes(spec, f)
+                    es = ESIZE[f.dtype]
+                    if f.wrap_k:
+                        K.append(f"      if (tk0 == 0) bytes_ += {kw * kh * es}u;")
+                        K.append(f"      if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
+                    if f.wrap_j:
+                        K.append(f"      if (tj0 == 0) bytes_ += {jw * jh * es}u;")
+                        K.append(f"      if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
+                K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
+                for f in tma_fields:
+                    base = f"smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}"
+                    lay = slot_layout(spec, f)
+                    hk = spec.hk(f)
+                    K.append(f"      tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
+                             f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
+                    if f.wrap_k:
+                        ti = tidx[(f.slot, "kstrip")]
+                        K.append(f"      if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
+                                 f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
+                        K.append(f"      if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
+                                 f"0, tj0, zq);")
+                    if f.wrap_j:
+                        ti = tidx[(f.slot, "jstrip")]
+                        K.append(f"      if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
+                                 f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
+                        K.append(f"      if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
+                                 f"(tk0 - {hk}) * {f.nc}, 0, zq);")
+                K.append("    }")
+            for f in lsu_fields:
+                w, h = spec.box(f)
+                ct = CTYPE[f.dtype]
+                rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+                rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
+                hk = spec.hk(f)
+                et = -(-(w * h) // cfg.threads)
+                K.append("    {")
+                K.append(f"      {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
+                K.append(f"      const {ct}* src = (const {ct}*)p.fld[{f.slot}];")
+                # tile box inside the field: plain row-offset loads, issued in groups of 8
+                # before their shared-memory stores (one memory latency per group)
+                K.append(f"      if (zq >= 0 && zq < p.nl && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && "
+                         f"tk0 >= {hk} && tk0 + TK + {hk} <= p.n2) {{")
+                K.append(f"        const {ct}* rowp = src + (((size_t)zq * p.n1 + (tj0 - {f.halo})) * p.n2 + (tk0 - {hk})) * {f.nc};")
+                K.append(f"        const int pitch = p.n2 * {f.nc};")
+                gsz = 4
+                K.append(f"        #pragma unroll 1\n        for (int t0 = 0; t0 < {et}; t0 += {gsz}) {{")
+                K.append(f"          {ct} v_[{gsz}];")
+                K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
+                         f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (yy * pitch + (e - yy * {w}))); }} }}")
+                K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
+                         f" if (e < {w * h}) dst[e] = v_[t]; }}")
+                K.append("        }")
+                K.append("      } else")
+                K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
+                K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
+                K.append(f"        int jg = tj0 - {f.halo} + yy;")
+                K.append(f"        const int xr = xx - {spec.hk(f)} * {f.nc};")
+                K.append(f"        int kg = tk0 + (xr >= 0 ? xr / {f.nc} : -((-xr + {f.nc} - 1) / {f.nc}));")
+                K.append(f"        const int c = xr - (kg - tk0) * {f.nc};")
+                for ax, var, n, rule in ((1, "jg", "p.n1", rj), (2, "kg", "p.n2", rk)):
+                    if rule == "periodic":
+                        K.append(f"        {var} = wrap_idx({var}, {n});")
+                    elif rule == "replicate":
+                        K.append(f"        {var} = clamp_idx({var}, {n});")
+                    elif rule == "reflect":
+                        K.append(f"        if ({n} > 1) {var} = reflect_idx({var}, {n});")
+                K.append(f"        {ct} v; v.bits = 0;" if ESIZE[f.dtype] == 2 else f"        {ct} v = ({ct})0;")
+                K.append("        if (zq >= 0 && zq < p.nl && jg >= 0 && jg < p.n1 && kg >= 0 && kg < p.n2)")
+                K.append(f"          v = src[(((size_t)zq * p.n1 + jg) * p.n2 + kg) * {f.nc} + c];")
+                K.append("        dst[e] = v;")
+                K.append("      }")
+                K.append("    }")
+            K.append("  };")
+            if ghost:
+                K += ["  " + x for x in _ghost_fill(spec, rings)]
+            K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
+            if lsu_fields:
+                K.append("  __syncthreads();")
+        K.append("  bool ok = true;")
+        # planes p_first .. ib+RAD must be resident (and ghosted) before the first plane
         if tma_fields:
-            K.append("      const int rel = i + 1 + RAD - p_first;")
-            K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+            K.append("  for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) {")
+            K.append("    const int rel = q - p_first;")
+            K.append("    ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+            K.append("  }")
         if ghost and staged:
-            K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
-        K.append("    }")
-    if staged:
-        # the ring slot of plane i - RAD is refilled next: every thread must be done with it
-        K.append("    ok = __syncthreads_and(ok);")
-        K.append("    if (!ok) break;")
-    K.append("    sb = (sb + 1 == NSLOT) ? 0 : sb + 1;")
-    if staged:
-        K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
-    K.append("  }")
-    K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
-    K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
-             % (" false" if batch else ""))
-    K += ["  " + k for k in _red_flush(spec, "cta")]
-    if batch:
-        if tma_fields:
-            # every requested plane was waited on: retire the barriers before the
-            # next item re-initialises this shared memory
+            K.append("  if (edge_cta) { for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) ghost_fill(q); }")
+        if staged:
             K.append("  __syncthreads();")
-            K.append("  if (tid == 0) { for (int s = 0; s < NSLOT; ++s) mbar_inval(&bars[s]); }")
-        K.append("  return true;")
+        # each thread owns KV adjacent columns (kt0 ..) of the tile and VPT consecutive rows;
+        # everything that does not depend on the plane is computed once, before the march
+        kvn = cfg.kv
+        K.append("  const int tk = (tid % TKT) * KV, tjb = (tid / TKT) * VPT;")
+        K.append("  const int kt0 = tk0 + tk;")
+        K.append("  bool k_ok[KV];")
+        K.append("  #pragma unroll")
+        if split and not ghost:
+            K.append("  for (int q = 0; q < KV; ++q) k_ok[q] = kt0 + q >= RAD && kt0 + q < p.n2 - RAD;")
+        else:
+            K.append("  for (int q = 0; q < KV; ++q) k_ok[q] = kt0 + q < p.n2;")
+        K.append("  const bool k_all = " + " && ".join(f"k_ok[{q}]" for q in range(kvn)) + ";")
+        K.append("  bool m_ok[VPT];")
+        K.append("  #pragma unroll")
+        K.append("  for (int m = 0; m < VPT; ++m) {")
+        K.append("    const int j = tj0 + tjb + m;")
+        if split and not ghost:
+            K.append("    m_ok[m] = j >= RAD && j < p.n1 - RAD;")
+        else:
+            K.append("    m_ok[m] = j < p.n1;")
+        K.append("  }")
+        for f in spec.fields:
+            if f.staged:
+                K.append(f"  const unsigned int ob{f.slot} = ((tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc})"
+                         f" * {ESIZE[f.dtype]};")
+        for ri, r in enumerate(reds):
+            if r.red == "integrate":
+                sm = 1 if r.method == "simpson" else 0
+                K.append(f"  double rv{ri}_wj[VPT], rv{ri}_wk[KV];")
+                K.append(f"  #pragma unroll\n  for (int m = 0; m < VPT; ++m) rv{ri}_wj[m] = sten_simpson_w(tj0 + tjb + m, p.n1, {r.dx[1]!r}, {sm});")
+                K.append(f"  #pragma unroll\n  for (int q = 0; q < KV; ++q) rv{ri}_wk[q] = sten_simpson_w(kt0 + q, p.n2, {r.dx[2]!r}, {sm});")
+        K.append("  const size_t col = (size_t)(tj0 + tjb) * p.n2 + kt0;")
+        K.append("  const size_t plane_n = (size_t)p.n1 * p.n2;")
+        K.append("  const size_t out_base = (size_t)p.out_lo * plane_n;")
+        K.append("  int ro_[VPT];  // element offset of row m from row 0")
+        K.append("  #pragma unroll\n  for (int m = 0; m < VPT; ++m) ro_[m] = m * p.n2;")
+        for r in spec.roots:
+            if r.kind in ("out", "scan"):
+                ct, nc = CTYPE[r.out_dtype], e.g.nodes[r.node].nc
+                K.append(f"  {ct}* orow{r.out_slot} = ({ct}*)p.out[{r.out_slot}] + ((size_t)(ib - p.out_lo) * plane_n + col) * {nc};")
+        for f in spec.fields:
+            if not f.staged:
+                K.append(f"  const {CTYPE[f.dtype]}* frow{f.slot} = (const {CTYPE[f.dtype]}*)p.fld[{f.slot}] + "
+                         f"((size_t)ib * plane_n + col) * {f.nc};")
+        # ring slots of planes i-RAD .. i+RAD: shifted by one each plane, the newcomer is
+        # the slot of plane i+RAD+1 (snext)
+        for f in spec.fields:
+            if f.staged:
+                K.append(f"  #pragma unroll\n  for (int d = 0; d < 2 * RAD + 1; ++d) "
+                         f"x.sb{f.slot}[d] = {rings[f.slot]}u + (unsigned)d * {plane_bytes(spec, f)}u + ob{f.slot};")
+        K.append("  int snext = (2 * RAD + 1) % NSLOT;")
+        K.append("  for (int i = ib; i < ie; ++i) {")
+        K.append("    const int gi = i + p.i_base;")
+        if ghost and spec.i_periodic:
+            K.append("    const bool i_in = true;")
+        else:
+            K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
+        K.append("    const size_t pbase = (size_t)i * plane_n + col;")
+        for ri, r in enumerate(reds):
+            if r.red == "integrate":
+                sm = 1 if r.method == "simpson" else 0
+                K.append(f"    const double rv{ri}_wi = sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm});")
+        if split:
+            K.append("    if (i_in) {")
+        # KV-wide stores for single-component outputs
+        vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1 and kvn > 1
+                    and r.out_dtype in ("f32", "f16", "bf16")]
+        for m in range(vpt):
+            K.append(f"    if (m_ok[{m}]) {{")
+            K.append(f"      const int j = tj0 + tjb + {m};")
+            K.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
+            K.append(f"      float rvk[KV][{nroot}];")
+            for kk in range(kvn):
+                K.append(f"      if (k_ok[{kk}]) {{")
+                K.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
+                K.append(f"        const size_t vox = rowvox + {kk};")
+                K.append(f"        float* rv = rvk[{kk}];")
+                for f in spec.fields:
+                    if not f.staged:
+                        K.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
+                if split or R == 0:
+                    K.append(f"        eval_fast<{m}, {kk}>(x, rv);")
+                else:
+                    K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
+                    K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
+                K += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk)]
+                K.append("      }")
+            for r in vec_outs:
+                ct = CTYPE[r.out_dtype]
+                off = e.offsets[spec.roots.index(r)]
+                vals = ", ".join(f"rvk[{q}][{off}]" for q in range(kvn))
+                K.append(f"      {{ {ct}* o_ = orow{r.out_slot} + ro_[{m}];")
+                K.append(f"        if (k_all && (((size_t)o_) & {kvn * ESIZE[r.out_dtype] - 1}) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
+                K.append("        else {")
+                for q in range(kvn):
+                    K.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, rvk[{q}][{off}]);")
+                K.append("        }")
+                K.append("      }")
+            K.append("    }")
+        if split:
+            K.append("    }")
+        for r in spec.roots:
+            if r.kind in ("out", "scan"):
+                K.append(f"    orow{r.out_slot} += plane_n * {e.g.nodes[r.node].nc};")
+        for f in spec.fields:
+            if not f.staged:
+                K.append(f"    frow{f.slot} += plane_n * {f.nc};")
+        # the next plane (i+1+RAD) must be resident and ghosted before the barrier
+        if tma_fields or (ghost and staged):
+            K.append("    if (i + 1 < ie) {")
+            if tma_fields:
+                K.append("      const int rel = i + 1 + RAD - p_first;")
+                K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+            if ghost and staged:
+                K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
+            K.append("    }")
+        if staged:
+            # the ring slot of plane i - RAD is refilled next: every thread must be done with it
+            K.append("    ok = __syncthreads_and(ok);")
+            K.append("    if (!ok) break;")
+        for f in spec.fields:
+            if f.staged:
+                K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD; ++d) x.sb{f.slot}[d] = x.sb{f.slot}[d + 1];")
+                K.append(f"    x.sb{f.slot}[2 * RAD] = {rings[f.slot]}u + (unsigned)snext * {plane_bytes(spec, f)}u + ob{f.slot};")
+        K.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
+        if staged:
+            K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
+        K.append("  }")
+        K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
+        K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
+                 % (" false" if batch else ""))
+        K += ["  " + k for k in _red_flush(spec, "cta")]
+        if batch:
+            if tma_fields:
+                # every requested plane was waited on: retire the barriers before the
+                # next item re-initialises this shared memory
+                K.append("  __syncthreads();")
+                K.append("  if (tid == 0) { for (int s = 0; s < NSLOT; ++s) mbar_inval(&bars[s]); }")
+            K.append("  return true;")
     K.append("}")
 
     if regions:
@@ -1483,7 +1611,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("}")
         K.append(f"}}  // namespace {batch_ns}")
         K.append("#undef TJ\n#undef TK\n#undef NT\n#undef RAD\n#undef NSLOT\n#undef VPT\n#undef NSLOTS_RED"
-                 "\n#undef KV\n#undef TKT")
+                 "\n#undef KV\n#undef TKT\n#undef FV\n#undef FITER")
     return "\n".join(L) + "\n" + "\n".join(K) + "\n"
 
 

@@ -87,6 +87,42 @@ STEN_DEV float chunk_elem(const unsigned char* row) {
     else return f16_bits_to_f32((u16)h);
   }
 }
+// N consecutive elements from global memory (read-only path) as floats: one 16/8/4-byte
+// load per 16/8/4 bytes when the address is aligned to that width (ld_vec_f32), or
+// element by element with the first n valid (ld_part_f32; the rest are zero).
+STEN_DEV void unpack_f32(u32 w, const float*, float* o) { o[0] = __uint_as_float(w); }
+STEN_DEV void unpack_f32(u32 w, const bf16_t*, float* o) {
+  o[0] = __uint_as_float(w << 16); o[1] = __uint_as_float(w & 0xffff0000u);
+}
+STEN_DEV void unpack_f32(u32 w, const f16_t*, float* o) {
+  o[0] = f16_bits_to_f32((u16)(w & 0xffffu)); o[1] = f16_bits_to_f32((u16)(w >> 16));
+}
+template <typename T, int N>
+STEN_DEV void ld_vec_f32(const T* p, float* out) {
+  constexpr int B = N * (int)sizeof(T), PW = 4 / (int)sizeof(T);   // elements per 32-bit word
+  if constexpr (B % 16 == 0) {
+    #pragma unroll
+    for (int q = 0; q < B / 16; ++q) {
+      const uint4 v = __ldg((const uint4*)p + q);
+      unpack_f32(v.x, p, out + (4 * q + 0) * PW); unpack_f32(v.y, p, out + (4 * q + 1) * PW);
+      unpack_f32(v.z, p, out + (4 * q + 2) * PW); unpack_f32(v.w, p, out + (4 * q + 3) * PW);
+    }
+  } else if constexpr (B % 8 == 0) {
+    #pragma unroll
+    for (int q = 0; q < B / 8; ++q) {
+      const uint2 v = __ldg((const uint2*)p + q);
+      unpack_f32(v.x, p, out + (2 * q + 0) * PW); unpack_f32(v.y, p, out + (2 * q + 1) * PW);
+    }
+  } else {
+    #pragma unroll
+    for (int q = 0; q < B / 4; ++q) unpack_f32(__ldg((const u32*)p + q), p, out + q * PW);
+  }
+}
+template <typename T, int N>
+STEN_DEV void ld_part_f32(const T* p, int n, float* out) {
+  #pragma unroll
+  for (int q = 0; q < N; ++q) out[q] = q < n ? ldg_as_f32(p + q) : 0.0f;
+}
 // KV consecutive values to a (KV x element size)-aligned global address.
 STEN_DEV u32 pack2(const f16_t*, float lo, float hi) {
   u32 w; asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(hi), "f"(lo)); return w;

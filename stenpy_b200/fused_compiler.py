@@ -34,7 +34,7 @@ import torch
 
 from . import _native as N
 from .codegen import (ESIZE, SHELL_THREADS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec, analyse_ghosts,
-                      emit_pass, param_layout, shell_count, shell_regions, smem_layout, tmap_specs)
+                      emit_pass, param_layout, pass_grid, shell_count, shell_regions, smem_layout, tmap_specs)
 from .graph import Graph
 from .lowering import LoweringError, OpLowerer, dx3
 from .registry import KNOWN_OPS
@@ -376,6 +376,8 @@ class Planner:
             es = ESIZE[f.dtype]
             f.tma = (n2 * f.nc * es) % 16 == 0 and (w * es) % 16 == 0 and w <= 256 and h <= 256
             f.staged = f.tma or f.slot in offset_read
+            if radius == 0 and not has_scan:
+                f.tma = f.staged = False     # flat pass: vector loads straight from HBM
         if self.ghosts:
             analyse_ghosts(spec)
         return PassPlan(spec, field_nodes, out_nodes, reductions, hists)
@@ -602,9 +604,8 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
         spec = pp.spec
         cfg = spec.cfg
         tiles_k = -(-n2 // cfg.tk)
-        tiles_j = -(-n1 // cfg.tj)
-        nseg = -(-n0 // cfg.seg_len)
-        grid = (tiles_j * tiles_k, nseg, 1)
+        gx, gy = pass_grid(spec, n1, n2, n0)
+        grid = (gx, gy, 1)
         ncta = grid[0] * grid[1]
         fptrs: List[int] = []
         for f, nid in zip(spec.fields, pp.field_nodes):

@@ -32,7 +32,7 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import SHELL_THREADS, PassConfig, shell_count, shell_regions
+from .codegen import SHELL_THREADS, PassConfig, pass_grid, shell_count, shell_regions
 from .graph import Graph
 
 
@@ -170,8 +170,8 @@ class LazyPipeline:
             for ci, c in enumerate(chunks):
                 b = ci % 2
                 n_out = c.e - c.s
-                nseg = -(-n_out // cfg.seg_len)
-                grid = (tiles_j * tiles_k, nseg, 1)
+                gx, gy = pass_grid(spec, self.n1, self.n2, n_out)
+                grid = (gx, gy, 1)
                 nl = c.hi - c.lo
                 fptrs = [bufs[b].data_ptr() for bufs in slabs]
                 tmaps = FC.encode_tmaps(spec, fptrs, nl, self.n1, self.n2)

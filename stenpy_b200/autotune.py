@@ -55,13 +55,23 @@ def _valid(spec: PassSpec, cfg: PassConfig) -> bool:
     return total <= SMEM_LIMIT and 2 * spec.radius + 1 + cfg.prefetch <= 16
 
 
+def default_kv(spec: PassSpec) -> int:
+    """Two k-adjacent voxels per thread for interleaved 3-component 16-bit fields: a
+    thread's 12-byte chunk makes consecutive threads' shared-memory reads
+    conflict-free (6-byte voxels put every other thread on a shared bank)."""
+    return 2 if any(f.nc == 3 and ESIZE[f.dtype] == 2 for f in spec.fields) else 1
+
+
 def candidates(spec: PassSpec) -> List[PassConfig]:
     out = []
     uses_ghost = with_config(spec, dataclasses.replace(spec.cfg, ghost=True)).ghosts is not None
+    kv = default_kv(spec)
     for tk, nt, vpt in _SHAPES:
         for seg in _SEGS:
             for gh in (_GHOST if uses_ghost else (True,)):
-                cfg = PassConfig(tj=(nt // tk) * vpt, tk=tk, threads=nt, prefetch=2, seg_len=seg, ghost=gh)
+                cfg = PassConfig(tj=(nt // tk) * vpt, tk=tk, threads=nt, prefetch=2, seg_len=seg, ghost=gh, kv=kv)
+                if not valid_shape(cfg):
+                    cfg.kv = 1
                 if spec.has_scan:
                     cfg.seg_len = spec.cfg.seg_len
                 if _valid(spec, cfg):
@@ -125,7 +135,11 @@ def _launches(pp: FC.PassPlan, spec: PassSpec, values: Dict[str, Any], shape, de
     outs = []
     for (nid, kind, nc), r in zip(pp.out_nodes, [r for r in spec.roots if r.kind in ("out", "scan")]):
         outs.append(torch.empty((n0, n1, n2) + FC.comp_shape(nc), dtype=FC.DT_TORCH[r.out_dtype], device=device))
-    vals = dict(fld=fptrs, out=[o.data_ptr() for o in outs], scal=table.data_ptr(), part=part.data_ptr(), hist=0,
+    nbins = max([r.slot + r.bins for r in spec.roots if r.kind == "red" and r.red == "hist"] + [0])
+    hist = torch.zeros(max(nbins, 1), dtype=torch.int64, device=device)
+    outs.append(hist)   # keeps the histogram buffer alive with the launches
+    vals = dict(fld=fptrs, out=[o.data_ptr() for o in outs[:-1]], scal=table.data_ptr(), part=part.data_ptr(),
+                hist=hist.data_ptr(),
                 err=err.data_ptr(), n0g=n0, n1=n1, n2=n2, nl=n0, i_base=0, out_lo=0, n_out=n0,
                 seg_len=cfg.seg_len, tiles_k=tiles_k, cta_off=0)
     ls = [(grid, (cfg.threads, 1, 1), FC.pack_params(spec, vals, tmaps))]

@@ -1465,35 +1465,47 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         # KV-wide stores for single-component outputs
         vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1 and kvn > 1
                     and r.out_dtype in ("f32", "f16", "bf16")]
+        # all voxels of the plane first, stores and accumulation after: with every field
+        # staged the reads stay inside the ring even for voxels beyond the grid, so the
+        # evaluation is unconditional and taps shared by neighbouring voxels load once
+        eager = (split or R == 0) and all(f.staged for f in spec.fields)
+        if eager:
+            K.append(f"    float rvk[VPT][KV][{nroot}];")
+            for m in range(vpt):
+                for kk in range(kvn):
+                    K.append(f"    eval_fast<{m}, {kk}>(x, rvk[{m}][{kk}]);")
         for m in range(vpt):
             K.append(f"    if (m_ok[{m}]) {{")
             K.append(f"      const int j = tj0 + tjb + {m};")
             K.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
-            K.append(f"      float rvk[KV][{nroot}];")
+            if not eager:
+                K.append(f"      float rvm[KV][{nroot}];")
+            arr = f"rvk[{m}]" if eager else "rvm"
             for kk in range(kvn):
                 K.append(f"      if (k_ok[{kk}]) {{")
                 K.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
                 K.append(f"        const size_t vox = rowvox + {kk};")
-                K.append(f"        float* rv = rvk[{kk}];")
-                for f in spec.fields:
-                    if not f.staged:
-                        K.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
-                if split or R == 0:
-                    K.append(f"        eval_fast<{m}, {kk}>(x, rv);")
-                else:
-                    K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-                    K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
+                K.append(f"        float* rv = {arr}[{kk}];")
+                if not eager:
+                    for f in spec.fields:
+                        if not f.staged:
+                            K.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
+                    if split or R == 0:
+                        K.append(f"        eval_fast<{m}, {kk}>(x, rv);")
+                    else:
+                        K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
+                        K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
                 K += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk)]
                 K.append("      }")
             for r in vec_outs:
                 ct = CTYPE[r.out_dtype]
                 off = e.offsets[spec.roots.index(r)]
-                vals = ", ".join(f"rvk[{q}][{off}]" for q in range(kvn))
+                vals = ", ".join(f"{arr}[{q}][{off}]" for q in range(kvn))
                 K.append(f"      {{ {ct}* o_ = orow{r.out_slot} + ro_[{m}];")
                 K.append(f"        if (k_all && (((size_t)o_) & {kvn * ESIZE[r.out_dtype] - 1}) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
                 K.append("        else {")
                 for q in range(kvn):
-                    K.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, rvk[{q}][{off}]);")
+                    K.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, {arr}[{q}][{off}]);")
                 K.append("        }")
                 K.append("      }")
             K.append("    }")

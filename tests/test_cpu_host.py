@@ -238,3 +238,27 @@ def test_batch_queue_check_rejects_bad_items():
                 torch.cat([items[:-1], torch.tensor([[0, 1, 0, 1]], dtype=torch.int32)])):
         with pytest.raises(ValueError):
             check_queue(bad, ph)
+
+
+def test_cost_model_fixture_and_baselines_without_gpu():
+    """The timing fixture is well formed and the model-free baselines evaluate on it
+    (the learned model itself trains with GPU kernels, see the GPU tests)."""
+    import gzip
+    import json
+    from stenpy_b200 import costmodel as CM
+    path = os.path.join(REPO, "tests", "golden", "autotune_timings.jsonl.gz")
+    with gzip.open(path, "rt") as fh:
+        recs = [json.loads(line) for line in fh]
+    hold = [r for r in recs if r["tag"].startswith("cm-hold")]
+    assert hold and any(r["tag"].startswith("cm-train") for r in recs)
+    X, y = CM.records_to_xy(recs[:50])
+    assert X.shape[0] == 50 and torch.isfinite(X).all() and torch.isfinite(y).all()
+    yc = CM.centred_targets(hold)
+    assert abs(float(yc.sum())) < 1e-3 * len(hold)   # centred per pass
+
+    class Zero:
+        def predict(self, X):
+            return torch.zeros(X.shape[0], dtype=torch.float64)
+
+    ev = CM.evaluate(Zero(), hold, k=3)
+    assert ev["passes"] > 10 and 0.0 <= ev["analytic_topk"]["mean"] < ev["random_topk"]["mean"] + 0.1

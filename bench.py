@@ -652,9 +652,9 @@ def main():
     ap.add_argument("--tune-log", default="")
     ap.add_argument("--schedule", default="", help="JSON PassConfig for every pass (no autotuning), "
                                                     "e.g. '{\"tj\": 16, \"tk\": 32, \"seg_len\": 32}'")
-    ap.add_argument("--dags", type=int, default=300)
-    ap.add_argument("--heldout", type=int, default=60)
-    ap.add_argument("--train-cands", type=int, default=6)
+    ap.add_argument("--dags", type=int, default=2000)
+    ap.add_argument("--heldout", type=int, default=200)
+    ap.add_argument("--train-cands", type=int, default=8)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--ensemble", type=int, default=5)
     ap.add_argument("--seed", type=int, default=0)

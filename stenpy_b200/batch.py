@@ -63,6 +63,10 @@ def batch_candidates(threads: Optional[int] = None) -> List[PassConfig]:
     return out
 
 
+def batch_min_blocks(threads: int) -> int:
+    return max(1, 512 // threads)
+
+
 def program_key(spec: PassSpec) -> str:
     return hashlib.sha1(emit_pass(spec).encode()).hexdigest()[:20]
 
@@ -113,7 +117,11 @@ def group_key(job: BatchJob, threads: int = 128) -> str:
 class BatchModule:
     """The compiled batch kernel for a set of pass programs (one block size)."""
 
-    def __init__(self, specs: Sequence[PassSpec], threads: int, device: torch.device, min_blocks: int = 1):
+    def __init__(self, specs: Sequence[PassSpec], threads: int, device: torch.device,
+                 min_blocks: Optional[int] = None):
+        # at most 128 registers a thread: the kernel's register count is the maximum
+        # over all of its programs, so the heaviest would otherwise set the occupancy
+        min_blocks = min_blocks or batch_min_blocks(threads)
         self.threads = threads
         self.keys: List[str] = []
         self.index: Dict[str, int] = {}
@@ -393,7 +401,7 @@ def _as_jobs(jobs: Sequence[Any]) -> List[BatchJob]:
 
 
 def build(jobs: Sequence[Any], device: Any = "cuda", configs: Optional[Dict[str, PassConfig]] = None,
-          threads: int = 128, min_blocks: int = 1) -> BatchProgram:
+          threads: int = 128, min_blocks: Optional[int] = None) -> BatchProgram:
     """Plan, compile and resolve a batch. ``configs`` maps group keys (``group_key``)
     to schedules; groups without an entry use the first candidate of ``threads``."""
     device = torch.device(device)

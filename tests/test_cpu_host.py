@@ -196,7 +196,7 @@ def test_batch_module_compiles_for_sm100a(threads):
                 seen.add(k)
                 specs.append(pp.spec)
     assert len(specs) >= 16          # 8 expressions x 2 dtypes (+ the entropy min/max passes)
-    key, cubin = N.compile_cached(emit_batch_module(specs, threads), FC.NVRTC_OPTS)
+    key, cubin = N.compile_cached(emit_batch_module(specs, threads, B.batch_min_blocks(threads)), FC.NVRTC_OPTS)
     assert len(cubin) > 10000
     # job outputs follow the storage dtype of the job's field
     assert {j.out_dtype for j in jobs} == {torch.float32, torch.bfloat16}

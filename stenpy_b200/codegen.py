@@ -132,6 +132,7 @@ class PassSpec:
     # ghost-cell mode: {(field slot, axis): rule}; None when some stencil is nested
     ghosts: Optional[Dict[Tuple[int, int], str]] = None
     i_periodic: bool = False   # every tap along dim 0 wraps: planes are loaded wrapped
+    nested_ok: bool = False    # dims 1 and 2 have >= 4 points (two-layer extrapolation)
 
     def hk(self, f: FieldSpec) -> int:
         """k-halo in elements, rounded so TMA x-coordinates stay 16-byte aligned."""
@@ -177,19 +178,33 @@ def analyse_ghosts(spec: "PassSpec") -> None:
 
     rules: Dict[Tuple[int, int], str] = {}
     i_periodic = True
+
+    def second_derivative(n) -> bool:
+        """d1(d1(field, a), a), both with edge order 2: reproduced by two ghost layers."""
+        inner = g.nodes[n.ins[0]]
+        return (spec.nested_ok and n.op == "d1" and n.a("mode") == "edge2" and inner.op == "d1"
+                and inner.a("mode") == "edge2" and inner.a("axis") == n.a("axis")
+                and g.nodes[inner.ins[0]].op == "field")
+
+    live: set = set()
+    for r in spec.roots:
+        subtree(r.node, live)
     for n in g.nodes:
-        if n.op not in ("d1", "lap"):
+        if n.op not in ("d1", "lap") or n.id not in live:
             continue
         sub = subtree(n.ins[0], set())
-        if any(g.nodes[x].op in ("d1", "lap") for x in sub):
+        nested = any(g.nodes[x].op in ("d1", "lap") for x in sub)
+        if nested and not second_derivative(n):
             return
-        direct = g.nodes[n.ins[0]].op == "field"
+        direct = g.nodes[n.ins[0]].op == "field" or nested
         if n.op == "lap":
             rule, axes = n.a("pad"), (0, 1, 2)
         else:
             rule, axes = n.a("mode"), (n.a("axis"),)
             if rule == "zero":
                 continue
+            if nested:
+                rule = "edge2x2"
         if rule not in _REMAP_RULES and not direct:
             return
         for x in sub:
@@ -197,7 +212,12 @@ def analyse_ghosts(spec: "PassSpec") -> None:
                 continue
             slot = g.nodes[x].a("field")
             for ax in axes:
-                if rules.setdefault((slot, ax), rule) != rule:
+                have = rules.setdefault((slot, ax), rule)
+                if have != rule:
+                    # the two-layer rule's first layer is the edge-order-2 ghost
+                    if {have, rule} == {"edge2", "edge2x2"}:
+                        rules[(slot, ax)] = "edge2x2"
+                        continue
                     return
                 if ax == 0 and rule != "periodic":
                     i_periodic = False
@@ -274,10 +294,18 @@ class _Emitter:
         self.R = spec.radius
         self.lines: List[str] = []
         self.tmp = 0
-        # which nodes need offset (fast) / point (slow) functions
+        # which nodes need offset (fast) / point (slow) functions (live nodes only:
+        # lowering may leave unused components behind)
+        live: set = set()
+        stack = [r.node for r in spec.roots]
+        while stack:
+            x = stack.pop()
+            if x not in live:
+                live.add(x)
+                stack += list(self.g.nodes[x].ins)
         self.need_fn = set()
         for n in self.g.nodes:
-            if n.op in ("d1", "lap"):
+            if n.op in ("d1", "lap") and n.id in live:
                 self._mark(n.ins[0])
 
     def _mark(self, nid: int) -> None:
@@ -953,9 +981,22 @@ def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
     return K
 
 
+def _ghost_expr2(at, n: str, side: str) -> str:
+    """Second ghost layer of a second derivative with edge order 2 on both levels:
+    f[-2] = 7f0 - 11f1 + 6f2 - f3 makes the inner central difference at -1 equal
+    3g0 - 3g1 + g2 (g the inner derivative), so the outer central difference at 0 is
+    torch.gradient's one-sided (-3g0 + 4g1 - g2)/2h of the one-sided inner values."""
+    if side == "lo":
+        return f"(7.0f * {at('0')} - 11.0f * {at('1')} + 6.0f * {at('2')} - {at('3')})"
+    return (f"(7.0f * {at(n + ' - 1')} - 11.0f * {at(n + ' - 2')} + 6.0f * {at(n + ' - 3')}"
+            f" - {at(n + ' - 4')})")
+
+
 def _ghost_expr(rule: str, at, n: str, side: str) -> Optional[str]:
     """Ghost value next to a face for ``rule``; ``at(idx)`` reads the field at an
     in-domain index along the axis (fp32). None: nothing to write."""
+    if rule == "edge2x2":
+        rule = "edge2"
     if side == "lo":
         v = {"replicate": f"{at('0')}",
              "reflect": f"({n} > 1 ? {at('1')} : 0.0f)",
@@ -999,45 +1040,58 @@ def _ghost_fill(spec: PassSpec, rings: Dict[int, int]) -> List[str]:
         K.append(f"    unsigned char* slot_ = smem + {rings[f.slot]} + s * {plane_bytes(spec, f)};")
         K.append(f"    {ct}* dst = ({ct}*)slot_;")
         if todo_k:
-            for side, cond, col in (("lo", "tk0 == 0", f"{hk} - 1"), ("hi", "tk0 + TK >= p.n2", f"p.n2 - tk0 + {hk}")):
-                K.append(f"    if ({cond}) for (int e = tid; e < TJ * {nc}; e += NT) {{")
-                K.append(f"      const int yy = e / {nc}, c = e - yy * {nc};")
-                K.append("      if (tj0 + yy < p.n1) {")
-                if rk == "periodic":
-                    buf = "kl" if side == "lo" else "kr"
-                    scol = f"{hk} - 1" if side == "lo" else "0"
-                    K.append(f"        const {ct}* st = ({ct}*)(slot_ + {lay[buf]});")
-                    K.append(f"        dst[(yy + {f.halo}) * {w} + ({col}) * {nc} + c] = st[yy * {kw} + ({scol}) * {nc} + c];")
-                else:
-                    rowp = f"dst + (yy + {f.halo}) * {w}"
-                    expr = _ghost_expr(rk, lambda ix: f"ld_as_f32({rowp} + (({ix}) - tk0 + {hk}) * {nc} + c)", "p.n2", side)
-                    K.append(f"        st_from_f32(dst + (yy + {f.halo}) * {w} + ({col}) * {nc} + c, {expr});")
-                K.append("      }")
-                K.append("    }")
-        if todo_j:
-            for side, cond, row in (("lo", "tj0 == 0", f"{f.halo} - 1"), ("hi", "tj0 + TJ >= p.n1", f"p.n1 - tj0 + {f.halo}")):
-                K.append(f"    if ({cond}) for (int e = tid; e < TK * {nc}; e += NT) {{")
-                K.append(f"      const int xx = e / {nc}, c = e - xx * {nc};")
-                K.append("      if (tk0 + xx < p.n2) {")
-                if rj == "periodic":
-                    buf = "jt" if side == "lo" else "jb"
-                    srow = f"{f.halo} - 1" if side == "lo" else "0"
-                    K.append(f"        const {ct}* st = ({ct}*)(slot_ + {lay[buf]});")
-                    K.append(f"        dst[({row}) * {w} + (xx + {hk}) * {nc} + c] = st[({srow}) * {jw} + (xx + {hk}) * {nc} + c];")
-                else:
-                    def at_s(ix, f=f, w=w, hk=hk, nc=nc):
-                        return f"ld_as_f32(dst + (({ix}) - tj0 + {f.halo}) * {w} + (xx + {hk}) * {nc} + c)"
+            layers = 2 if rk == "edge2x2" else 1
+            for layer in range(1, layers + 1):
+                for side, cond, col in (("lo", "tk0 == 0", f"{hk} - {layer}"),
+                                        ("hi", "tk0 + TK >= p.n2", f"p.n2 - tk0 + {hk} + {layer - 1}")):
+                    K.append(f"    if ({cond}) for (int e = tid; e < TJ * {nc}; e += NT) {{")
+                    K.append(f"      const int yy = e / {nc}, c = e - yy * {nc};")
+                    K.append("      if (tj0 + yy < p.n1) {")
+                    if rk == "periodic":
+                        buf = "kl" if side == "lo" else "kr"
+                        scol = f"{hk} - 1" if side == "lo" else "0"
+                        K.append(f"        const {ct}* st = ({ct}*)(slot_ + {lay[buf]});")
+                        K.append(f"        dst[(yy + {f.halo}) * {w} + ({col}) * {nc} + c] = st[yy * {kw} + ({scol}) * {nc} + c];")
+                    else:
+                        rowp = f"dst + (yy + {f.halo}) * {w}"
 
-                    def at_g(ix, ct=ct, nc=nc, f=f):
-                        return (f"ldg_as_f32((const {ct}*)p.fld[{f.slot}] + (((size_t)zq * p.n1 + ({ix})) * p.n2"
-                                f" + tk0 + xx) * {nc} + c)")
-                    es_ = _ghost_expr(rj, at_s, "p.n1", side)
-                    if side == "hi":
-                        eg_ = _ghost_expr(rj, at_g, "p.n1", side)
-                        es_ = f"((p.n1 - tj0 >= 3 - {f.halo}) ? {es_} : {eg_})"
-                    K.append(f"        st_from_f32(dst + ({row}) * {w} + (xx + {hk}) * {nc} + c, {es_});")
-                K.append("      }")
-                K.append("    }")
+                        def at_k(ix, rowp=rowp, hk=hk, nc=nc):
+                            return f"ld_as_f32({rowp} + (({ix}) - tk0 + {hk}) * {nc} + c)"
+                        expr = (_ghost_expr(rk, at_k, "p.n2", side) if layer == 1 else
+                                _ghost_expr2(at_k, "p.n2", side))
+                        K.append(f"        st_from_f32(dst + (yy + {f.halo}) * {w} + ({col}) * {nc} + c, {expr});")
+                    K.append("      }")
+                    K.append("    }")
+        if todo_j:
+            layers = 2 if rj == "edge2x2" else 1
+            for layer in range(1, layers + 1):
+                for side, cond, row in (("lo", "tj0 == 0", f"{f.halo} - {layer}"),
+                                        ("hi", "tj0 + TJ >= p.n1", f"p.n1 - tj0 + {f.halo} + {layer - 1}")):
+                    K.append(f"    if ({cond}) for (int e = tid; e < TK * {nc}; e += NT) {{")
+                    K.append(f"      const int xx = e / {nc}, c = e - xx * {nc};")
+                    K.append("      if (tk0 + xx < p.n2) {")
+                    if rj == "periodic":
+                        buf = "jt" if side == "lo" else "jb"
+                        srow = f"{f.halo} - 1" if side == "lo" else "0"
+                        K.append(f"        const {ct}* st = ({ct}*)(slot_ + {lay[buf]});")
+                        K.append(f"        dst[({row}) * {w} + (xx + {hk}) * {nc} + c] = st[({srow}) * {jw} + (xx + {hk}) * {nc} + c];")
+                    else:
+                        def at_s(ix, f=f, w=w, hk=hk, nc=nc):
+                            return f"ld_as_f32(dst + (({ix}) - tj0 + {f.halo}) * {w} + (xx + {hk}) * {nc} + c)"
+
+                        def at_g(ix, ct=ct, nc=nc, f=f):
+                            return (f"ldg_as_f32((const {ct}*)p.fld[{f.slot}] + (((size_t)zq * p.n1 + ({ix})) * p.n2"
+                                    f" + tk0 + xx) * {nc} + c)")
+                        mk = (lambda at, side=side: _ghost_expr(rj, at, "p.n1", side)) if layer == 1 else \
+                             (lambda at, side=side: _ghost_expr2(at, "p.n1", side))
+                        es_ = mk(at_s)
+                        if side == "hi":
+                            # the rows n1-1 .. n1-need may lie above a thin last tile: read them globally
+                            need = 3 if layer == 1 else 4
+                            es_ = f"((p.n1 - tj0 >= {need} - {f.halo}) ? {es_} : {mk(at_g)})"
+                        K.append(f"        st_from_f32(dst + ({row}) * {w} + (xx + {hk}) * {nc} + c, {es_});")
+                    K.append("      }")
+                    K.append("    }")
         K.append("  }")
     K.append("};")
     return K

@@ -367,6 +367,7 @@ class Planner:
             cfg.seg_len = self.shape[0]
         cfg.prefetch = max(cfg.prefetch, 1)
         spec = PassSpec(pg, fields, rspecs, self.table_size, max(nslots, 1), radius, cfg, has_scan)
+        spec.nested_ok = self.shape[1] >= 4 and self.shape[2] >= 4
         n2 = self.shape[2]
         for f in fields:
             # every field goes through a TMA-filled plane ring when the layout allows;

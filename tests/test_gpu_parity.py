@@ -64,7 +64,7 @@ def test_ragged_shapes_against_oracle(shape, boundary):
     gg = uniform_field(shape, seed=12)
     exprs = ["laplacian(f) + tanh(g)*exp(f)", "gradient(f)"]
     if min(shape) >= 3:
-        exprs += ["_hessian(f)", "mean_curvature(g*g + 1)"]
+        exprs += ["_hessian(f)", "mean_curvature(g*g + 1)", "trace(_hessian(f)) + tanh(g)"]
     for expr in exprs:
         g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map={"f": f.to(dev), "g": gg.to(dev)})
         got = S.Runtime(device=dev).run(g)[sink]

@@ -133,12 +133,8 @@ def _barrier(world):
 
 
 def _max_over_ranks(x: float, world: int, dev) -> float:
-    if world == 1:
-        return x
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=dev)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from stenpy_b200.replicas import max_over_ranks
+    return max_over_ranks(x, world)
 
 
 def make_fields(size, device):

@@ -1302,6 +1302,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     L.append(_simpson_fn())
     tma_fields = [f for f in spec.fields if f.tma]
     lsu_fields = [f for f in spec.fields if f.staged and not f.tma]
+    # cooperative staging of 4-byte fields is asynchronous: one commit group per plane
+    async_lsu = any(ESIZE[f.dtype] == 4 for f in lsu_fields)
     total_smem, rings, red_off = smem_layout(spec)
     tma_bytes = sum(spec.box(f)[0] * spec.box(f)[1] * ESIZE[f.dtype] for f in tma_fields)
     reds = [r for r in spec.roots if r.kind == "red"]
@@ -1407,14 +1409,21 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                          f"tk0 >= {hk} && tk0 + TK + {hk} <= p.n2) {{")
                 K.append(f"        const {ct}* rowp = src + (((size_t)zq * p.n1 + (tj0 - {f.halo})) * p.n2 + (tk0 - {hk})) * {f.nc};")
                 K.append(f"        const int pitch = p.n2 * {f.nc};")
-                gsz = 4
-                K.append(f"        #pragma unroll 1\n        for (int t0 = 0; t0 < {et}; t0 += {gsz}) {{")
-                K.append(f"          {ct} v_[{gsz}];")
-                K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
-                         f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (yy * pitch + (e - yy * {w}))); }} }}")
-                K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
-                         f" if (e < {w * h}) dst[e] = v_[t]; }}")
-                K.append("        }")
+                if ESIZE[f.dtype] == 4:
+                    # 4-byte elements: asynchronous copies, completed by the wait before the
+                    # barrier that precedes the plane's first use (like the TMA ring)
+                    K.append(f"        #pragma unroll 4\n        for (int e = tid; e < {w * h}; e += NT) {{")
+                    K.append(f"          const int yy = e / {w}; cp_async4(dst + e, rowp + (yy * pitch + (e - yy * {w})));")
+                    K.append("        }")
+                else:
+                    gsz = 4
+                    K.append(f"        #pragma unroll 1\n        for (int t0 = 0; t0 < {et}; t0 += {gsz}) {{")
+                    K.append(f"          {ct} v_[{gsz}];")
+                    K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
+                             f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (yy * pitch + (e - yy * {w}))); }} }}")
+                    K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
+                             f" if (e < {w * h}) dst[e] = v_[t]; }}")
+                    K.append("        }")
                 K.append("      } else")
                 K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
                 K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
@@ -1438,7 +1447,11 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             K.append("  };")
             if ghost:
                 K += ["  " + x for x in _ghost_fill(spec, rings)]
-            K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
+            if async_lsu:
+                K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) { request(q); cp_async_commit(); }")
+                K.append("  cp_async_wait<0>();")
+            else:
+                K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
             if lsu_fields:
                 K.append("  __syncthreads();")
         K.append("  bool ok = true;")
@@ -1580,6 +1593,9 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             if ghost and staged:
                 K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
             K.append("    }")
+        if async_lsu:
+            # this thread's copies of plane i+1+RAD (issued PREFETCH iterations ago) are done
+            K.append(f"    cp_async_wait<{cfg.prefetch - 1}>();")
         if staged:
             # the ring slot of plane i - RAD is refilled next: every thread must be done with it
             K.append("    ok = __syncthreads_and(ok);")
@@ -1591,12 +1607,16 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
         if staged:
             K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
+            if async_lsu:
+                K.append("    cp_async_commit();  // one group per plane, empty near the segment end")
         K.append("  }")
         K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
         K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
                  % (" false" if batch else ""))
         K += ["  " + k for k in _red_flush(spec, "cta")]
         if batch:
+            if async_lsu:
+                K.append("  cp_async_wait<0>();")
             if tma_fields:
                 # every requested plane was waited on: retire the barriers before the
                 # next item re-initialises this shared memory

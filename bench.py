@@ -434,15 +434,21 @@ def run_lazy(args):
 def run_costmodel(args):
     """Config 4: random expression DAGs timed by the autotuner, an MLP (the library's
     CUDA forward/backward/Adam kernels) trained on the timings, top-3 regret on
-    held-out DAGs whose every candidate was timed."""
+    held-out DAGs whose every candidate was timed. Held-out DAGs are compiled and
+    timed first; training DAGs follow in chunks until ``--cm-budget`` seconds have
+    passed (the line reports how many were used). Progress goes to stderr."""
     import numpy as np
     from stenpy_b200 import autotune as AT
     from stenpy_b200 import costmodel as CM
     from stenpy_b200 import fused_compiler as FC
+    t_start = time.time()
+
+    def log(msg):
+        print(f"[costmodel {time.time() - t_start:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
     rng = np.random.default_rng(args.seed)
     n_dag, n_hold, n_sub = args.dags, args.heldout, args.train_cands
     dags = []
-    sources = []
     for d in range(n_dag):
         g, wanted, shape, dtype = CM.random_dag(rng)
         try:
@@ -450,37 +456,66 @@ def run_costmodel(args):
         except FC.FusionError:
             continue
         held = d >= n_dag - n_hold
-        picks = []
+        picks, srcs = [], []
         for pp in plan.passes:
             cands = AT.candidates(pp.spec)
             if not held:
                 idx = rng.choice(len(cands), size=min(n_sub, len(cands)), replace=False)
                 cands = [cands[i] for i in sorted(idx)]
             picks.append(cands)
-            sources += [FC.emit_pass(AT.with_config(pp.spec, c)) for c in cands]
-        dags.append((d, g, wanted, shape, dtype, held, picks))
-    t0 = time.time()
-    n_comp = CM.precompile(sources)          # spawn pool, before the first CUDA call
-    compile_s = time.time() - t0
-    dev = torch.device("cuda", 0)
-    t0 = time.time()
-    tune_s_total = 0.0
-    tune_s_hold, n_hold_passes = 0.0, 0
-    for d, g, wanted, shape, dtype, held, picks in dags:
-        gd = CM.materialize(g, dev, seed=d * 10)
-        plan = FC.Planner(gd, wanted, dtype).plan()
-        values, _ = FC.bind(plan, gd, wanted)
-        for pp, cands in zip(plan.passes, picks):
-            t1 = time.time()
-            AT.tune_pass(pp, values, plan.shape, dev, cands=[AT.with_config(pp.spec, c).cfg for c in cands],
-                         tag=f"cm-{'hold' if held else 'train'}-{d}", reuse=False)
-            tune_s_total += time.time() - t1
-            if held:
-                tune_s_hold += time.time() - t1
-                n_hold_passes += 1
-        del gd, values
+            srcs += [FC.emit_pass(AT.with_config(pp.spec, c)) for c in cands]
+        dags.append((d, g, wanted, shape, dtype, held, picks, srcs))
+    hold_dags = [x for x in dags if x[5]]
+    train_dags = [x for x in dags if not x[5]]
+    log(f"{len(dags)} DAGs planned ({len(hold_dags)} held out)")
+    compile_s = collect_s = tune_s_hold = 0.0
+    n_comp = n_hold_passes = n_train_used = 0
+    # compile everything of a chunk with a spawn pool BEFORE this process touches
+    # CUDA; later chunks compile in the same pool while nothing else runs
+    import multiprocessing as mp
+    pool = mp.get_context("spawn").Pool(max(1, min(32, (os.cpu_count() or 2) - 1)))
+
+    def compile_chunk(chunk):
+        nonlocal compile_s, n_comp
+        t = time.time()
+        todo = list(dict.fromkeys(src for x in chunk for src in x[7]))
+        n_comp += sum(pool.map(CM._compile_worker, todo, chunksize=4))
+        compile_s += time.time() - t
+
+    def time_chunk(chunk, dev):
+        nonlocal collect_s, tune_s_hold, n_hold_passes
+        t = time.time()
+        for d, g, wanted, shape, dtype, held, picks, _ in chunk:
+            gd = CM.materialize(g, dev, seed=d * 10)
+            plan = FC.Planner(gd, wanted, dtype).plan()
+            values, _ = FC.bind(plan, gd, wanted)
+            for pp, cands in zip(plan.passes, picks):
+                t1 = time.time()
+                AT.tune_pass(pp, values, plan.shape, dev, cands=[AT.with_config(pp.spec, c).cfg for c in cands],
+                             tag=f"cm-{'hold' if held else 'train'}-{d}", reuse=False, unload=True)
+                if held:
+                    tune_s_hold += time.time() - t1
+                    n_hold_passes += 1
+            del gd, values
         torch.cuda.empty_cache()
-    collect_s = time.time() - t0
+        collect_s += time.time() - t
+
+    compile_chunk(hold_dags)
+    log(f"held-out kernels compiled ({n_comp}, {compile_s:.0f}s)")
+    dev = torch.device("cuda", 0)
+    time_chunk(hold_dags, dev)
+    log(f"held-out DAGs timed ({collect_s:.0f}s)")
+    step = 200
+    for c0 in range(0, len(train_dags), step):
+        if time.time() - t_start > args.cm_budget:
+            break
+        chunk = train_dags[c0:c0 + step]
+        compile_chunk(chunk)
+        time_chunk(chunk, dev)
+        n_train_used += len(chunk)
+        log(f"{n_train_used} training DAGs timed (compile {compile_s:.0f}s, timing {collect_s:.0f}s)")
+    pool.close()
+    pool.join()
     recs = CM.load_records(AT.LOG_PATH, tags=["cm-"])
     train = [r for r in recs if r["tag"].startswith("cm-train")]
     hold = [r for r in recs if r["tag"].startswith("cm-hold")]
@@ -498,15 +533,17 @@ def run_costmodel(args):
     rmse = float(((model.predict(Xh) - yh.double()) ** 2).mean().sqrt())
     line = {"metric": "cost-model top-3 schedule regret vs exhaustive autotuning", "value": (ev["model_topk"] or {}).get("mean"),
             "unit": "fraction", "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
-            "config": {"workload": f"{len(dags)} random DAGs of 3-20 ops, grids 64..512 per dim (multiples of 32), "
-                                   f"FP32/BF16; {n_hold} held out with every candidate timed, training DAGs "
-                                   f"with {n_sub} random candidates each",
+            "config": {"workload": f"{len(hold_dags) + n_train_used} random DAGs of 3-20 ops, grids 64..512 per dim "
+                                   f"(multiples of 32), FP32/BF16; {len(hold_dags)} held out with every candidate "
+                                   f"timed, {n_train_used} training DAGs with {n_sub} random candidates each "
+                                   f"(of {n_dag} generated, time budget {args.cm_budget:.0f}s)",
                        "candidates_per_pass": ev["candidates_per_pass"]},
             "regret": ev, "train_records": len(train), "heldout_records": len(hold),
             "heldout_rmse_centred_log_time": rmse, "ensemble": args.ensemble,
             "autotune_seconds_per_pass": {"exhaustive": tune_s_hold / max(1, n_hold_passes),
                                           "model_top3_est": tune_s_hold / max(1, n_hold_passes) * 3.0 /
-                                          max(1.0, ev["candidates_per_pass"])}, "loss_history": hist[::5] + hist[-1:],
+                                          max(1.0, ev["candidates_per_pass"])},
+            "loss_history": hist[::5] + hist[-1:],
             "seconds": {"compile": compile_s, "collect": collect_s, "fit": fit_s, "kernels_compiled": n_comp}}
     print(json.dumps(line), flush=True)
 
@@ -681,6 +718,7 @@ def main():
     ap.add_argument("--train-cands", type=int, default=8)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--ensemble", type=int, default=5)
+    ap.add_argument("--cm-budget", type=float, default=1500.0, help="seconds for collecting cost-model timings")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--lazy-shape", default="1536x1536x1024")
     ap.add_argument("--budget-gb", type=float, default=8.0)

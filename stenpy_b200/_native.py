@@ -167,6 +167,14 @@ def load_module(key: str, cubin: bytes, kernel_name: str, dyn_smem_max: int, dev
     return out.value
 
 
+def unload_module(key: str, device: int) -> None:
+    """Release a loaded module (the caller guarantees no launch of it is pending)."""
+    with _lock:
+        h = _modules.pop((key, device), None)
+    if h is not None:
+        lib().stenpy_module_free(h)
+
+
 def module_info(module: int, block_threads: int, dyn_smem: int) -> Tuple[int, int, int]:
     """(resident blocks per SM, registers per thread, local bytes per thread)."""
     b, r, loc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -150,7 +150,7 @@ def _launches(pp: FC.PassPlan, spec: PassSpec, values: Dict[str, Any], shape, de
 
 
 def time_schedule(pp: FC.PassPlan, cfg: PassConfig, values: Dict[str, Any], shape, device,
-                  reps: int = 5) -> float:
+                  reps: int = 5, unload: bool = False) -> float:
     """Median milliseconds of one pass (main + shell kernel) under ``cfg``."""
     dev_idx = device.index if device.index is not None else torch.cuda.current_device()
     spec = with_config(pp.spec, cfg)
@@ -185,6 +185,10 @@ def time_schedule(pp: FC.PassPlan, cfg: PassConfig, values: Dict[str, Any], shap
         b.synchronize()
         ts.append(a.elapsed_time(b))
     FC.ErrorFlag.check(device)
+    if unload:   # a one-off timing (cost-model data): do not keep thousands of modules loaded
+        N.unload_module(key, dev_idx)
+        if shell_mod is not None:
+            N.unload_module(key + ":shell", dev_idx)
     ts.sort()
     return ts[len(ts) // 2]
 
@@ -214,7 +218,8 @@ def _save_best(best: Dict[str, Any]) -> None:
 
 
 def tune_pass(pp: FC.PassPlan, values: Dict[str, Any], shape, device, cands: Optional[List[PassConfig]] = None,
-              tag: str = "", reuse: bool = True) -> Tuple[PassConfig, List[Tuple[PassConfig, float]]]:
+              tag: str = "", reuse: bool = True, unload: bool = False
+              ) -> Tuple[PassConfig, List[Tuple[PassConfig, float]]]:
     """Exhaustively time ``cands`` (default: all candidates) and return the fastest."""
     key = pass_key(pp.spec, shape)
     best_db = _load_best() if reuse else {}
@@ -225,7 +230,7 @@ def tune_pass(pp: FC.PassPlan, values: Dict[str, Any], shape, device, cands: Opt
     feats = features(pp.spec, shape)
     results = []
     for cfg in cands:
-        ms = time_schedule(pp, cfg, values, shape, device)
+        ms = time_schedule(pp, cfg, values, shape, device, unload=unload)
         results.append((cfg, ms))
         log_record({"key": key, "tag": tag, "features": feats, "schedule": schedule_features(pp.spec, cfg),
                     "cfg": vars(cfg), "ms": ms, "time": time.time()})

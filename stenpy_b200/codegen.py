@@ -1042,8 +1042,12 @@ def _ghost_fill(spec: PassSpec, rings: Dict[int, int]) -> List[str]:
         if todo_k:
             layers = 2 if rk == "edge2x2" else 1
             for layer in range(1, layers + 1):
+                # periodic strips exist only for tiles at the face; extrapolated ghosts also
+                # for tiles whose halo crosses it (kept inside the box)
+                hi_k = ("tk0 + TK >= p.n2" if rk == "periodic" else
+                        f"tk0 + TK + RAD > p.n2 && p.n2 - tk0 + {layer - 1} < TK + {hk}")
                 for side, cond, col in (("lo", "tk0 == 0", f"{hk} - {layer}"),
-                                        ("hi", "tk0 + TK >= p.n2", f"p.n2 - tk0 + {hk} + {layer - 1}")):
+                                        ("hi", hi_k, f"p.n2 - tk0 + {hk} + {layer - 1}")):
                     K.append(f"    if ({cond}) for (int e = tid; e < TJ * {nc}; e += NT) {{")
                     K.append(f"      const int yy = e / {nc}, c = e - yy * {nc};")
                     K.append("      if (tj0 + yy < p.n1) {")
@@ -1065,8 +1069,10 @@ def _ghost_fill(spec: PassSpec, rings: Dict[int, int]) -> List[str]:
         if todo_j:
             layers = 2 if rj == "edge2x2" else 1
             for layer in range(1, layers + 1):
+                hi_j = ("tj0 + TJ >= p.n1" if rj == "periodic" else
+                        f"tj0 + TJ + RAD > p.n1 && p.n1 - tj0 + {layer - 1} < TJ + {f.halo}")
                 for side, cond, row in (("lo", "tj0 == 0", f"{f.halo} - {layer}"),
-                                        ("hi", "tj0 + TJ >= p.n1", f"p.n1 - tj0 + {f.halo} + {layer - 1}")):
+                                        ("hi", hi_j, f"p.n1 - tj0 + {f.halo} + {layer - 1}")):
                     K.append(f"    if ({cond}) for (int e = tid; e < TK * {nc}; e += NT) {{")
                     K.append(f"      const int xx = e / {nc}, c = e - xx * {nc};")
                     K.append("      if (tk0 + xx < p.n2) {")
@@ -1330,7 +1336,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  const int ib = p.out_lo + by * p.seg_len;")
         K.append("  const int ie = min(ib + p.seg_len, p.out_lo + p.n_out);")
         K.append("  const int cta = p.cta_off + by * gdx + bx;")
-        K.append("  const bool edge_cta = tk0 == 0 || tk0 + TK >= p.n2 || tj0 == 0 || tj0 + TJ >= p.n1;")
+        # a tile whose halo reaches past a face (reach RAD) needs ghost cells there
+        K.append("  const bool edge_cta = tk0 == 0 || tk0 + TK + RAD > p.n2 || tj0 == 0 || tj0 + TJ + RAD > p.n1;")
         K.append("  FCtx x;")
         K.append(f"  #pragma unroll\n  for (int s = 0; s < {max(spec.n_scalars, 1)}; ++s) "
                  f"x.sc[s] = (s < {spec.n_scalars}) ? (float)__ldcg(p.scal + s) : 0.0f;")

@@ -64,6 +64,10 @@ def all_sources():
     g, sink, *_ = S.compile_expression("divergence(gradient(f)) + l2norm(curl(u))", boundary="periodic",
                                        field_map={"f": _ph((40, 48, 64)), "u": _ph((40, 48, 64, 3))})
     src += plan_sources(g, [sink] + [g.add(r, (sink,), {}) for r in ("sum", "mean", "variance")])  # no-alloc
+    for shape in [(10, 17, 65), (9, 33, 97), (12, 18, 66)]:     # second-derivative ghosts
+        for tk, tj in ((32, 16), (64, 8)):
+            g, sink, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": _ph(shape)})
+            src += plan_sources(g, [sink], torch.float32, PassConfig(tj=tj, tk=tk, threads=128, seg_len=8))
     expr = "divergence(gradient(f)) + l2norm(curl(u)) + laplacian(f)*tanh(f)"
     for dt in (torch.float32, torch.float16, torch.bfloat16):   # KV chunk parity
         for bnd in ("periodic", "neumann"):

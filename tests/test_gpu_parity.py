@@ -112,3 +112,21 @@ def test_kv_chunks_match_one_voxel_per_thread(dtype, boundary):
         for key, (o, v) in outs.items():
             assert torch.equal(o, ref), (key, shape, (o.float() - ref.float()).abs().max().item())
             assert abs(v - vref) <= 1e-12 * abs(vref), (key, v, vref)
+
+
+@pytest.mark.parametrize("tk,tj", [(32, 16), (64, 8)])
+@pytest.mark.parametrize("shape", [(10, 17, 65), (9, 33, 97), (12, 18, 66)])
+def test_second_derivative_ghosts_where_tile_halos_cross_faces(shape, tk, tj):
+    """Two-layer ghost cells of d1(d1(f)) (reach 2): tiles whose own voxels stop one
+    short of a face still read past it and must get the extrapolated values."""
+    import stenpy_b200 as S
+    from stenpy_b200.codegen import PassConfig
+    from stenpy_b200.synth import sinusoid_field
+    dev = _dev()
+    f = sinusoid_field(shape, seed=9)
+    cfg = PassConfig(tj=tj, tk=tk, threads=128, seg_len=8)
+    g, sink, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": f.to(dev)})
+    got = S.Runtime(device=dev, config=cfg).run(g)[sink]
+    g2, sink2, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": f.double()})
+    ref = O.evaluate(g2, [sink2])[sink2]
+    assert rel_err(got, ref) <= 1e-5, (shape, tk, tj, rel_err(got, ref))

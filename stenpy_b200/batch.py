@@ -474,8 +474,13 @@ def tune_batch(jobs: Sequence[Any], device: Any = "cuda", cands: Optional[List[P
             prog = BatchProgram([jobs[i] for i in idx], [plans[i] for i in idx], module, device)
             t = time_program(prog, reps)
             if log is not None:
-                log.append({"group": gk[:12], "jobs": len(idx), "cfg": vars(cfg).copy(), "ms": t,
-                            "blocks_per_sm": module.blocks_per_sm, "regs": module.regs})
+                j0, p0 = jobs[idx[0]], plans[idx[0]]
+                label = "+".join(j0.graph._nodes[w].op_name for w in j0.wanted)
+                label += f" {FC.TORCH_DT[j0.out_dtype]} tma={any(f.tma for pp in p0.passes for f in pp.spec.fields)}"
+                vox = sum(plans[i].shape[0] * plans[i].shape[1] * plans[i].shape[2] for i in idx)
+                log.append({"group": gk[:12], "label": label, "jobs": len(idx), "voxels": vox,
+                            "cfg": vars(cfg).copy(), "ms": t, "blocks_per_sm": module.blocks_per_sm,
+                            "regs": module.regs})
             cur = best.setdefault(cfg.threads, {}).get(gk)
             if cur is None or t < cur[0]:
                 best[cfg.threads][gk] = (t, cfg)

@@ -26,6 +26,7 @@ keeps the fastest per group (all groups share the block size).
 """
 from __future__ import annotations
 
+import dataclasses
 import hashlib
 import statistics
 import struct
@@ -97,7 +98,14 @@ class BatchJob:
 
 
 def plan_job(job: BatchJob, cfg: PassConfig) -> FC.FusedPlan:
+    from .autotune import default_kv
+    from .codegen import valid_shape
     plan = FC.Planner(job.graph, job.wanted, job.out_dtype, cfg).plan()
+    kv = max([default_kv(pp.spec) for pp in plan.passes] + [1])
+    if kv != cfg.kv:
+        cfg2 = dataclasses.replace(cfg, kv=kv)
+        if valid_shape(cfg2):
+            plan = FC.Planner(job.graph, job.wanted, job.out_dtype, cfg2).plan()
     if plan.scalar_source:
         raise FC.FusionError("batch: sinks that are expressions of reduction results are not batched")
     if any(pp.spec.has_scan for pp in plan.passes):

@@ -241,7 +241,7 @@ def valid_shape(cfg: "PassConfig") -> bool:
 
 
 FLAT_V = 4       # voxels per thread per step of a flat (stencil-free) pass
-FLAT_ITER = 8    # steps per work item: an item covers threads x FLAT_V x FLAT_ITER voxels
+FLAT_ITER = 32   # steps per work item: an item covers threads x FLAT_V x FLAT_ITER voxels
 
 
 def is_flat(spec: "PassSpec") -> bool:
@@ -889,6 +889,9 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
                     if where == "main" and not is_flat(spec):
                         # per-plane and per-column weights computed outside the voxel loop
                         K.append(f"rv{ri_here}_a += {val} * rv{ri_here}_wi * rv{ri_here}_wj[{{M}}] * rv{ri_here}_wk[{{KK}}];")
+                    elif where == "flat":
+                        K.append(f"rv{ri_here}_a += {val} * rv{ri_here}_wi * rv{ri_here}_wj"
+                                 f" * sten_simpson_w(k, p.n2, {r.dx[2]!r}, {sm});")
                     else:
                         K.append(f"rv{ri_here}_a += {val} * sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm})"
                                  f" * sten_simpson_w(j, p.n1, {r.dx[1]!r}, {sm}) * sten_simpson_w(k, p.n2, {r.dx[2]!r}, {sm});")
@@ -1167,6 +1170,12 @@ def _flat_body(spec: PassSpec, e: "_Emitter", red_off: int, batch: bool) -> List
     if need_idx:
         K.append("    size_t i_ = base / plane_n; const size_t r_ = base - i_ * plane_n;")
         K.append("    int jq = (int)(r_ / (size_t)p.n2), kq = (int)(r_ - (size_t)jq * p.n2);")
+        for ri, r in enumerate(reds):
+            if r.red == "integrate":
+                sm = 1 if r.method == "simpson" else 0
+                # plane and row weights change only when the voxel run wraps a row
+                K.append(f"    double rv{ri}_wi = sten_simpson_w((int)i_ + p.i_base, p.n0g, {r.dx[0]!r}, {sm}), "
+                         f"rv{ri}_wj = sten_simpson_w(jq, p.n1, {r.dx[1]!r}, {sm});")
     K.append(f"    float rvk[FV][{nroot}];")
     for v in range(FLAT_V):
         K.append(f"    if ({v} < nv) {{")
@@ -1178,7 +1187,13 @@ def _flat_body(spec: PassSpec, e: "_Emitter", red_off: int, batch: bool) -> List
         K += ["      " + k for k in _epilogue(spec, e, scan_ok=False, skip=vec_outs, where="flat", m=0, kk=v)]
         K.append("    }")
         if need_idx and v + 1 < FLAT_V:
-            K.append("    if (++kq == p.n2) { kq = 0; if (++jq == p.n1) { jq = 0; ++i_; } }")
+            upd = []
+            for ri, r in enumerate(reds):
+                if r.red == "integrate":
+                    sm = 1 if r.method == "simpson" else 0
+                    upd.append(f"rv{ri}_wi = sten_simpson_w((int)i_ + p.i_base, p.n0g, {r.dx[0]!r}, {sm}); "
+                               f"rv{ri}_wj = sten_simpson_w(jq, p.n1, {r.dx[1]!r}, {sm});")
+            K.append("    if (++kq == p.n2) { kq = 0; if (++jq == p.n1) { jq = 0; ++i_; } " + " ".join(upd) + " }")
     for r in vec_outs:
         ct = CTYPE[r.out_dtype]
         off = e.offsets[spec.roots.index(r)]
@@ -1309,7 +1324,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     tma_fields = [f for f in spec.fields if f.tma]
     lsu_fields = [f for f in spec.fields if f.staged and not f.tma]
     # cooperative staging of 4-byte fields is asynchronous: one commit group per plane
-    async_lsu = any(ESIZE[f.dtype] == 4 for f in lsu_fields)
+    async_lsu = any(ESIZE[f.dtype] in (2, 4) for f in lsu_fields)
     total_smem, rings, red_off = smem_layout(spec)
     tma_bytes = sum(spec.box(f)[0] * spec.box(f)[1] * ESIZE[f.dtype] for f in tma_fields)
     reds = [r for r in spec.roots if r.kind == "red"]
@@ -1421,6 +1436,17 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                     # barrier that precedes the plane's first use (like the TMA ring)
                     K.append(f"        #pragma unroll 4\n        for (int e = tid; e < {w * h}; e += NT) {{")
                     K.append(f"          const int yy = e / {w}; cp_async4(dst + e, rowp + (yy * pitch + (e - yy * {w})));")
+                    K.append("        }")
+                elif ESIZE[f.dtype] == 2:
+                    # 2-byte elements: element pairs as 4-byte asynchronous copies on rows whose
+                    # global start is 4-byte aligned (the shared row always is); plain copies
+                    # on the others
+                    K.append(f"        #pragma unroll 4\n        for (int e2 = tid; e2 < {w // 2 * h}; e2 += NT) {{")
+                    K.append(f"          const int yy = e2 / {w // 2}, x2 = 2 * (e2 - yy * {w // 2});")
+                    K.append(f"          const {ct}* sr = rowp + yy * pitch + x2;")
+                    K.append(f"          {ct}* dr = dst + yy * {w} + x2;")
+                    K.append("          if ((((size_t)sr) & 3) == 0) cp_async4(dr, sr);")
+                    K.append("          else { dr[0] = ldg_raw(sr); dr[1] = ldg_raw(sr + 1); }")
                     K.append("        }")
                 else:
                     gsz = 4

@@ -48,6 +48,10 @@ REDS = ("sum", "mean", "variance")
 FORM_DT = {"fp32": torch.float32, "fp16": torch.float16, "bf16": torch.bfloat16}
 ALG_BYTES = {"fp32": 20, "fp16": 10, "bf16": 10}   # f + u(3) + out, each once
 HEADLINE = "fp16"
+# DRAM bytes (read + write) of one launch of the headline form's dominant pass at
+# 512^3, from an ncu capture of this command's kernels (profiles/ summary of
+# sten_kernel at 512^3, FP16); null for other sizes or forms
+NCU_TRAFFIC = {("fp16", 512): 274057728 + 234228480}
 
 
 def _peaks():
@@ -788,7 +792,8 @@ def main():
             "launches_per_step": n_launch,
             "schedules": [dict(vars(p.spec.cfg)) for p in plan.passes],
             "kernels_ms": [round(t, 4) for _, t in kt],
-            "dominant": {"ms": dom_ms, "alg_bytes": alg, "GBps": alg / (dom_ms * 1e-3) / 1e9},
+            "dominant": {"ms": dom_ms, "alg_bytes": alg, "GBps": alg / (dom_ms * 1e-3) / 1e9,
+                         "frac_of_peak": alg / (dom_ms * 1e-3) / 1e9 / peak},
         }
         del cg
     head = results[HEADLINE] if HEADLINE in results else results[forms[0]]
@@ -804,7 +809,8 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": head["dominant"]["GBps"], "peak": peak, "unit": "GB/s",
                          "frac": head["dominant"]["GBps"] / peak, "peak_kind": peak_kind,
-                         "traffic": None, "kernel": "dominant pass of the headline form",
+                         "traffic": NCU_TRAFFIC.get((head_form, args.size)),
+                         "kernel": "dominant pass of the headline form",
                          "step_frac": head["step_frac_of_peak"]},
             "forms": results, "gpu_launches": head["launches_per_step"] * args.steps, "clocks": clocks}
     if not args.no_e2e:

@@ -127,6 +127,15 @@ class Runtime:
         return out
 
     def _run_fused(self, g: Graph, wanted: List[str]) -> Dict[str, Any]:
+        try:
+            return self._run_fused_or_raise(g, wanted)
+        except FC.FusionError as exc:
+            # as the reference does when fusion fails (stenpy_engine.py:949-954): warn and
+            # run the graph node by node, still on the GPU
+            warnings.warn(f"Fusion failed, falling back to node-by-node execution: {exc}", RuntimeWarning)
+            return self._run_eager(g, wanted)
+
+    def _run_fused_or_raise(self, g: Graph, wanted: List[str]) -> Dict[str, Any]:
         while True:
             order = [n.id for n in g.topological_sort()]
             live = set(g.live_nodes(wanted))

@@ -19,6 +19,25 @@ def _ph(t_or_shape, dtype=torch.float32):
     return torch.zeros(1, dtype=dtype).expand(*shape)
 
 
+def eager_sources(g, S, O):
+    """Sources of a node-by-node run: each node as a one-node graph on inputs of the
+    shapes its producers give (values from the oracle)."""
+    from stenpy_b200.prewarm import plan_sources
+    src, vals = [], {}
+    for node in g.topological_sort():
+        if node.op_name == "_constant":
+            vals[node.id] = node.params["value"]
+            continue
+        g1 = S.Graph()
+        ids = [g1.add("_constant", (), {"value": vals[i] if (not isinstance(vals[i], torch.Tensor) or vals[i].ndim == 0)
+                                        else _ph(vals[i].shape, torch.float32)})
+               for i in node.input_ids]
+        nid = g1.add(node.op_name, ids, node.params)
+        src += plan_sources(g1, [nid])
+        vals[node.id] = O.evaluate(g1, [nid])[nid]
+    return src
+
+
 def all_sources():
     import stenpy_b200 as S
     from stenpy_b200 import batch as B
@@ -36,17 +55,7 @@ def all_sources():
         src += plan_sources(g, [sink])
     for c in cases[:6]:   # eager mode: one kernel per node on the node's own inputs
         g, sink, *_ = S.compile_expression(c["expr"], dx=c["dx"], boundary=c["boundary"], field_map=c["inputs"])
-        vals = {}
-        for node in g.topological_sort():
-            if node.op_name == "_constant":
-                vals[node.id] = node.params["value"]
-                continue
-            g1 = S.Graph()
-            ids = [g1.add("_constant", (), {"value": vals[i] if vals[i].ndim == 0 else _ph(vals[i].shape)})
-                   for i in node.input_ids]
-            nid = g1.add(node.op_name, ids, node.params)
-            src += plan_sources(g1, [nid])
-            vals[node.id] = O.evaluate(g1, [nid])[nid]
+        src += eager_sources(g, S, O)
     for shape in [(5, 7, 33), (3, 3, 3), (17, 9, 130), (2, 40, 64)]:   # ragged shapes
         for b in ["periodic", "neumann", "dirichlet"]:
             exprs = ["laplacian(f) + tanh(g)*exp(f)", "gradient(f)"]
@@ -64,6 +73,11 @@ def all_sources():
     g, sink, *_ = S.compile_expression("divergence(gradient(f)) + l2norm(curl(u))", boundary="periodic",
                                        field_map={"f": _ph((40, 48, 64)), "u": _ph((40, 48, 64, 3))})
     src += plan_sources(g, [sink] + [g.add(r, (sink,), {}) for r in ("sum", "mean", "variance")])  # no-alloc
+    from stenpy_b200.synth import sinusoid_field   # node-by-node fallback (two grids)
+    g, sinks, *_ = S.compile_expressions({"a": "laplacian(f)", "b": "laplacian(g) * 2"}, boundary="periodic",
+                                         field_map={"f": sinusoid_field((8, 9, 16), seed=1).double(),
+                                                    "g": sinusoid_field((10, 12, 16), seed=2).double()})
+    src += eager_sources(g, S, O)
     for shape in [(10, 17, 65), (9, 33, 97), (12, 18, 66)]:     # second-derivative ghosts
         for tk, tj in ((32, 16), (64, 8)):
             g, sink, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": _ph(shape)})

@@ -130,3 +130,25 @@ def test_second_derivative_ghosts_where_tile_halos_cross_faces(shape, tk, tj):
     g2, sink2, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": f.double()})
     ref = O.evaluate(g2, [sink2])[sink2]
     assert rel_err(got, ref) <= 1e-5, (shape, tk, tj, rel_err(got, ref))
+
+
+def test_unfusable_graph_warns_and_runs_node_by_node():
+    """Fields on two different grids cannot share fused passes: like the reference,
+    the runtime warns and runs the graph node by node (on the GPU)."""
+    import warnings as W
+    import stenpy_b200 as S
+    from stenpy_b200.synth import sinusoid_field
+    dev = _dev()
+    f = sinusoid_field((8, 9, 16), seed=1)
+    g = sinusoid_field((10, 12, 16), seed=2)
+    gr, sinks, *_ = S.compile_expressions({"a": "laplacian(f)", "b": "laplacian(g) * 2"}, boundary="periodic",
+                                          field_map={"f": f.to(dev), "g": g.to(dev)})
+    with W.catch_warnings(record=True) as rec:
+        W.simplefilter("always")
+        res = S.Runtime(device=dev).run(gr, wanted=list(sinks.values()))
+    assert any("Fusion failed" in str(w.message) for w in rec)
+    g2, sinks2, *_ = S.compile_expressions({"a": "laplacian(f)", "b": "laplacian(g) * 2"}, boundary="periodic",
+                                           field_map={"f": f.double(), "g": g.double()})
+    ref = O.evaluate(g2, list(sinks2.values()))
+    for k in ("a", "b"):
+        assert rel_err(res[sinks[k]], ref[sinks2[k]]) <= 1e-5, k

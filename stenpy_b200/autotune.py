@@ -11,8 +11,8 @@ register estimate (fused_compiler.py:20-43); here schedules are measured.
 CUDA events (median of repeated launches on the pass's real inputs) and keeps the
 fastest; every measurement is appended to a JSON-lines log together with the
 pass's features (``features``), which is the training set of the learned ranking
-model (``costmodel.py``). Exhaustive tuning is the fallback and the judge of the
-model's regret.
+model (``costmodel.py``). Exhaustive tuning is the fallback and the yardstick of
+the model's regret.
 """
 from __future__ import annotations
 

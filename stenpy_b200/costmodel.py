@@ -282,6 +282,16 @@ def evaluate(model: CostModel, heldout: Sequence[Dict[str, Any]], k: int = 3, se
             "timing_runs_saved_frac": (1.0 - k / mean_c) if mean_c else None}
 
 
+DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "costmodel_b200.npz")
+
+
+def load_default(device: Any = "cuda") -> "Ensemble":
+    """The ensemble trained on B200 autotuner timings of random DAGs (shipped with
+    the package): ``autotune.tune_plan(plan, values, dev, chooser=chooser(load_default()))``
+    then times only its top candidates."""
+    return Ensemble.load(DEFAULT_MODEL, device)
+
+
 def chooser(model: CostModel, k: int = 3):
     """``autotune.tune_plan(chooser=...)`` hook: keep the model's top-k candidates."""
     from . import autotune as AT

@@ -262,3 +262,20 @@ def test_cost_model_fixture_and_baselines_without_gpu():
 
     ev = CM.evaluate(Zero(), hold, k=3)
     assert ev["passes"] > 10 and 0.0 <= ev["analytic_topk"]["mean"] < ev["random_topk"]["mean"] + 0.1
+
+
+def test_shipped_cost_model_matches_feature_layout():
+    """The ensemble shipped with the package takes the current feature vector."""
+    import numpy as np
+    from stenpy_b200 import costmodel as CM
+    z = np.load(CM.DEFAULT_MODEL)
+    feat = {"radius": 1, "n0": 64, "n1": 64, "n2": 64, "voxels": 64.0 ** 3, "in_bytes": 4, "out_bytes": 4}
+    sched = {"tj": 8, "tk": 64, "threads": 128, "vpt": 4, "seg_len": 32, "prefetch": 2, "smem": 1e4,
+             "ghost": 1, "shell": 0, "kv": 1}
+    d = len(CM.vectorize(feat, sched))
+    assert int(z["n"]) >= 1
+    for i in range(int(z["n"])):
+        h = int(z[f"m{i}_hidden"])
+        assert int(z[f"m{i}_in_dim"]) == d
+        assert z[f"m{i}_params"].size == d * h + h + h * h + h + h + 1
+        assert np.isfinite(z[f"m{i}_params"]).all()

@@ -93,3 +93,24 @@ def test_learned_ranking_beats_the_methods_without_it():
     assert m < ev["analytic_topk"]["mean"] and m < ev["random_topk"]["mean"], ev
     assert m < ev["default_schedule"]["mean"], ev
     assert m <= 0.05, ev
+
+
+def test_shipped_model_ranks_heldout_passes_and_prunes_candidates():
+    """The shipped ensemble (trained on the training DAGs of the same B200 run) keeps
+    top-3 regret on the held-out passes within 5 %, and as the autotuner's chooser
+    returns three of a pass's candidates."""
+    import stenpy_b200 as S
+    from stenpy_b200 import autotune as AT
+    from stenpy_b200 import costmodel as CM
+    from stenpy_b200 import fused_compiler as FC
+    dev = _dev()
+    model = CM.load_default(dev)
+    _, hold = _fixture()
+    ev = CM.evaluate(model, hold, k=3)
+    assert ev["model_topk"]["mean"] <= 0.05 and ev["model_topk"]["mean"] < ev["analytic_topk"]["mean"], ev
+    f = torch.zeros(64, 96, 128)
+    g, sink, *_ = S.compile_expression("laplacian(f) * tanh(f)", boundary="periodic", field_map={"f": f})
+    pp = FC.Planner(g, [sink]).plan().passes[0]
+    cands = AT.candidates(pp.spec)
+    pick = CM.chooser(model, k=3)(pp, cands, (64, 96, 128))
+    assert len(pick) == 3 and all(any(vars(c) == vars(p) for c in cands) for p in pick)

@@ -78,6 +78,9 @@ def all_sources():
                                          field_map={"f": sinusoid_field((8, 9, 16), seed=1).double(),
                                                     "g": sinusoid_field((10, 12, 16), seed=2).double()})
     src += eager_sources(g, S, O)
+    g, sink, *_ = S.compile_expression("laplacian(f) * tanh(f)", boundary="periodic",   # cost-model chooser
+                                       field_map={"f": _ph((64, 96, 128))})
+    src += plan_sources(g, [sink])
     for shape in [(10, 17, 65), (9, 33, 97), (12, 18, 66)]:     # second-derivative ghosts
         for tk, tj in ((32, 16), (64, 8)):
             g, sink, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": _ph(shape)})

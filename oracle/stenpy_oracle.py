@@ -202,6 +202,54 @@ def mean_curvature(t, dx=1.0, boundary="neumann", eps: float = 1e-15):
     return divergence(g / mag, dx=h, boundary=boundary)
 
 
+def material_derivative(t, velocity, dx=1.0, boundary="neumann"):
+    """Σ_d velocity[..., d] · ∂_d t with ∂ = gradient_nd, accumulated from zero in
+    axis order (stenpy_engine.py:2223-2244)."""
+    g = gradient_nd(t, dx)
+    out = torch.zeros_like(t)
+    for d in range(t.ndim):
+        out = out + velocity[..., d] * g[..., d]
+    return out
+
+
+def moving_average(t, window: int = 3, boundary: str = "neumann"):
+    """Mean over ``window`` cells along each axis in turn (axis 0 first), each axis
+    padded by ``window // 2`` cells with ``_pad1d``'s rule (stenpy_engine.py:2385-2408).
+    Even windows change the length and the reference fails; so does this."""
+    if t.ndim > 3:
+        raise NotImplementedError("moving_average: only 1-D/2-D/3-D supported")
+    window = int(window)
+    r = window // 2
+    out = t
+    for d in range(t.ndim):
+        n = out.shape[d]
+        p = _pad1d(out, d, r, boundary)
+        if p.shape[d] - window + 1 != n:
+            raise RuntimeError(f"moving_average: window {window} changes the length of axis {d}")
+        acc = torch.zeros_like(out)
+        for s in range(window):
+            acc = acc + p.narrow(d, s, n)
+        out = acc / window
+    return out
+
+
+def conv3d_spectral(a, boundary: str = "periodic"):
+    """The 27-point Gaussian (1,2,1)⊗(1,2,1)⊗(1,2,1)/64 as a circular convolution,
+    whatever ``boundary`` says: the reference's CPU path multiplies FFTs
+    (stenpy_engine.py:2800-2860). Restated as a direct sum of rolled copies (equal up
+    to FP64 rounding); every axis needs ≥ 3 points, as the reference's kernel
+    placement requires."""
+    if a.ndim != 3 or min(a.shape) < 3:
+        raise ValueError(f"conv3d_spectral: needs a 3-D field with >= 3 points per axis, got {tuple(a.shape)}")
+    w1 = {-1: 1.0, 0: 2.0, 1: 1.0}
+    out = torch.zeros_like(a)
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            for dk in (-1, 0, 1):
+                out = out + (w1[di] * w1[dj] * w1[dk]) * torch.roll(a, (-di, -dj, -dk), (0, 1, 2))
+    return out / 64.0
+
+
 def grad_mag(t, dx=1.0, boundary="neumann"):
     """|gradient(t)| with gradient's boundary conventions (not in the reference)."""
     return torch.linalg.norm(gradient(t, dx, boundary), dim=-1)
@@ -329,7 +377,8 @@ OPS: Dict[str, Callable] = {
     "exp": exp, "log": log, "sqrt": sqrt, "sin": sin, "cos": cos, "tanh": tanh, "abs": abs_,
     "laplacian": laplacian, "gradient": gradient, "divergence": divergence, "curl": curl,
     "hessian": hessian, "jacobian": jacobian, "mean_curvature": mean_curvature,
-    "grad_mag": grad_mag, "gradient_nd": gradient_nd,
+    "grad_mag": grad_mag, "gradient_nd": gradient_nd, "material_derivative": material_derivative,
+    "moving_average": moving_average, "conv3d_spectral": conv3d_spectral,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

@@ -99,10 +99,13 @@ def candidates(spec: PassSpec) -> List[PassConfig]:
 
 
 def features(spec: PassSpec, shape: Sequence[int]) -> Dict[str, float]:
-    """Schedule-independent description of a pass (graph op mix, reach, dtypes, grid)."""
-    ops: Dict[str, int] = {}
+    """Schedule-independent description of a pass (graph op mix, reach, dtypes, grid).
+    A weighted-tap stencil counts as (taps / 7) Laplacians, by the neighbours it reads."""
+    ops: Dict[str, float] = {}
     for n in spec.graph.nodes:
         ops[n.op] = ops.get(n.op, 0) + 1
+        if n.op == "taps":
+            ops["lap"] = ops.get("lap", 0) + len(n.a("taps")) / 7.0
     trans = sum(ops.get(k, 0) for k in ("exp", "log", "sqrt", "sin", "cos", "tanh", "normalize", "norm", "eig"))
     arith = sum(ops.get(k, 0) for k in ("add", "sub", "mul", "div", "neg", "abs", "clamp", "mulk", "trace",
                                         "select", "stack"))

@@ -16,7 +16,9 @@ Primitives (every graph operator is lowered onto these, see ``lowering.py``):
   difference, torch.roll semantics), ``edge2`` / ``edge1`` (torch.gradient's
   one-sided second/first-order edges), ``zero`` (axis of length 1);
 * ``lap``: compact 7-point Laplacian with a padding rule (periodic, replicate,
-  zero, reflect).
+  zero, reflect);
+* ``taps``: weighted sum of a node at compile-time offsets within a reach (box
+  and Gaussian smoothing), out-of-range offsets remapped by a padding rule.
 
 Kernel shape (``emit_pass``): a CTA owns a TJ × TK tile of the (dim1, dim2) plane
 and marches along dim 0 over a segment of planes. Every field read at an offset
@@ -147,6 +149,7 @@ class PassSpec:
 
 
 _REMAP_RULES = ("periodic", "replicate", "reflect")
+STENCIL_PRIMS = ("d1", "lap", "taps")   # primitives that read their input at offsets
 
 
 def analyse_ghosts(spec: "PassSpec") -> None:
@@ -190,10 +193,14 @@ def analyse_ghosts(spec: "PassSpec") -> None:
     for r in spec.roots:
         subtree(r.node, live)
     for n in g.nodes:
-        if n.op not in ("d1", "lap") or n.id not in live:
+        if n.op not in STENCIL_PRIMS or n.id not in live:
             continue
+        if n.op == "taps":
+            # diagonal taps read the tile's corner cells, which the ghost fill does not
+            # write: every face goes to the shell kernel
+            return
         sub = subtree(n.ins[0], set())
-        nested = any(g.nodes[x].op in ("d1", "lap") for x in sub)
+        nested = any(g.nodes[x].op in STENCIL_PRIMS for x in sub)
         if nested and not second_derivative(n):
             return
         direct = g.nodes[n.ins[0]].op == "field" or nested
@@ -305,7 +312,7 @@ class _Emitter:
                 stack += list(self.g.nodes[x].ins)
         self.need_fn = set()
         for n in self.g.nodes:
-            if n.op in ("d1", "lap") and n.id in live:
+            if n.op in STENCIL_PRIMS and n.id in live:
                 self._mark(n.ins[0])
 
     def _mark(self, nid: int) -> None:
@@ -461,8 +468,33 @@ class _Emitter:
                 parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
                 body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
             return
+        if n.op == "taps":
+            off = [di, dj, dk]
+            vals = []
+            for tap in n.a("taps"):
+                q = [off[ax] if not tap[ax] else
+                     (f"({off[ax]}) + {tap[ax]}" if tap[ax] > 0 else f"({off[ax]}) - {-tap[ax]}")
+                     for ax in range(3)]
+                vals.append((self.fast_call(n.ins[0], *q, body), tap[3]))
+            self._tap_sum(n, vals, o, body)
+            return
         ins = [self.fast_call(i, di, dj, dk, body) for i in n.ins]
         self.pointwise(n, ins, o, body)
+
+    def _tap_sum(self, n: PNode, vals, o: str, body: List[str]) -> None:
+        """o = scale * Σ w·v over (array, weight) pairs, accumulated in tap order."""
+        for c in range(n.nc):
+            acc = None
+            for arr, w in vals:
+                term = f"{arr}[{c}]" if w == 1.0 else f"{arr}[{c}] * {_lit(w)}"
+                if acc is None:
+                    acc = self.t()
+                    body.append(f"float {acc} = {term};")
+                elif w == 1.0:
+                    body.append(f"{acc} += {arr}[{c}];")
+                else:
+                    body.append(f"{acc} = fmaf({arr}[{c}], {_lit(w)}, {acc});")
+            body.append(f"{o}[{c}] = {acc} * {_lit(n.a('scale'))};")
 
     # -- slow (boundary) functions: runtime global coordinates
     def emit_slow_fns(self) -> None:
@@ -514,6 +546,9 @@ class _Emitter:
             return
         if n.op == "lap":
             self.slow_lap(n, i, j, k, o, body)
+            return
+        if n.op == "taps":
+            self.slow_taps(n, i, j, k, o, body)
             return
         ins = [self.slow_call(x, i, j, k, body) for x in n.ins]
         self.pointwise(n, ins, o, body)
@@ -627,6 +662,45 @@ class _Emitter:
             parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
             body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
 
+    def slow_taps(self, n: PNode, i, j, k, o, body):
+        """Taps at runtime coordinates: remapped by the padding rule, or skipped
+        (zero padding) when they fall outside the grid."""
+        pad = n.a("pad")
+        crd = [i, j, k]
+        dims = ["p.n0g", "p.n1", "p.n2"]
+        remap = {"periodic": "wrap_idx", "replicate": "clamp_idx", "reflect": "reflect_idx"}.get(pad)
+        acc = self.t()
+        body.append(f"float {acc}[{n.nc}];")
+        body.append(f"for (int c = 0; c < {n.nc}; ++c) {acc}[c] = 0.0f;")
+        for tap in n.a("taps"):
+            q, conds = [], []
+            for ax in range(3):
+                d = tap[ax]
+                if not d:
+                    q.append(crd[ax])
+                    continue
+                e = f"({crd[ax]}) + {d}" if d > 0 else f"({crd[ax]}) - {-d}"
+                if remap:
+                    q.append(f"{remap}({e}, {dims[ax]})")
+                else:
+                    q.append(f"({e})")
+                    conds.append(f"({e}) >= 0 && ({e}) < {dims[ax]}")
+            sub: List[str] = []
+            arr = self.slow_call(n.ins[0], *q, sub)
+            w = tap[3]
+            for c in range(n.nc):
+                sub.append(f"{acc}[{c}] += {arr}[{c}]" + ("" if w == 1.0 else f" * {_lit(w)}") + ";")
+            if conds:
+                body.append(f"if ({' && '.join(conds)}) {{")
+                body += ["  " + x for x in sub]
+                body.append("}")
+            else:
+                body.append("{")
+                body += ["  " + x for x in sub]
+                body.append("}")
+        for c in range(n.nc):
+            body.append(f"{o}[{c}] = {acc}[{c}] * {_lit(n.a('scale'))};")
+
     # -- per-voxel root evaluation
     def emit_eval(self) -> None:
         roots = self.s.roots
@@ -645,7 +719,7 @@ class _Emitter:
             if nid in memo:
                 return memo[nid]
             n = self.g.nodes[nid]
-            if n.op in ("d1", "lap") or n.op == "field" or n.op == "scalar":
+            if n.op in STENCIL_PRIMS or n.op == "field" or n.op == "scalar":
                 arr = self.t()
                 body.append(f"float {arr}[{n.nc}];")
                 self.fast_value(n, "0", "M", "KK", arr, body)
@@ -672,7 +746,7 @@ class _Emitter:
             if nid in memo_s:
                 return memo_s[nid]
             n = self.g.nodes[nid]
-            if nid in self.need_fn or n.op in ("d1", "lap", "field", "scalar"):
+            if nid in self.need_fn or n.op in STENCIL_PRIMS or n.op in ("field", "scalar"):
                 arr = self.t()
                 body.append(f"float {arr}[{n.nc}];")
                 self.slow_value(n, "i", "j", "k", arr, body)

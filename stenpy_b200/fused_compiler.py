@@ -33,11 +33,15 @@ from typing import Any, Dict, List, Optional, Sequence, Set, Tuple
 import torch
 
 from . import _native as N
-from .codegen import (ESIZE, SHELL_THREADS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec, analyse_ghosts,
-                      emit_pass, param_layout, pass_grid, shell_count, shell_regions, smem_layout, tmap_specs)
+from .codegen import (ESIZE, SHELL_THREADS, STENCIL_PRIMS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec,
+                      analyse_ghosts, emit_pass, param_layout, pass_grid, shell_count, shell_regions, smem_layout,
+                      tmap_specs)
 from .graph import Graph
 from .lowering import LoweringError, OpLowerer, dx3
 from .registry import KNOWN_OPS
+
+MAX_RING_SLOTS = 16         # one 8-byte mbarrier per plane-ring slot in a 128-byte block
+MAX_SMEM_BYTES = 227 * 1024  # dynamic shared memory one CTA may opt into on sm_100a
 
 TORCH_DT = {torch.float32: "f32", torch.float64: "f64", torch.bfloat16: "bf16", torch.float16: "f16"}
 DT_TORCH = {v: k for k, v in TORCH_DT.items()}
@@ -359,7 +363,7 @@ class Planner:
                     mark(y)
 
         for n in pg.nodes:
-            if n.op in ("d1", "lap"):
+            if n.op in STENCIL_PRIMS:
                 mark(n.ins[0])
         offset_read = {pg.nodes[x].a("field") for x in staged if pg.nodes[x].op == "field"}
         cfg = PassConfig(**vars(self.cfg))
@@ -381,6 +385,10 @@ class Planner:
                 f.tma = f.staged = False     # flat pass: vector loads straight from HBM
         if self.ghosts:
             analyse_ghosts(spec)
+        if 2 * radius + 1 + cfg.prefetch > MAX_RING_SLOTS:
+            raise FusionError(f"stencil reach {radius} needs more than {MAX_RING_SLOTS} plane-ring slots")
+        if smem_layout(spec)[0] > MAX_SMEM_BYTES:
+            raise FusionError(f"stencil reach {radius}: the plane rings exceed {MAX_SMEM_BYTES} B of shared memory")
         return PassPlan(spec, field_nodes, out_nodes, reductions, hists)
 
     def _scalar_source(self, sinks: Dict[str, int]) -> str:

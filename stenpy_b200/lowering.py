@@ -16,7 +16,15 @@ Each operator keeps the reference CPU path's boundary conventions:
   with edge order 2 when every axis has ≥ 3 points, else 1, boundary ignored
   (stenpy_engine.py:2037-2130, 2133-2177);
 * ``mean_curvature`` — gradient_nd, normalise by max(|∇f|, eps), then
-  ``divergence`` with the requested boundary (stenpy_engine.py:2180-2197).
+  ``divergence`` with the requested boundary (stenpy_engine.py:2180-2197);
+* ``material_derivative`` — Σ_d v[..., d] · gradient_nd(f)[..., d]
+  (stenpy_engine.py:2223-2244);
+* ``moving_average`` — a window³ box mean, the per-axis 1-D means of the
+  reference composed, each axis padded by the ``_pad1d`` rule (default neumann)
+  (stenpy_engine.py:2385-2408);
+* ``conv3d_spectral`` — the 27-point Gaussian (1-2-1)⊗(1-2-1)⊗(1-2-1)/64 as a
+  circular convolution, whatever the boundary: the reference's CPU path multiplies
+  FFTs (stenpy_engine.py:2800-2860).
 """
 from __future__ import annotations
 
@@ -27,6 +35,9 @@ from .codegen import PGraph
 
 class LoweringError(ValueError):
     pass
+
+
+MAX_TAP_REACH = 4   # widest weighted-tap stencil (window 9): the plane ring holds 2R+1+P slots
 
 
 def dx3(dx: Any) -> Tuple[float, float, float]:
@@ -103,6 +114,13 @@ class OpLowerer:
         rad = self.r(x) + (0 if mode == "zero" else 1)
         return self.pg.add("d1", (x,), nc, rad, axis=axis, mode=mode, comp=comp,
                            inv2h=1.0 / (2.0 * h), invh=1.0 / h)
+
+    def taps(self, x: int, reach: int, taps: Sequence[Tuple[int, int, int, float]], scale: float,
+             pad: str) -> int:
+        """Weighted sum of ``x`` at offsets (di, dj, dk) within ``reach`` of the voxel,
+        times ``scale``; out-of-range offsets follow the padding rule ``pad``."""
+        return self.pg.add("taps", (x,), self.nc(x), self.r(x) + reach, taps=tuple(taps),
+                           scale=float(scale), pad=pad, reach=reach)
 
     def stack(self, xs: Sequence[int]) -> int:
         return self.pg.add("stack", tuple(xs), sum(self.nc(x) for x in xs), self.r(*xs))
@@ -257,4 +275,51 @@ class OpLowerer:
             nh = self.pg.add("normalize", (g,), 3, self.r(g), eps=float(p.get("eps", 1e-15)))
             t = [self.d1(nh, a, _strict_edge2(bnd, self.shape[a], op), h[a], comp=a) for a in range(3)]
             return self.binop("add", self.binop("add", t[0], t[1]), t[2])
+        if op == "material_derivative":
+            need(2); no_extra("dx", "boundary")
+            f, v = ins
+            if self.nc(f) != 1 or self.nc(v) != 3:
+                raise LoweringError("material_derivative: needs a scalar field and a (*, 3) velocity")
+            h = dx3(p.get("dx", 1.0))
+            mode = _gnd_mode(self.shape, op)
+            t = []
+            for d in range(3):
+                vd = self.component(v, d)
+                if vd is None:
+                    vd = self.pg.add("select", (v,), 1, self.r(v), index=d)
+                t.append(self.binop("mul", vd, self.d1(f, d, mode, h[d])))
+            return self.binop("add", self.binop("add", t[0], t[1]), t[2])
+        if op == "moving_average":
+            need(1); no_extra("window", "boundary")
+            x = ins[0]
+            if self.nc(x) != 1:
+                raise LoweringError("moving_average: scalar fields only")
+            w = int(p.get("window", 3))
+            if w < 1 or w % 2 == 0:
+                raise LoweringError(f"moving_average: window must be odd and positive, got {w}")
+            rr = w // 2
+            if rr > MAX_TAP_REACH:
+                raise LoweringError(f"moving_average: window {w} exceeds {2 * MAX_TAP_REACH + 1}")
+            bnd = str(p.get("boundary", "neumann"))
+            pad = _pad_mode(bnd)
+            for n in self.shape:
+                if pad == "periodic" and rr > n:
+                    raise LoweringError(f"moving_average: circular padding of {rr} wider than an axis of {n}")
+                if pad == "reflect" and rr >= n:
+                    raise LoweringError(f"moving_average: reflect padding of {rr} needs axes longer than {rr}")
+            if rr == 0:    # window 1: the field itself
+                return self.pg.add("mulk", (x,), 1, self.r(x), k=1.0)
+            rng = range(-rr, rr + 1)
+            return self.taps(x, rr, [(a, b, c, 1.0) for a in rng for b in rng for c in rng],
+                             (1.0 / w) ** 3, pad)
+        if op == "conv3d_spectral":
+            need(1); no_extra("dx", "boundary")
+            x = ins[0]
+            if self.nc(x) != 1:
+                raise LoweringError("conv3d_spectral: scalar fields only")
+            if min(self.shape) < 3:
+                raise LoweringError(f"conv3d_spectral: axes need >= 3 points, got {self.shape}")
+            rng = (-1, 0, 1)
+            return self.taps(x, 1, [(a, b, c, float(2 ** (3 - abs(a) - abs(b) - abs(c))))
+                                    for a in rng for b in rng for c in rng], 1.0 / 64.0, "periodic")
         raise LoweringError(f"no lowering for operator '{op}'")

@@ -78,6 +78,10 @@ KNOWN_OPS: Dict[str, OpSpec] = {
     "divergence": OpSpec("stencil", 1, True), "curl": OpSpec("stencil", 1, True),
     "hessian": OpSpec("stencil", 2, True), "mean_curvature": OpSpec("stencil", 2, True),
     "grad_mag": OpSpec("stencil", 1, True), "jacobian": OpSpec("stencil", 1, True),
+    "material_derivative": OpSpec("stencil", 1, True),
+    # box and Gaussian smoothing (stenpy_engine.py:2385-2408, 2755-2860); the reach of
+    # moving_average is window // 2
+    "moving_average": OpSpec("stencil", 1), "conv3d_spectral": OpSpec("stencil", 1),
     # global reductions (stenpy_engine.py:2340-2459, 2546-2667)
     "sum": OpSpec("reduction"), "mean": OpSpec("reduction"), "norm_l2": OpSpec("reduction"),
     "variance": OpSpec("reduction"), "entropy": OpSpec("reduction"),
@@ -97,8 +101,9 @@ NO_STENCIL_OPS = {
     "select_component", "norm_last", "div_last", "neg_stack3", "scale_eye",
     "velocity_dot_grad", "integrate", "cumulative_integral", "spectral_gradient",
     "spectral_laplacian",
-    # added
-    "cos", "abs", "entropy_hist",
+    # added (conv3d_spectral accepts no dx: the reference's expression path passes one
+    # and fails, here the op is reachable from expressions)
+    "cos", "abs", "entropy_hist", "conv3d_spectral",
 }
 
 
@@ -125,6 +130,8 @@ _BUILTINS: List[Tuple[str, int, str, int, int, int]] = [
     ("divergence", 1, "medium", 0, 0, 0), ("curl", 1, "high", 0, 0, 0),
     ("hessian", 2, "very_high", 0, 0, 0), ("mean_curvature", 2, "very_high", 0, 0, 0),
     ("grad_mag", 1, "medium", 0, 0, 0), ("jacobian", 1, "high", 0, 0, 0),
+    ("material_derivative", 1, "high", 0, 0, 0), ("moving_average", 0, "medium", 0, 0, 0),
+    ("conv3d_spectral", 0, "very_high", 2, 8, 8),
     ("trace", 0, "low", 0, 0, 0), ("eigenvalues", 0, "very_high", 0, 0, 0),
     ("select_component", 0, "low", 0, 0, 0),
     ("sum", 0, "low", 0, 0, 0), ("mean", 0, "low", 0, 0, 0), ("norm_l2", 0, "low", 0, 0, 0),

@@ -110,10 +110,46 @@ def all_sources():
         src += plan_sources(g, list(sinks.values()))
         g, sink, *_ = S.compile_expression("entropy_hist(f)", field_map={"f": _ph((8, 9, 16), dt)})
         src += plan_sources(g, [sink])
+    # smoothing / advection stencils
+    S4 = [(5, 7, 33), (17, 9, 130), (9, 33, 97), (3, 3, 3)]
+    for shape in S4:
+        for w in (3, 5):
+            for b in ("neumann", "periodic", "dirichlet", "reflect"):
+                g, sink, *_ = S.compile_expression(f"moving_average(f, window={w}, boundary='{b}')",
+                                                   boundary="periodic", field_map={"f": _ph(shape)})
+                src += plan_sources(g, [sink])
+        for dt in (torch.float32, torch.bfloat16):
+            g, sink, *_ = S.compile_expression("conv3d_spectral(f)", boundary="periodic",
+                                               field_map={"f": _ph(shape, dt)})
+            src += plan_sources(g, [sink]) + plan_sources(g, [sink], torch.bfloat16)
+    for shape in S4 + [(2, 40, 64)]:
+        for b in ("neumann", "periodic"):
+            for e in ("material_derivative(f, u)", "material_derivative(f*f, curl(u)) + f")[:1 + (min(shape) >= 3)]:
+                g, sink, *_ = S.compile_expression(e, boundary=b, field_map={"f": _ph(shape),
+                                                                             "u": _ph(shape + (3,))})
+                src += plan_sources(g, [sink])
+    for shape in [(20, 33, 130), (7, 12, 45)]:
+        for e in ("moving_average(laplacian(f)) + conv3d_spectral(g)*2",
+                  "laplacian(moving_average(f, window=3, boundary='periodic'))",
+                  "conv3d_spectral(tanh(f)) - moving_average(g, window=5, boundary='reflect')"):
+            for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8)):
+                g, sink, *_ = S.compile_expression(e, boundary="periodic", field_map={"f": _ph(shape), "g": _ph(shape)})
+                src += plan_sources(g, [sink], torch.float32, PassConfig(tj=tj, tk=tk, threads=128, seg_len=8, kv=kv))
+    g, sinks, *_ = S.compile_expressions({"a": "sum(f + 2)", "b": "sum(conv3d_spectral(f + 2))",
+                                          "c": "sum(moving_average(f + 2, window=3, boundary='periodic'))"},
+                                         boundary="periodic", field_map={"f": _ph((256,) * 3)})
+    src += plan_sources(g, list(sinks.values()))
+    for e in ("conv3d_spectral(f)", "moving_average(f, window=5)", "moving_average(f, boundary='periodic')"):
+        for shape in ((33, 21, 45), (40, 24, 80), (37, 24, 64)):
+            g, sink, *_ = S.compile_expression(e, boundary="periodic", field_map={"f": _ph(shape)})
+            src += plan_sources(g, [sink])
     # batched executor: per-job runtime plans and the batch modules of the tests
     import test_gpu_batch as TB
+    smooth = [(e, torch.float32, [(33, 21, 45), (40, 24, 80)][i % 2], 0) for i, e in
+              enumerate(["conv3d_spectral(f)", "moving_average(f, window=5)",
+                         "moving_average(f, boundary='periodic')"] * 2)]
     for specs, threads in ((TB._mixed_specs(), 128), (TB._mixed_specs(), 256),
-                           (batch_specs(48, seed=7, lo=32, hi=72), 128)):
+                           (batch_specs(48, seed=7, lo=32, hi=72), 128), (smooth, 128)):
         jobs = []
         for e, dt, shape, _ in specs:
             full = tuple(shape) + ((3,) if e.startswith("curl") else ())

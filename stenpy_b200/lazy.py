@@ -72,6 +72,20 @@ def slab_pieces(c: Chunk, n0: int) -> List[Tuple[int, int, int]]:
     return pieces
 
 
+def wraps_dim0(spec) -> bool:
+    """Whether a pass reads across the dim-0 faces with periodic wrap (then every
+    chunk's slab must hold the wrapped planes): a periodic first derivative along
+    dim 0, a periodic Laplacian, or periodic taps with a dim-0 offset."""
+    for n in spec.graph.nodes:
+        if n.op == "d1" and n.a("axis") == 0 and n.a("mode") == "periodic":
+            return True
+        if n.op == "lap" and n.a("pad") == "periodic":
+            return True
+        if n.op == "taps" and n.a("pad") == "periodic" and any(t[0] for t in n.a("taps")):
+            return True
+    return False
+
+
 def pass_halo(pp: FC.PassPlan) -> int:
     R = pp.spec.radius
     onesided = any(n.op == "d1" and n.a("mode") in ("edge2", "edge1") for n in pp.spec.graph.nodes)
@@ -143,7 +157,9 @@ class LazyPipeline:
             FC.compile_pass(pp, dev_idx)
             H = pass_halo(pp)
             C = self._choose_chunk(pp, H)
-            chunks = plan_chunks(self.n0, C, H, self.periodic)
+            # a pass that wraps along dim 0 always gets wrapped slabs, whatever the
+            # caller's ``periodic`` says (its slow path reads planes across the faces)
+            chunks = plan_chunks(self.n0, C, H, self.periodic or wraps_dim0(pp.spec))
             maxslab = max(c.hi - c.lo for c in chunks)
             spec = pp.spec
             cfg = spec.cfg

@@ -89,6 +89,8 @@ def test_plan_structure_config1():
     ("eigenvalues(hessian(f)) + 0*mean_curvature(f)", "neumann"),
     ("curl(u) * 2", "dirichlet"),
     ("cumulative_integral(exp(f)) + integrate(g) + entropy(f) + variance(g)", "periodic"),
+    ("material_derivative(f, u) + conv3d_spectral(g) + moving_average(f, window=5, boundary='dirichlet')",
+     "neumann"),
 ])
 def test_generated_kernels_compile_for_sm100a(expr, boundary):
     fm = {"f": torch.zeros(20, 24, 32), "g": torch.zeros(20, 24, 32, dtype=torch.bfloat16),
@@ -123,6 +125,8 @@ def test_cpu_device_is_rejected():
     ("laplacian(f) + gradient(f)*0 + curl(u)", "neumann"),
     ("laplacian(f)", "periodic"),
     ("eigenvalues(hessian(f))", "periodic"),
+    ("conv3d_spectral(f) + moving_average(f, window=5)", "neumann"),
+    ("laplacian(f) + moving_average(f, window=9, boundary='reflect')", "periodic"),
 ])
 def test_every_tma_x_coordinate_is_16_byte_aligned(dtype, expr, boundary):
     """The x coordinate of each tiled TMA load must be a multiple of 16 bytes (an
@@ -279,3 +283,41 @@ def test_shipped_cost_model_matches_feature_layout():
         assert int(z[f"m{i}_in_dim"]) == d
         assert z[f"m{i}_params"].size == d * h + h + h * h + h + h + 1
         assert np.isfinite(z[f"m{i}_params"]).all()
+
+
+def test_smoothing_plans_and_limits():
+    """Weighted-tap stencils: reach = window // 2, no ghost cells (every face goes to
+    the shell kernel), the widest window and the ring-slot bound raise FusionError,
+    and chunked runs wrap dim 0 exactly when a pass reads across it periodically."""
+    from stenpy_b200.lazy import wraps_dim0
+    f = torch.zeros(16, 20, 32)
+    u = torch.zeros(16, 20, 32, 3)
+
+    def plan(expr, boundary="neumann"):
+        g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map={"f": f, "u": u})
+        return FC.Planner(g, [sink]).plan()
+
+    p = plan("moving_average(f, window=5)")
+    spec = p.passes[0].spec
+    assert spec.radius == 2 and spec.ghosts is None
+    assert [n.a("pad") for n in spec.graph.nodes if n.op == "taps"] == ["replicate"]
+    assert not wraps_dim0(spec)
+    assert wraps_dim0(plan("conv3d_spectral(f)").passes[0].spec)
+    assert wraps_dim0(plan("laplacian(f)", "periodic").passes[0].spec)
+    assert not wraps_dim0(plan("curl(u)", "periodic").passes[0].spec)
+    taps = [n for n in plan("conv3d_spectral(f)").passes[0].spec.graph.nodes if n.op == "taps"][0]
+    assert len(taps.a("taps")) == 27 and sum(t[3] for t in taps.a("taps")) * taps.a("scale") == 1.0
+    assert plan("moving_average(f, window=9)").passes[0].spec.radius == 4
+    for bad in ("moving_average(f, window=11)", "moving_average(f, window=4)"):
+        with pytest.raises(FC.FusionError):
+            plan(bad)
+    # reach 8 needs 19 ring slots (nested keyword arguments do not parse, as in the
+    # reference: the graph is built directly)
+    g, sink, *_ = S.compile_expression("moving_average(f, window=9)", field_map={"f": f})
+    outer = g.add("moving_average", (sink,), {"window": 9})
+    with pytest.raises(FC.FusionError, match="ring"):
+        FC.Planner(g, [outer]).plan()
+    with pytest.raises(FC.FusionError):     # reflect padding wider than an axis
+        g, sink, *_ = S.compile_expression("moving_average(f, window=7, boundary='reflect')",
+                                           field_map={"f": torch.zeros(3, 20, 32)})
+        FC.Planner(g, [sink]).plan()

@@ -66,7 +66,9 @@ def test_material_derivative_against_oracle(boundary):
 
 def test_smoothing_fused_with_other_stencils_under_every_schedule():
     """Taps nested under and over other stencils, several taps nodes in one pass, and
-    the same voxels under thread mappings with 1, 2 and 4 voxels per thread."""
+    the same voxels under thread mappings with 1, 2 and 4 voxels per thread. Nested
+    stencils are inlined per offset, so the compiler may contract a different set of
+    multiply-adds per schedule: schedules agree to FP32 rounding, not bit for bit."""
     from stenpy_b200.codegen import PassConfig
     from stenpy_b200.synth import sinusoid_field, uniform_field
     exprs = ["moving_average(laplacian(f)) + conv3d_spectral(g)*2",
@@ -79,7 +81,7 @@ def test_smoothing_fused_with_other_stencils_under_every_schedule():
             outs = [_check(expr, {"f": f, "g": g}, cfg=PassConfig(tj=tj, tk=tk, threads=128, seg_len=8, kv=kv))
                     for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8))]
             for o in outs[1:]:
-                assert torch.equal(o, outs[0]), (expr, shape, (o - outs[0]).abs().max().item())
+                assert rel_err(o, outs[0]) <= 2e-6, (expr, shape, rel_err(o, outs[0]))
 
 
 def test_smoothing_preserves_the_sum_at_256():

@@ -233,6 +233,17 @@ def moving_average(t, window: int = 3, boundary: str = "neumann"):
     return out
 
 
+def surface_normals(t, dx=1.0, boundary="neumann"):
+    """Unit normals (−∂₀t, −∂₁t, 1)/max(|·|, 1e-15) of a 2-D height field with
+    torch.gradient's edge order 2, boundary ignored (stenpy_engine.py:2199-2220)."""
+    if t.ndim != 2:
+        raise ValueError(f"surface_normals: expected 2D field, got {t.ndim}D")
+    h = (float(dx),) * 2 if isinstance(dx, (int, float)) else tuple(float(v) for v in dx)
+    gx, gy = torch.gradient(t, spacing=h, edge_order=2)
+    n = torch.stack([-gx, -gy, torch.ones_like(gx)], dim=-1)
+    return n / torch.linalg.norm(n, dim=-1, keepdim=True).clamp(min=1e-15)
+
+
 def conv3d_spectral(a, boundary: str = "periodic"):
     """The 27-point Gaussian (1,2,1)⊗(1,2,1)⊗(1,2,1)/64 as a circular convolution,
     whatever ``boundary`` says: the reference's CPU path multiplies FFTs
@@ -379,6 +390,7 @@ OPS: Dict[str, Callable] = {
     "hessian": hessian, "jacobian": jacobian, "mean_curvature": mean_curvature,
     "grad_mag": grad_mag, "gradient_nd": gradient_nd, "material_derivative": material_derivative,
     "moving_average": moving_average, "conv3d_spectral": conv3d_spectral,
+    "surface_normals": surface_normals,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

@@ -106,7 +106,8 @@ def features(spec: PassSpec, shape: Sequence[int]) -> Dict[str, float]:
         ops[n.op] = ops.get(n.op, 0) + 1
         if n.op == "taps":
             ops["lap"] = ops.get("lap", 0) + len(n.a("taps")) / 7.0
-    trans = sum(ops.get(k, 0) for k in ("exp", "log", "sqrt", "sin", "cos", "tanh", "normalize", "norm", "eig"))
+    trans = sum(ops.get(k, 0) for k in ("exp", "log", "sqrt", "sin", "cos", "tanh", "normalize", "norm", "eig",
+                                        "surfnorm"))
     arith = sum(ops.get(k, 0) for k in ("add", "sub", "mul", "div", "neg", "abs", "clamp", "mulk", "trace",
                                         "select", "stack"))
     in_bytes = sum(ESIZE[f.dtype] * f.nc for f in spec.fields)

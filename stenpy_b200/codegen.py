@@ -10,7 +10,8 @@ Primitives (every graph operator is lowered onto these, see ``lowering.py``):
 
 * ``field`` / ``scalar`` leaves;
 * pointwise math: add sub mul div neg exp log sqrt sin cos tanh abs clamp, trace,
-  eig (3×3 symmetric eigenvalues), select, stack, normalize, norm;
+  eig (3×3 symmetric eigenvalues), select, stack, normalize, norm, surfnorm
+  ((−a, −b, 1)/|·|);
 * ``d1``: first derivative of (one component of) a node along one axis, with the
   edge rule of the operator that produced it — ``periodic`` (wrapped central
   difference, torch.roll semantics), ``edge2`` / ``edge1`` (torch.gradient's
@@ -384,6 +385,13 @@ class _Emitter:
             out.append(f"{m} = fmaxf({m}, {_lit(n.a('eps', 1e-15))});")
             for c in range(3):
                 out.append(f"{o}[{c}] = {a}[{c}] / {m};")
+        elif op == "surfnorm":
+            gx, gy = ins[0] + "[0]", ins[1] + "[0]"
+            m = self.t()
+            out.append(f"const float {m} = fmaxf(sqrtf({gx}*{gx} + {gy}*{gy} + 1.0f), 1e-15f);")
+            out.append(f"{o}[0] = -{gx} / {m};")
+            out.append(f"{o}[1] = -{gy} / {m};")
+            out.append(f"{o}[2] = 1.0f / {m};")
         elif op == "norm":
             a = ins[0]
             out.append(f"{o}[0] = sqrtf({' + '.join(f'{a}[{c}]*{a}[{c}]' for c in range(self.g.nodes[n.ins[0]].nc))});")

@@ -40,6 +40,10 @@ from .graph import Graph
 from .lowering import LoweringError, OpLowerer, dx3
 from .registry import KNOWN_OPS
 
+# operators fused on 2-D fields besides the pointwise ones (the reference's 2-D-only
+# surface_normals, and global reductions of the values)
+OPS_2D = {"surface_normals", "sum", "mean", "norm_l2", "variance", "entropy", "min_max", "entropy_hist"}
+
 MAX_RING_SLOTS = 16         # one 8-byte mbarrier per plane-ring slot in a 128-byte block
 MAX_SMEM_BYTES = 227 * 1024  # dynamic shared memory one CTA may opt into on sm_100a
 
@@ -59,7 +63,9 @@ class FusionError(ValueError):
 
 
 def is_field_value(v: Any) -> bool:
-    return isinstance(v, torch.Tensor) and v.ndim >= 3
+    """A per-voxel input: a 3-D grid (scalar, (*, 3) or (*, 3, 3)) or a 2-D scalar
+    field, which runs as a grid of one plane."""
+    return isinstance(v, torch.Tensor) and v.ndim >= 2
 
 
 def is_scalar_value(v: Any) -> bool:
@@ -69,7 +75,7 @@ def is_scalar_value(v: Any) -> bool:
 
 def field_nc(shape: Sequence[int]) -> int:
     shape = tuple(shape)
-    if len(shape) == 3:
+    if len(shape) in (2, 3):
         return 1
     if len(shape) == 4 and shape[3] == 3:
         return 3
@@ -134,6 +140,11 @@ class FusedPlan:
     buffers: Dict[str, torch.Tensor] = dc_field(default_factory=dict)
     scalar_module: Optional[int] = None
     hist_size: int = 0
+    dims2: bool = False    # 2-D fields: the grid is (1, n0, n1), per-voxel results are (n0, n1, ...)
+
+    def out_shape(self, nc: int) -> Tuple[int, ...]:
+        """Shape of a per-voxel result with ``nc`` components."""
+        return (self.shape[1:] if self.dims2 else self.shape) + comp_shape(nc)
 
     def kernel_sources(self) -> List[str]:
         return [emit_pass(p.spec) for p in self.passes]
@@ -155,13 +166,17 @@ class Planner:
     def analyse(self) -> None:
         infos: Dict[str, _Info] = {}
         shape: Optional[Tuple[int, int, int]] = None
+        ndims = set()
         for nid in self.live:
             node = self.nodes[nid]
             op = node.op_name
             if op == "_constant":
                 v = node.params.get("value")
                 if is_field_value(v):
-                    s = tuple(int(x) for x in v.shape[:3])
+                    ndims.add(2 if v.ndim == 2 else 3)
+                    if len(ndims) > 1:
+                        raise FusionError("2-D and 3-D fields in one graph")
+                    s = (1,) + tuple(int(x) for x in v.shape) if v.ndim == 2 else tuple(int(x) for x in v.shape[:3])
                     if shape is None:
                         shape = s
                     elif s != shape:
@@ -178,6 +193,8 @@ class Planner:
             spec = KNOWN_OPS.get(op)
             if spec is None:
                 raise FusionError(f"operator '{op}' is not known to the fused executor")
+            if ndims == {2} and op not in OPS_2D and spec.kind != "pointwise":
+                raise FusionError(f"{op} on 2-D fields is not fused")
             ins = [infos[i] for i in node.input_ids]
             if spec.kind == "reduction":
                 if not ins or ins[0].kind in ("scalar", "red"):
@@ -207,6 +224,7 @@ class Planner:
                 raise FusionError("graph has no 3-D field input")
             shape = (1, 1, 1)  # scalar-only graph: evaluated by the scalar kernel alone
         self.infos, self.shape = infos, shape
+        self.dims2 = ndims == {2}
 
     def plan(self, key: str = "") -> FusedPlan:
         self.analyse()
@@ -246,11 +264,11 @@ class Planner:
         scalar_source = self._scalar_source(scalar_sinks) if scalar_sinks else None
         return FusedPlan(key, self.shape, infos, passes, self.table_size, self.const_index, self.red_index,
                          scalar_sinks, scalar_source, self.wanted, self.out_dtype, list(self.live),
-                         hist_size=self.hist_base)
+                         hist_size=self.hist_base, dims2=self.dims2)
 
     def _build_pass(self, roots: List[Tuple[str, str]]) -> PassPlan:
         pg = PGraph()
-        low = OpLowerer(pg, self.shape)
+        low = OpLowerer(pg, self.shape, dims2=self.dims2)
         slots: Dict[str, int] = {}
         field_nodes: List[str] = []
         fields: List[FieldSpec] = []
@@ -631,7 +649,7 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
         for (nid, okind, nc), r in zip(pp.out_nodes, [r for r in spec.roots if r.kind in ("out", "scan")]):
             o = outputs.get(nid) if (outputs and okind == "out") else None
             if o is None:
-                o = torch.empty((n0, n1, n2) + comp_shape(nc), dtype=DT_TORCH[r.out_dtype], device=device)
+                o = torch.empty(plan.out_shape(nc), dtype=DT_TORCH[r.out_dtype], device=device)
             outs.append(o)
             produced[nid] = o
             if nid in plan.wanted:

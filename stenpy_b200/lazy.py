@@ -104,6 +104,8 @@ class LazyPipeline:
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.plan = FC.Planner(graph, self.wanted, out_dtype, config).plan()
+        if self.plan.dims2:
+            raise FC.FusionError("lazy mode chunks 3-D fields along dim 0; 2-D fields run whole")
         if any(pp.spec.has_scan for pp in self.plan.passes):
             raise FC.FusionError("cumulative_integral is not supported in lazy mode")
         if self.plan.hist_size:

@@ -22,6 +22,8 @@ Each operator keeps the reference CPU path's boundary conventions:
 * ``moving_average`` — a window³ box mean, the per-axis 1-D means of the
   reference composed, each axis padded by the ``_pad1d`` rule (default neumann)
   (stenpy_engine.py:2385-2408);
+* ``surface_normals`` — 2-D fields only: (−∂₀f, −∂₁f, 1)/|·| with torch.gradient's
+  edge order 2 on both axes, boundary ignored (stenpy_engine.py:2199-2220);
 * ``conv3d_spectral`` — the 27-point Gaussian (1-2-1)⊗(1-2-1)⊗(1-2-1)/64 as a
   circular convolution, whatever the boundary: the reference's CPU path multiplies
   FFTs (stenpy_engine.py:2800-2860).
@@ -80,9 +82,10 @@ def _pad_mode(boundary: str) -> str:
 class OpLowerer:
     """Lower one graph op given already-lowered inputs. ``shape`` = (n0, n1, n2)."""
 
-    def __init__(self, pg: PGraph, shape: Tuple[int, int, int]):
+    def __init__(self, pg: PGraph, shape: Tuple[int, int, int], dims2: bool = False):
         self.pg = pg
         self.shape = shape
+        self.dims2 = dims2   # the fields are 2-D: shape is (1, n0, n1)
 
     def nc(self, nid: int) -> int:
         return self.pg.nodes[nid].nc
@@ -312,6 +315,23 @@ class OpLowerer:
             rng = range(-rr, rr + 1)
             return self.taps(x, rr, [(a, b, c, 1.0) for a in rng for b in rng for c in rng],
                              (1.0 / w) ** 3, pad)
+        if op == "surface_normals":
+            need(1); no_extra("dx", "boundary")
+            x = ins[0]
+            if not self.dims2:
+                raise LoweringError("surface_normals: expected a 2-D field, got a 3-D one")
+            if self.nc(x) != 1:
+                raise LoweringError("surface_normals: scalar fields only")
+            dx = p.get("dx", 1.0)
+            h = (float(dx),) * 2 if isinstance(dx, (int, float)) else tuple(float(v) for v in dx)
+            if len(h) != 2:
+                raise LoweringError(f"surface_normals: dx must be a number or 2 values, got {dx!r}")
+            if min(self.shape[1:]) < 3:
+                raise LoweringError(f"surface_normals: torch.gradient edge_order=2 needs >= 3 points per axis, "
+                                    f"got {self.shape[1:]}")
+            gx = self.d1(x, 1, "edge2", h[0])
+            gy = self.d1(x, 2, "edge2", h[1])
+            return self.pg.add("surfnorm", (gx, gy), 3, self.r(gx, gy))
         if op == "conv3d_spectral":
             need(1); no_extra("dx", "boundary")
             x = ins[0]

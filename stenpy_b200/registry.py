@@ -78,7 +78,7 @@ KNOWN_OPS: Dict[str, OpSpec] = {
     "divergence": OpSpec("stencil", 1, True), "curl": OpSpec("stencil", 1, True),
     "hessian": OpSpec("stencil", 2, True), "mean_curvature": OpSpec("stencil", 2, True),
     "grad_mag": OpSpec("stencil", 1, True), "jacobian": OpSpec("stencil", 1, True),
-    "material_derivative": OpSpec("stencil", 1, True),
+    "material_derivative": OpSpec("stencil", 1, True), "surface_normals": OpSpec("stencil", 1, True),
     # box and Gaussian smoothing (stenpy_engine.py:2385-2408, 2755-2860); the reach of
     # moving_average is window // 2
     "moving_average": OpSpec("stencil", 1), "conv3d_spectral": OpSpec("stencil", 1),
@@ -131,7 +131,7 @@ _BUILTINS: List[Tuple[str, int, str, int, int, int]] = [
     ("hessian", 2, "very_high", 0, 0, 0), ("mean_curvature", 2, "very_high", 0, 0, 0),
     ("grad_mag", 1, "medium", 0, 0, 0), ("jacobian", 1, "high", 0, 0, 0),
     ("material_derivative", 1, "high", 0, 0, 0), ("moving_average", 0, "medium", 0, 0, 0),
-    ("conv3d_spectral", 0, "very_high", 2, 8, 8),
+    ("conv3d_spectral", 0, "very_high", 2, 8, 8), ("surface_normals", 1, "high", 0, 0, 0),
     ("trace", 0, "low", 0, 0, 0), ("eigenvalues", 0, "very_high", 0, 0, 0),
     ("select_component", 0, "low", 0, 0, 0),
     ("sum", 0, "low", 0, 0, 0), ("mean", 0, "low", 0, 0, 0), ("norm_l2", 0, "low", 0, 0, 0),

@@ -63,6 +63,8 @@ S_MIX = (9, 10, 11)
 
 
 def _fields(shape, seed, names):
+    if len(shape) == 2:     # 2-D fields: the first plane of a one-plane 3-D field
+        return {k: v[0].contiguous() for k, v in _fields((1,) + tuple(shape), seed, names).items()}
     out = {}
     for n in names:
         if n == "f":
@@ -129,6 +131,11 @@ CASES = [
     ("gauss27", "conv3d_spectral(f)", "f", "periodic", 1.0, S_MIX),
     ("gauss27_odd", "conv3d_spectral(g)", "g", "neumann", 1.0, S_ODD),
     ("gauss27_of_expr", "conv3d_spectral(f*g + 1)", "fg", "periodic", 1.0, S_EVEN),
+    ("surfnorm_a", "surface_normals(f)", "f", "periodic", 1.0, (10, 11)),
+    ("surfnorm_dx", "surface_normals(f)", "f", "neumann", 0.5, (12, 16)),
+    ("surfnorm_small", "surface_normals(f*g)", "fg", "neumann", 1.0, (3, 5)),
+    ("field2d_reduce", "sum(f*f) + mean(g)", "fg", "periodic", 1.0, (9, 13)),
+    ("field2d_pointwise", "tanh(f)*exp(g) + f**2", "fg", "periodic", 1.0, (9, 13)),
 ]
 
 # The reference's expression path hands conv3d_spectral a ``dx`` it does not accept

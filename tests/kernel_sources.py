@@ -143,13 +143,21 @@ def all_sources():
         for shape in ((33, 21, 45), (40, 24, 80), (37, 24, 64)):
             g, sink, *_ = S.compile_expression(e, boundary="periodic", field_map={"f": _ph(shape)})
             src += plan_sources(g, [sink])
+    for dt in (torch.float32, torch.bfloat16):   # 2-D surface normals
+        for shape in [(3, 3), (5, 33), (40, 130), (64, 64), (37, 128)]:
+            for e, bnd in (("surface_normals(f)", "neumann"), ("surface_normals(f*f) * 2 + mean(f)", "periodic"),
+                           ("variance(tanh(f))", "periodic")):
+                g, sink, *_ = S.compile_expression(e, boundary=bnd, field_map={"f": _ph(shape, dt)})
+                src += plan_sources(g, [sink])
     # batched executor: per-job runtime plans and the batch modules of the tests
     import test_gpu_batch as TB
     smooth = [(e, torch.float32, [(33, 21, 45), (40, 24, 80)][i % 2], 0) for i, e in
               enumerate(["conv3d_spectral(f)", "moving_average(f, window=5)",
                          "moving_average(f, boundary='periodic')"] * 2)]
+    mixed2d = [("surface_normals(f)", torch.float32, (40, 130), 0), ("conv3d_spectral(f)", torch.float32, (20, 24, 80), 0),
+               ("surface_normals(f)", torch.float32, (64, 64), 0), ("laplacian(f)", torch.float32, (19, 37, 50), 0)]
     for specs, threads in ((TB._mixed_specs(), 128), (TB._mixed_specs(), 256),
-                           (batch_specs(48, seed=7, lo=32, hi=72), 128), (smooth, 128)):
+                           (batch_specs(48, seed=7, lo=32, hi=72), 128), (smooth, 128), (mixed2d, 128)):
         jobs = []
         for e, dt, shape, _ in specs:
             full = tuple(shape) + ((3,) if e.startswith("curl") else ())

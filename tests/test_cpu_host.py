@@ -321,3 +321,25 @@ def test_smoothing_plans_and_limits():
         g, sink, *_ = S.compile_expression("moving_average(f, window=7, boundary='reflect')",
                                            field_map={"f": torch.zeros(3, 20, 32)})
         FC.Planner(g, [sink]).plan()
+
+
+def test_2d_fields_plan_as_one_plane_grids():
+    """surface_normals needs 2-D fields (3-D raises, as in the reference); 2-D graphs
+    plan on a (1, n0, n1) grid with (n0, n1, ...) results; stencils other than the
+    surface normals, and 2-D next to 3-D fields, are not fused."""
+    f2 = torch.zeros(12, 20)
+    g, sink, *_ = S.compile_expression("surface_normals(f) * 2", field_map={"f": f2})
+    plan = FC.Planner(g, [sink]).plan()
+    assert plan.dims2 and plan.shape == (1, 12, 20) and plan.out_shape(3) == (12, 20, 3)
+    spec = plan.passes[0].spec
+    assert spec.radius == 1 and spec.ghosts is not None and spec.i_periodic
+    g, sink, *_ = S.compile_expression("surface_normals(f)", field_map={"f": torch.zeros(4, 5, 6)})
+    with pytest.raises(FC.FusionError, match="2-D"):
+        FC.Planner(g, [sink]).plan()
+    for expr in ("laplacian(f)", "integrate(f)"):
+        g, sink, *_ = S.compile_expression(expr, field_map={"f": f2})
+        with pytest.raises(FC.FusionError, match="2-D"):
+            FC.Planner(g, [sink]).plan()
+    g, sinks, *_ = S.compile_expressions({"a": "f*2", "b": "g*2"}, field_map={"f": f2, "g": torch.zeros(3, 12, 20)})
+    with pytest.raises(FC.FusionError, match="2-D and 3-D"):
+        FC.Planner(g, list(sinks.values())).plan()

@@ -1,6 +1,7 @@
-"""Smoothing and advection stencils on the fused executor — ``moving_average`` (box
-mean, every padding rule), ``conv3d_spectral`` (27-point Gaussian, circular) and
-``material_derivative`` — against the CPU FP64 oracle on the same stored values.
+"""Smoothing, advection and surface stencils on the fused executor —
+``moving_average`` (box mean, every padding rule), ``conv3d_spectral`` (27-point
+Gaussian, circular), ``material_derivative`` and ``surface_normals`` (2-D fields) —
+against the CPU FP64 oracle on the same stored values.
 
 Tolerance: norm-wise relative error <= 1e-5 for FP32-stored results (FP32 compute of
 at most 125 taps); BF16-stored results add the BF16 unit roundoff."""
@@ -137,3 +138,39 @@ def test_window_limits_raise():
     g, sink, *_ = S.compile_expression("moving_average(f, window=4)", field_map={"f": f})
     with pytest.raises(Exception, match="window"):
         S.Runtime(device=dev).run(g)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_surface_normals_on_2d_fields(dtype):
+    """2-D height fields run as one-plane grids; the normals come back (n0, n1, 3).
+    Shapes cover TMA rows (64 FP32 / 128 BF16 columns) and ragged ones."""
+    from stenpy_b200.synth import sinusoid_field
+    for shape in [(3, 3), (5, 33), (40, 130), (64, 64), (37, 128)]:
+        f = sinusoid_field((1,) + shape, seed=50)[0].contiguous().to(dtype)
+        got = _check("surface_normals(f)", {"f": f}, boundary="neumann")
+        assert tuple(got.shape) == shape + (3,)
+        _check("surface_normals(f*f) * 2 + mean(f)", {"f": f})
+        _check("variance(tanh(f))", {"f": f})
+
+
+def test_surface_normals_in_a_batch():
+    """2-D jobs next to 3-D ones in one persistent launch."""
+    import stenpy_b200 as S
+    from stenpy_b200 import batch as B
+    from stenpy_b200.synth import sinusoid_field
+    dev = _dev()
+    items = [("surface_normals(f)", (1, 40, 130)), ("conv3d_spectral(f)", (20, 24, 80)),
+             ("surface_normals(f)", (1, 64, 64)), ("laplacian(f)", (19, 37, 50))]
+    jobs, host = [], []
+    for i, (e, shape) in enumerate(items):
+        f = sinusoid_field(shape, seed=60 + i)
+        if shape[0] == 1:
+            f = f[0].contiguous()
+        g, sink, *_ = S.compile_expression(e, boundary="periodic", field_map={"f": f.to(dev)})
+        jobs.append(B.BatchJob(g, [sink]))
+        host.append((e, f, sink))
+    for (e, f, sink), res in zip(host, B.run_batch(jobs, dev)):
+        g2, s2, *_ = S.compile_expression(e, boundary="periodic", field_map={"f": f.double()})
+        ref = O.evaluate(g2, [s2])[s2]
+        assert tuple(res[sink].shape) == tuple(ref.shape)
+        assert rel_err(res[sink], ref) <= 1e-5, (e, tuple(f.shape))

@@ -151,6 +151,7 @@ class PassSpec:
 
 _REMAP_RULES = ("periodic", "replicate", "reflect")
 STENCIL_PRIMS = ("d1", "lap", "taps")   # primitives that read their input at offsets
+_EXTRAPOLATED = ("edge2", "edge1", "edge2x2")  # ghost rules that compute a value, not copy one
 
 
 def analyse_ghosts(spec: "PassSpec") -> None:
@@ -164,6 +165,8 @@ def analyse_ghosts(spec: "PassSpec") -> None:
     linear for edge order 1). Index-remap rules commute with pointwise ops, so they
     also apply through pointwise subexpressions; zero padding and extrapolation only
     when the stencil reads the field directly. Each (field, axis) must get one rule.
+    Extrapolated ghosts are only written into FP32/FP64 rings: a 16-bit ring would
+    round them.
     """
     g = spec.graph
     spec.ghosts = None
@@ -219,6 +222,10 @@ def analyse_ghosts(spec: "PassSpec") -> None:
             if g.nodes[x].op != "field":
                 continue
             slot = g.nodes[x].a("field")
+            if rule in _EXTRAPOLATED and spec.fields[slot].dtype in ("bf16", "f16"):
+                # the ring stores the field's own dtype: an extrapolated ghost would be
+                # rounded to 16 bits, so these faces are left to the shell kernel
+                return
             for ax in axes:
                 have = rules.setdefault((slot, ax), rule)
                 if have != rule:

@@ -110,6 +110,13 @@ def all_sources():
         src += plan_sources(g, list(sinks.values()))
         g, sink, *_ = S.compile_expression("entropy_hist(f)", field_map={"f": _ph((8, 9, 16), dt)})
         src += plan_sources(g, [sink])
+    for dt in (torch.float16, torch.bfloat16):   # 16-bit fields, one-sided edges, FP32 results
+        for shape in [(12, 20, 64), (9, 17, 37)]:
+            for e in ("curl(u)", "gradient(f) * 2", "_hessian(f)", "divergence(u) + laplacian(f)"):
+                for ghost in (True, False):
+                    g, sink, *_ = S.compile_expression(e, boundary="neumann", field_map={
+                        "f": _ph(shape, dt), "u": _ph(shape + (3,), dt)})
+                    src += plan_sources(g, [sink], torch.float32, PassConfig(ghost=ghost))
     # smoothing / advection stencils
     S4 = [(5, 7, 33), (17, 9, 130), (9, 33, 97), (3, 3, 3)]
     for shape in S4:

@@ -114,6 +114,27 @@ def test_kv_chunks_match_one_voxel_per_thread(dtype, boundary):
             assert abs(v - vref) <= 1e-12 * abs(vref), (key, v, vref)
 
 
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_16bit_fields_with_one_sided_edges_keep_fp32_accuracy(dtype):
+    """16-bit stored fields with FP32 results: one-sided edges must be formed from the
+    stored values in FP32 (an extrapolated ghost written into the 16-bit ring would be
+    rounded to 16 bits and show up as a ~1e-3 error at the faces)."""
+    import stenpy_b200 as S
+    from stenpy_b200.codegen import PassConfig
+    from stenpy_b200.synth import sinusoid_field, smoothed_vector
+    dev = _dev()
+    for shape in [(12, 20, 64), (9, 17, 37)]:
+        f = sinusoid_field(shape, seed=70).to(dtype)
+        u = smoothed_vector(shape, seed=71).to(dtype)
+        for expr in ("curl(u)", "gradient(f) * 2", "_hessian(f)", "divergence(u) + laplacian(f)"):
+            for ghost in (True, False):
+                g, sink, *_ = S.compile_expression(expr, boundary="neumann", field_map={"f": f.to(dev), "u": u.to(dev)})
+                got = S.Runtime(device=dev, config=PassConfig(ghost=ghost)).run(g)[sink]
+                g2, s2, *_ = S.compile_expression(expr, boundary="neumann", field_map={"f": f.double(), "u": u.double()})
+                ref = O.evaluate(g2, [s2])[s2]
+                assert rel_err(got, ref) <= 1e-5, (expr, shape, ghost, rel_err(got, ref))
+
+
 @pytest.mark.parametrize("tk,tj", [(32, 16), (64, 8)])
 @pytest.mark.parametrize("shape", [(10, 17, 65), (9, 33, 97), (12, 18, 66)])
 def test_second_derivative_ghosts_where_tile_halos_cross_faces(shape, tk, tj):

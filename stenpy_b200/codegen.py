@@ -93,6 +93,7 @@ class FieldSpec:
     halo: int = 0         # j/k halo of the staged tile (0 for fields read only at the voxel)
     wrap_k: bool = False  # periodic ghosts along dim 2 come from extra TMA strips
     wrap_j: bool = False  # periodic ghosts along dim 1 come from extra TMA strips
+    vec: int = 1          # cooperative staging: elements per asynchronous copy (row alignment)
 
 
 @dataclass
@@ -1073,6 +1074,212 @@ def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
     return K
 
 
+def _remap_line(var: str, n: str, rule: Optional[str], indent: str) -> List[str]:
+    if rule == "periodic":
+        return [f"{indent}{var} = wrap_idx({var}, {n});"]
+    if rule == "replicate":
+        return [f"{indent}{var} = clamp_idx({var}, {n});"]
+    if rule == "reflect":
+        return [f"{indent}if ({n} > 1) {var} = reflect_idx({var}, {n});"]
+    return []
+
+
+def lsu_vec(pitch_bytes: int, es: int) -> int:
+    """Elements per asynchronous copy for rows of ``pitch_bytes``: the widest copy
+    (4, 8 or 16 bytes) that every row start is aligned to, so that units inside a
+    row need no per-row alignment (16-bit rows of odd length use element pairs: every
+    other row is then copied element-wise)."""
+    a = 16
+    while a > es and pitch_bytes % a:
+        a //= 2
+    return max(a // es, 2 if es == 2 else 1)
+
+
+def _lsu_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig"):
+    w, h = spec.box(f)
+    es = ESIZE[f.dtype]
+    v = f.vec                        # elements per copy unit
+    u = w // v                       # units per row
+    tc, ncc, rp, nk = lsu_mapping(u, h, cfg.threads)
+    return w, h, es, v, u, tc, ncc, rp, nk
+
+
+def _lsu_elem(spec: "PassSpec", f: "FieldSpec", x: str, rule: Optional[str], ind: str, tag: str) -> List[str]:
+    """Global column of box column ``x`` (an element index inside the row): kg{tag},
+    component c{tag}, validity ok{tag}, byte offset off{tag} inside the row."""
+    es = ESIZE[f.dtype]
+    L = [f"{ind}const int xr{tag} = {x} - {spec.hk(f)} * {f.nc};",
+         f"{ind}int kg{tag} = tk0 + (xr{tag} >= 0 ? xr{tag} / {f.nc} : -((-xr{tag} + {f.nc} - 1) / {f.nc}));",
+         f"{ind}const int c{tag} = xr{tag} - (kg{tag} - tk0) * {f.nc};"]
+    L += _remap_line(f"kg{tag}", "p.n2", rule, ind)
+    L.append(f"{ind}const bool ok{tag} = kg{tag} >= 0 && kg{tag} < p.n2;")
+    L.append(f"{ind}const u32 off{tag} = ok{tag} ? (u32)((kg{tag} * {f.nc} + c{tag}) * {es}) : 0u;")
+    return L
+
+
+def _lsu_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -> List[str]:
+    """Per-tile column plan of a cooperatively staged field: for each copy unit
+    (``vec`` adjacent elements of a row) this thread copies in every row, its byte
+    offset inside the row after the dim-2 rule and its size (0: outside the grid, the
+    unit is zero). Units split by the rule (not adjacent in memory, or partly outside)
+    are marked for the element-wise path; ``lsu2`` says whether this thread can have
+    element-wise work at all (split units, or rows not aligned to the unit)."""
+    w, h, es, v, u, tc, ncc, rp, nk = _lsu_geometry(spec, f, cfg)
+    ub = v * es
+    sl = f.slot
+    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+    L = [f"// staging plan of field {sl}: {u} units of {v} element(s) per row, {h} rows",
+         f"const int c0{sl}_ = tid % {tc}, rs{sl}_ = tid / {tc};",
+         f"u32 coff{sl}_[{ncc}], csz{sl}_[{ncc}];"]
+    if v > 1:
+        L.append(f"bool cbad{sl}_[{ncc}];")
+        L.append(f"bool lsu2{sl}_ = ((p.n2 * {f.nc * es}) % {ub}) != 0 || (((size_t)p.fld[{sl}]) % {ub}) != 0;")
+    L.append(f"#pragma unroll\nfor (int cc = 0; cc < {ncc}; ++cc) {{")
+    L.append(f"  const int un = c0{sl}_ + cc * {tc};")
+    for e in range(v):
+        L += _lsu_elem(spec, f, f"un * {v} + {e}", rk, "  ", str(e))
+    if v == 1:
+        L.append(f"  coff{sl}_[cc] = off0; csz{sl}_[cc] = (un < {u} && ok0) ? {es}u : 0u;")
+    else:
+        allok = " && ".join(f"ok{e}" for e in range(v))
+        anyok = " || ".join(f"ok{e}" for e in range(v))
+        contig = " && ".join(f"off{e} == off0 + {e * es}u" for e in range(1, v))
+        L.append(f"  coff{sl}_[cc] = off0; csz{sl}_[cc] = ({allok}) ? {ub}u : 0u;")
+        L.append(f"  cbad{sl}_[cc] = un < {u} && (({anyok}) && !(({allok}) && {contig} && (off0 % {ub}u) == 0u));")
+        L.append(f"  lsu2{sl}_ = lsu2{sl}_ || cbad{sl}_[cc];")
+    L.append("}")
+    return L
+
+
+def _lsu_request(spec: "PassSpec", f: "FieldSpec", rings: Dict[int, int], cfg: "PassConfig",
+                 ghost: bool) -> List[str]:
+    """Staging of plane ``zq`` of a field whose rows TMA cannot describe, into ring
+    slot ``s``: every row (remapped by its dim-1 rule, or zero outside the grid) as
+    asynchronous copies of the planned units. Units that are split by the dim-2 rule
+    or whose global address is not aligned to the unit are copied element-wise after
+    that, loaded in groups before their stores."""
+    w, h, es, v, u, tc, ncc, rp, nk = _lsu_geometry(spec, f, cfg)
+    sl = f.slot
+    rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
+    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+    ct = CTYPE[f.dtype]
+    ub = v * es
+    L = ["{",
+         f"  const u32 sb = smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}) + "
+         f"(u32)((rs{sl}_ * {w} + c0{sl}_ * {v}) * {es});",
+         f"  const char* fb = (const char*)p.fld[{sl}];",
+         "  const bool zok = zq >= 0 && zq < p.nl;"]
+
+    def row(ind: str) -> List[str]:
+        R = [f"{ind}int jg = tj0 - {f.halo} + r;"]
+        R += _remap_line("jg", "p.n1", rj, ind)
+        R.append(f"{ind}const bool rok = zok && jg >= 0 && jg < p.n1;")
+        R.append(f"{ind}const char* rowb = fb + (rok ? ((size_t)zq * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es}) : (size_t)0);")
+        return R
+
+    guard_rs = rp * tc < cfg.threads
+    guard_r = nk * rp > h
+    guard_c = ncc * tc > u
+    zero = {4: "st_shared_u32({sa}, 0u);", 8: "st_shared_u64({sa}, 0ull);", 16: "st_shared_zero16({sa});"}[ub] \
+        if v > 1 else ""
+    # tiles whose box lies inside the field, on rows aligned to the unit: every unit is
+    # one full copy from a row pointer that advances by a fixed stride
+    pitch = f"((size_t)p.n2 * {f.nc * es})"
+    L.append(f"  if (zok && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && tk0 >= {spec.hk(f)} && "
+             f"tk0 + TK + {spec.hk(f)} <= p.n2 && {pitch} % {ub} == 0 && ((size_t)fb) % {ub} == 0) {{")
+    L.append(f"    if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{")
+    L.append(f"      const char* g = fb + ((size_t)zq * p.n1 + (tj0 - {f.halo} + rs{sl}_)) * {pitch} + "
+             f"(size_t)((tk0 - {spec.hk(f)}) * {f.nc * es} + c0{sl}_ * {ub});")
+    L.append(f"      const size_t rstep = {rp} * {pitch};")
+    for k in range(nk):
+        cond = [f"rs{sl}_ + {k * rp} < {h}"] if guard_r else []
+        body = []
+        for cc in range(ncc):
+            cc_cond = f"c0{sl}_ + {cc * tc} < {u}" if guard_c and cc == ncc - 1 else ""
+            st = f"cp_async_n<{ub}>(sb + {(k * rp * w + cc * tc * v) * es}u, g + {cc * tc * ub}, {ub}u);"
+            body.append(("if (" + cc_cond + ") " if cc_cond else "") + st)
+        pre = f"      if ({cond[0]}) {{ " if cond else "      { "
+        L.append(pre + " ".join(body) + (" g += rstep;" if k + 1 < nk else "") + " }")
+    L.append("    }")
+    L.append("  } else")
+    L.append(f"  if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{")
+    for k in range(nk):
+        L.append("    {")
+        L.append(f"      const int r = rs{sl}_ + {k * rp};")
+        if guard_r:
+            L.append(f"      if (r < {h}) {{")
+        ind = "        " if guard_r else "      "
+        L += row(ind)
+        if v == 1:
+            L.append(f"{ind}const u32 rsz = rok ? 0xffffffffu : 0u;")
+        for cc in range(ncc):
+            cond = f"c0{sl}_ + {cc * tc} < {u}" if guard_c and cc == ncc - 1 else ""
+            sa = f"sb + {(k * rp * w + cc * tc * v) * es}u"
+            if v == 1:
+                stmt = f"cp_async_n<{es}>({sa}, rowb + coff{sl}_[{cc}], csz{sl}_[{cc}] & rsz);"
+            else:
+                stmt = (f"{{ const char* gp = rowb + coff{sl}_[{cc}]; "
+                        f"if (!rok || (!cbad{sl}_[{cc}] && csz{sl}_[{cc}] == 0u)) {zero.format(sa=sa)} "
+                        f"else if (!cbad{sl}_[{cc}] && (((size_t)gp) % {ub}u) == 0) cp_async_n<{ub}>({sa}, gp, {ub}u); }}")
+            L.append(f"{ind}{'if (' + cond + ') ' if cond else ''}{stmt}")
+        if guard_r:
+            L.append("      }")
+        L.append("    }")
+    L.append("  }")
+    if v > 1:
+        # element-wise units: split by the dim-2 rule, or on rows not aligned to the unit
+        items = [(k, cc) for k in range(nk) for cc in range(ncc)]
+        G = max(1, 8 // v)
+        conds = [f"lsu2{sl}_"] + ([f"rs{sl}_ < {rp}"] if guard_rs else [])
+        L.append(f"  if ({' && '.join(conds)}) {{")
+        L.append(f"    {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
+        for g0 in range(0, len(items), G):
+            grp = items[g0:g0 + G]
+            L.append("    {")
+            L.append(f"      {ct} v_[{len(grp)}][{v}]; int d_[{len(grp)}];")
+            for t, (k, cc) in enumerate(grp):
+                L.append("      {")
+                L.append(f"        const int r = rs{sl}_ + {k * rp};")
+                L.append(f"        const int un = c0{sl}_ + {cc * tc};")
+                L.append(f"        d_[{t}] = -1;")
+                c2 = (["r < %d" % h] if guard_r else []) + (["un < %d" % u] if guard_c and cc == ncc - 1 else [])
+                L.append(f"        if ({' && '.join(c2) if c2 else 'true'}) {{")
+                L += row("          ")
+                L.append(f"          const char* gp = rowb + coff{sl}_[{cc}];")
+                L.append(f"          if (rok && (cbad{sl}_[{cc}] || (csz{sl}_[{cc}] != 0u && (((size_t)gp) % {ub}u) != 0))) {{")
+                L.append(f"            d_[{t}] = r * {w} + un * {v};")
+                L.append(f"            {ct} z_; " + ("z_.bits = 0;" if es == 2 else f"z_ = ({ct})0;"))
+                for e in range(v):
+                    L.append("            {")
+                    L += _lsu_elem(spec, f, f"un * {v} + {e}", rk, "              ", "")
+                    L.append(f"              v_[{t}][{e}] = ok ? ldg_raw((const {ct}*)(rowb + off)) : z_;")
+                    L.append("            }")
+                L.append("          }")
+                L.append("        }")
+                L.append("      }")
+            L.append(f"      #pragma unroll\n      for (int t_ = 0; t_ < {len(grp)}; ++t_)")
+            L.append("        if (d_[t_] >= 0) {")
+            for e in range(v):
+                L.append(f"          dst[d_[t_] + {e}] = v_[t_][{e}];")
+            L.append("        }")
+            L.append("    }")
+        L.append("  }")
+    L.append("}")
+    return L
+
+
+def lsu_mapping(w: int, h: int, nt: int) -> Tuple[int, int, int, int]:
+    """Thread mapping of the cooperative staging of a w × h element box: TC threads
+    per row, each owning CC columns (c0 + cc·TC) for every row it copies; RP rows in
+    parallel, each thread K rows (r0 + k·RP). Columns are fixed per thread, so their
+    global offsets and validity are computed once per tile, not per plane."""
+    tc = min(nt, w)
+    cc = -(-w // tc)
+    rp = nt // tc
+    k = -(-h // rp)
+    return tc, cc, rp, k
+
+
 def _ghost_expr2(at, n: str, side: str) -> str:
     """Second ghost layer of a second derivative with edge order 2 on both levels:
     f[-2] = 7f0 - 11f1 + 6f2 - f3 makes the inner central difference at -1 equal
@@ -1413,7 +1620,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     tma_fields = [f for f in spec.fields if f.tma]
     lsu_fields = [f for f in spec.fields if f.staged and not f.tma]
     # cooperative staging of 4-byte fields is asynchronous: one commit group per plane
-    async_lsu = any(ESIZE[f.dtype] in (2, 4) for f in lsu_fields)
+    async_lsu = any(ESIZE[f.dtype] in (2, 4, 8) for f in lsu_fields)
     total_smem, rings, red_off = smem_layout(spec)
     tma_bytes = sum(spec.box(f)[0] * spec.box(f)[1] * ESIZE[f.dtype] for f in tma_fields)
     reds = [r for r in spec.roots if r.kind == "red"]
@@ -1464,6 +1671,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
             K.append("  }")
             K.append("  __syncthreads();")
+        for f in lsu_fields:
+            K += ["  " + x for x in _lsu_plan(spec, f, cfg, ghost)]
         if staged:
             K.append("  auto request = [&](int q) {")
             K.append("    const int s = (q - p_first) % NSLOT;")
@@ -1505,67 +1714,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                                  f"(tk0 - {hk}) * {f.nc}, 0, zq);")
                 K.append("    }")
             for f in lsu_fields:
-                w, h = spec.box(f)
-                ct = CTYPE[f.dtype]
-                rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
-                rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-                hk = spec.hk(f)
-                et = -(-(w * h) // cfg.threads)
-                K.append("    {")
-                K.append(f"      {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
-                K.append(f"      const {ct}* src = (const {ct}*)p.fld[{f.slot}];")
-                # tile box inside the field: plain row-offset loads, issued in groups of 8
-                # before their shared-memory stores (one memory latency per group)
-                K.append(f"      if (zq >= 0 && zq < p.nl && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && "
-                         f"tk0 >= {hk} && tk0 + TK + {hk} <= p.n2) {{")
-                K.append(f"        const {ct}* rowp = src + (((size_t)zq * p.n1 + (tj0 - {f.halo})) * p.n2 + (tk0 - {hk})) * {f.nc};")
-                K.append(f"        const int pitch = p.n2 * {f.nc};")
-                if ESIZE[f.dtype] == 4:
-                    # 4-byte elements: asynchronous copies, completed by the wait before the
-                    # barrier that precedes the plane's first use (like the TMA ring)
-                    K.append(f"        #pragma unroll 4\n        for (int e = tid; e < {w * h}; e += NT) {{")
-                    K.append(f"          const int yy = e / {w}; cp_async4(dst + e, rowp + (yy * pitch + (e - yy * {w})));")
-                    K.append("        }")
-                elif ESIZE[f.dtype] == 2:
-                    # 2-byte elements: element pairs as 4-byte asynchronous copies on rows whose
-                    # global start is 4-byte aligned (the shared row always is); plain copies
-                    # on the others
-                    K.append(f"        #pragma unroll 4\n        for (int e2 = tid; e2 < {w // 2 * h}; e2 += NT) {{")
-                    K.append(f"          const int yy = e2 / {w // 2}, x2 = 2 * (e2 - yy * {w // 2});")
-                    K.append(f"          const {ct}* sr = rowp + yy * pitch + x2;")
-                    K.append(f"          {ct}* dr = dst + yy * {w} + x2;")
-                    K.append("          if ((((size_t)sr) & 3) == 0) cp_async4(dr, sr);")
-                    K.append("          else { dr[0] = ldg_raw(sr); dr[1] = ldg_raw(sr + 1); }")
-                    K.append("        }")
-                else:
-                    gsz = 4
-                    K.append(f"        #pragma unroll 1\n        for (int t0 = 0; t0 < {et}; t0 += {gsz}) {{")
-                    K.append(f"          {ct} v_[{gsz}];")
-                    K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
-                             f" if (e < {w * h}) {{ const int yy = e / {w}; v_[t] = ldg_raw(rowp + (yy * pitch + (e - yy * {w}))); }} }}")
-                    K.append(f"          #pragma unroll\n          for (int t = 0; t < {gsz}; ++t) {{ const int e = tid + (t0 + t) * NT;"
-                             f" if (e < {w * h}) dst[e] = v_[t]; }}")
-                    K.append("        }")
-                K.append("      } else")
-                K.append(f"      for (int e = tid; e < {w * h}; e += NT) {{")
-                K.append(f"        const int yy = e / {w}, xx = e - yy * {w};")
-                K.append(f"        int jg = tj0 - {f.halo} + yy;")
-                K.append(f"        const int xr = xx - {spec.hk(f)} * {f.nc};")
-                K.append(f"        int kg = tk0 + (xr >= 0 ? xr / {f.nc} : -((-xr + {f.nc} - 1) / {f.nc}));")
-                K.append(f"        const int c = xr - (kg - tk0) * {f.nc};")
-                for ax, var, n, rule in ((1, "jg", "p.n1", rj), (2, "kg", "p.n2", rk)):
-                    if rule == "periodic":
-                        K.append(f"        {var} = wrap_idx({var}, {n});")
-                    elif rule == "replicate":
-                        K.append(f"        {var} = clamp_idx({var}, {n});")
-                    elif rule == "reflect":
-                        K.append(f"        if ({n} > 1) {var} = reflect_idx({var}, {n});")
-                K.append(f"        {ct} v; v.bits = 0;" if ESIZE[f.dtype] == 2 else f"        {ct} v = ({ct})0;")
-                K.append("        if (zq >= 0 && zq < p.nl && jg >= 0 && jg < p.n1 && kg >= 0 && kg < p.n2)")
-                K.append(f"          v = src[(((size_t)zq * p.n1 + jg) * p.n2 + kg) * {f.nc} + c];")
-                K.append("        dst[e] = v;")
-                K.append("      }")
-                K.append("    }")
+                K += ["    " + x for x in _lsu_request(spec, f, rings, cfg, ghost)]
             K.append("  };")
             if ghost:
                 K += ["  " + x for x in _ghost_fill(spec, rings)]
@@ -1706,18 +1855,24 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         for f in spec.fields:
             if not f.staged:
                 K.append(f"    frow{f.slot} += plane_n * {f.nc};")
-        # the next plane (i+1+RAD) must be resident and ghosted before the barrier
+        # the next plane (i+1+RAD) must be resident and ghosted before the barrier;
+        # ghosts derived from cooperatively staged (asynchronous) rows wait for every
+        # thread's copies: an extra barrier, in edge tiles only
+        lsu_ghost = ghost and any(
+            (spec.ghosts or {}).get((f.slot, ax)) in _EXTRAPOLATED for f in lsu_fields for ax in (1, 2))
         if tma_fields or (ghost and staged):
             K.append("    if (i + 1 < ie) {")
             if tma_fields:
                 K.append("      const int rel = i + 1 + RAD - p_first;")
                 K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-            if ghost and staged:
+            if ghost and staged and not lsu_ghost:
                 K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
             K.append("    }")
         if async_lsu:
             # this thread's copies of plane i+1+RAD (issued PREFETCH iterations ago) are done
             K.append(f"    cp_async_wait<{cfg.prefetch - 1}>();")
+        if lsu_ghost:
+            K.append("    if (edge_cta) { __syncthreads(); if (i + 1 < ie) ghost_fill(i + 1 + RAD); }")
         if staged:
             # the ring slot of plane i - RAD is refilled next: every thread must be done with it
             K.append("    ok = __syncthreads_and(ok);")

@@ -183,6 +183,18 @@ STEN_DEV void fence_mbar_init() {
 STEN_DEV void cp_async4(void* smem_dst, const void* gsrc) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
 }
+// asynchronous copy of N (4, 8 or 16) bytes to the shared address sdst, of which the
+// first src_bytes come from gsrc and the rest are zero (src_bytes 0: nothing is read;
+// gsrc must still be a mapped, N-aligned address)
+template <int N> STEN_DEV void cp_async_n(u32 sdst, const void* gsrc, u32 src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;"
+               :: "r"(sdst), "l"(gsrc), "n"(N), "r"(src_bytes) : "memory");
+}
+STEN_DEV void st_shared_u32(u32 saddr, u32 v) { asm volatile("st.shared.u32 [%0], %1;" :: "r"(saddr), "r"(v) : "memory"); }
+STEN_DEV void st_shared_u64(u32 saddr, u64 v) { asm volatile("st.shared.u64 [%0], %1;" :: "r"(saddr), "l"(v) : "memory"); }
+STEN_DEV void st_shared_zero16(u32 saddr) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" :: "r"(saddr), "r"(0u) : "memory");
+}
 STEN_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> STEN_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 STEN_DEV void fence_proxy_async() {

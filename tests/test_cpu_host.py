@@ -343,3 +343,152 @@ def test_2d_fields_plan_as_one_plane_grids():
     g, sinks, *_ = S.compile_expressions({"a": "f*2", "b": "g*2"}, field_map={"f": f2, "g": torch.zeros(3, 12, 20)})
     with pytest.raises(FC.FusionError, match="2-D and 3-D"):
         FC.Planner(g, list(sinks.values())).plan()
+
+
+def _emulate_staging(w, h, es, nc, halo, hk, tk0, tj0, n1, n2, rj, rk, nt, v, fb=0):
+    """Host model of the cooperative staging of one plane (the generated plan and
+    request code, formula for formula, both copy loops): returns {box element: global
+    element, or None for zero}, checking that every element is written once, every
+    global read is inside the field and every asynchronous copy is aligned."""
+    from stenpy_b200.codegen import lsu_mapping
+
+    def remap(x, n, rule):
+        if rule == "periodic":
+            return x + n if x < 0 else (x - n if x >= n else x)
+        if rule == "replicate":
+            return min(max(x, 0), n - 1)
+        if rule == "reflect" and n > 1:
+            x = -x if x < 0 else x
+            x = 2 * (n - 1) - x if x > n - 1 else x
+            return min(max(x, 0), n - 1)
+        return x
+
+    def elem(x):
+        xr = x - hk * nc
+        kg = tk0 + xr // nc
+        c = xr - (kg - tk0) * nc
+        kg = remap(kg, n2, rk)
+        ok = 0 <= kg < n2
+        return ok, ((kg * nc + c) * es if ok else 0)
+
+    ub = v * es
+    u = w // v
+    tc, ncc, rp, nk = lsu_mapping(u, h, nt)
+    pitch = n2 * nc * es
+    nbytes = n1 * pitch
+    out = {}
+
+    def put(dst, g):
+        assert dst not in out, ("written twice", dst)
+        out[dst] = g
+
+    tj, tk = h - 2 * halo, w // nc - 2 * hk
+    if (tj0 >= halo and tj0 + tj + halo <= n1 and tk0 >= hk and tk0 + tk + hk <= n2
+            and pitch % ub == 0 and fb % ub == 0):
+        # box inside the field: full units from a row pointer advancing by RP rows
+        for tid in range(nt):
+            c0, rs = tid % tc, tid // tc
+            if rs >= rp:
+                continue
+            g = fb + (tj0 - halo + rs) * pitch + (tk0 - hk) * nc * es + c0 * ub
+            for k in range(nk):
+                r = rs + k * rp
+                if r < h:
+                    for cc in range(ncc):
+                        if c0 + cc * tc < u:
+                            ga = g + cc * tc * ub
+                            assert ga % ub == 0 and fb <= ga and ga + ub <= fb + nbytes
+                            for e in range(v):
+                                put(r * w + (c0 + cc * tc) * v + e, (ga - fb) // es + e)
+                g += rp * pitch
+        return out
+
+    for tid in range(nt):
+        c0, rs = tid % tc, tid // tc
+        plan = []
+        lsu2 = pitch % ub != 0 or fb % ub != 0
+        for cc in range(ncc):
+            un = c0 + cc * tc
+            els = [elem(un * v + e) for e in range(v)]
+            csz = ub if all(ok for ok, _ in els) else 0
+            contig = all(els[e][1] == els[0][1] + e * es for e in range(v))
+            bad = un < u and any(ok for ok, _ in els) and not (csz and contig and els[0][1] % ub == 0)
+            lsu2 = lsu2 or bad
+            plan.append((un, els, csz, bad))
+        if rs >= rp:
+            continue
+        for k in range(nk):
+            r = rs + k * rp
+            if r >= h:
+                continue
+            jg = remap(tj0 - halo + r, n1, rj)
+            rok = 0 <= jg < n1
+            rowb = fb + (jg * pitch if rok else 0)
+            for un, els, csz, bad in plan:
+                if un >= u:
+                    continue
+                dst0 = r * w + un * v
+                gp = rowb + els[0][1]
+                if v == 1:
+                    n = csz if rok else 0
+                    assert gp % es == 0 and fb <= gp < fb + nbytes
+                    put(dst0, (gp - fb) // es if n else None)
+                    continue
+                if not rok or (not bad and csz == 0):
+                    for e in range(v):
+                        put(dst0 + e, None)
+                elif not bad and gp % ub == 0:
+                    assert fb <= gp and gp + ub <= fb + nbytes
+                    for e in range(v):
+                        put(dst0 + e, (gp - fb) // es + e)
+                else:
+                    assert lsu2          # the element-wise loop runs for this thread
+                    for e in range(v):
+                        ok, off = els[e]
+                        if ok:
+                            assert fb <= rowb + off < fb + nbytes
+                        put(dst0 + e, (rowb + off - fb) // es if ok else None)
+    return out
+
+
+@pytest.mark.parametrize("es,nc", [(4, 1), (4, 3), (2, 1), (2, 3), (8, 1)])
+@pytest.mark.parametrize("rule", [None, "periodic", "replicate", "reflect"])
+def test_cooperative_staging_covers_every_box_element_once(es, nc, rule):
+    """Every element of a staged box is written exactly once — with the element its
+    axis rules map it to, or zero outside the grid — every global read is inside the
+    field and every asynchronous copy aligned, for interior, face and corner tiles of
+    ragged grids, with 16-byte-aligned and merely element-aligned field bases."""
+    from stenpy_b200.codegen import PassConfig, PassSpec, FieldSpec, PGraph, lsu_vec
+
+    def rm(x_, n_):
+        if rule == "periodic":
+            return x_ + n_ if x_ < 0 else (x_ - n_ if x_ >= n_ else x_)
+        if rule == "replicate":
+            return min(max(x_, 0), n_ - 1)
+        if rule == "reflect" and n_ > 1:
+            y = -x_ if x_ < 0 else x_
+            y = 2 * (n_ - 1) - y if y > n_ - 1 else y
+            return min(max(y, 0), n_ - 1)
+        return x_
+
+    dt = {4: "f32", 2: "bf16", 8: "f64"}[es]
+    for tk, tj, nt in ((64, 8, 128), (32, 16, 128), (64, 16, 256)):
+        cfg = PassConfig(tj=tj, tk=tk, threads=nt)
+        for n1, n2 in ((37, 45), (9, 33), (40, 130), (5, 7), (12, 34), (11, 510), (6, 22)):
+            f = FieldSpec(0, dt, nc, staged=True, halo=2, vec=lsu_vec(n2 * nc * es, es))
+            spec = PassSpec(PGraph(), [f], [], 1, 1, 2, cfg)
+            hk = spec.hk(f)
+            w, h = spec.box(f)
+            for tj0 in range(0, n1, tj):
+                for tk0 in range(0, n2, tk):
+                    for fb in (0, es):
+                        got = _emulate_staging(w, h, es, nc, f.halo, hk, tk0, tj0, n1, n2, rule, rule, nt,
+                                               f.vec, fb)
+                        assert len(got) == w * h
+                        for dst, g in got.items():
+                            r, x = divmod(dst, w)
+                            xr = x - hk * nc
+                            kg, c = tk0 + xr // nc, xr % nc
+                            jg, kg = rm(tj0 - f.halo + r, n1), rm(kg, n2)
+                            want = (jg * n2 + kg) * nc + c if (0 <= jg < n1 and 0 <= kg < n2) else None
+                            assert g == want, (dst, g, want, tj0, tk0, n1, n2, fb)

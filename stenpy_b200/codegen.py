@@ -966,14 +966,22 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
                 elif r.red == "minmax":
                     K.append(f"{{ const double t_ = {val}; rv{ri_here}_a = fmin(rv{ri_here}_a, t_); rv{ri_here}_b = fmax(rv{ri_here}_b, t_); }}")
                 elif r.red == "hist":
-                    # bin index as the oracle forms it: floor((x - lo) / (hi - lo) * bins), FP64
-                    # (the product with a precomputed bins/(hi-lo) rounds differently from the
-                    # quotient only within a few ulps; near a bin edge the quotient is formed)
-                    K.append(f"if (rv{ri_here}_hh > rv{ri_here}_hl) {{ const double d_ = {val} - rv{ri_here}_hl;"
-                             f" double t_ = d_ * rv{ri_here}_hinv;"
-                             f" if (fabs(t_ - rint(t_)) <= 1e-9) t_ = d_ / (rv{ri_here}_hh - rv{ri_here}_hl) * {float(r.bins)!r};"
-                             f" int b_ = (int)floor(t_);"
-                             f" b_ = b_ < 0 ? 0 : (b_ > {r.bins - 1} ? {r.bins - 1} : b_); sten_hist_add(rv{ri_here}_hs, b_); }}")
+                    # bin index as the oracle forms it: floor((x - lo) / (hi - lo) * bins) in
+                    # FP64. FP32 first when its error bound (rv_f32) keeps it within 2.5e-4 of
+                    # the exact t and t is more than 1e-3 from an integer (then both floors
+                    # agree); else the FP64 product, and within 1e-9 of an edge the FP64
+                    # quotient. Counts are run-length merged per thread (smooth data puts
+                    # consecutive voxels in one bin) before the shared-memory atomic.
+                    h = f"rv{ri_here}"
+                    K.append(f"if ({h}_hh > {h}_hl) {{ int b_;"
+                             f" const float t32_ = (rv[{off + c}] - {h}_hl32) * {h}_hi32;"
+                             f" if ({h}_f32 && fabsf(t32_ - rintf(t32_)) > 1e-3f) b_ = (int)floorf(t32_);"
+                             f" else {{ const double d_ = {val} - {h}_hl; double t_ = d_ * {h}_hinv;"
+                             f" if (fabs(t_ - rint(t_)) <= 1e-9) t_ = d_ / ({h}_hh - {h}_hl) * {float(r.bins)!r};"
+                             f" b_ = (int)floor(t_); }}"
+                             f" b_ = b_ < 0 ? 0 : (b_ > {r.bins - 1} ? {r.bins - 1} : b_);"
+                             f" if (b_ == {h}_hb) ++{h}_hn;"
+                             f" else {{ if ({h}_hn) atomicAdd({h}_hs + {h}_hb, ({h}_cnt_t){h}_hn); {h}_hb = b_; {h}_hn = 1u; }} }}")
                 elif r.red == "integrate":
                     sm = 1 if r.method == "simpson" else 0
                     if where == "main" and not is_flat(spec):
@@ -1012,10 +1020,18 @@ def _red_decls(spec: PassSpec, where: str = "main") -> List[str]:
             K.append(f"const double rv{ri}_hl = __ldcg(p.scal + {r.lohi_index}), "
                      f"rv{ri}_hh = __ldcg(p.scal + {r.lohi_index + 1});")
             K.append(f"const double rv{ri}_hinv = rv{ri}_hh > rv{ri}_hl ? {float(r.bins)!r} / (rv{ri}_hh - rv{ri}_hl) : 0.0;")
+            # FP32 binning is exact-floor-safe when bins·(4·max|lo,hi|/(hi-lo) + 2)·2^-23,
+            # twice its worst-case error of t, is at most 2.5e-4
+            K.append(f"const float rv{ri}_hl32 = (float)rv{ri}_hl, rv{ri}_hi32 = (float)rv{ri}_hinv;")
+            K.append(f"const bool rv{ri}_f32 = rv{ri}_hh > rv{ri}_hl && {float(r.bins)!r} * (4.0 * fmax(fabs(rv{ri}_hl), "
+                     f"fabs(rv{ri}_hh)) / (rv{ri}_hh - rv{ri}_hl) + 2.0) * 1.1920928955078125e-07 <= 2.5e-4;")
+            K.append(f"int rv{ri}_hb = 0; unsigned int rv{ri}_hn = 0u;")
             if where == "main":
+                K.append(f"typedef unsigned int rv{ri}_cnt_t;")
                 K.append(f"unsigned int* rv{ri}_hs = (unsigned int*)(smem + {hoffs[ri]});")
                 K.append(f"for (int b_ = tid; b_ < {r.bins}; b_ += NT) rv{ri}_hs[b_] = 0u;")
             else:
+                K.append(f"typedef unsigned long long rv{ri}_cnt_t;")
                 K.append(f"unsigned long long* rv{ri}_hs = p.hist + {r.slot};")
         elif r.red == "var":
             K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
@@ -1048,6 +1064,7 @@ def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
     for ri, r in enumerate(reds):
         base = f"p.part[(size_t)({cta}) * NSLOTS_RED + {r.slot}"
         if r.red == "hist":
+            K.append(f"if (rv{ri}_hn) atomicAdd(rv{ri}_hs + rv{ri}_hb, (rv{ri}_cnt_t)rv{ri}_hn);")
             if where == "main":
                 K.append("__syncthreads();")
                 K.append(f"for (int b_ = tid; b_ < {r.bins}; b_ += NT) {{ const unsigned int c_ = rv{ri}_hs[b_];"

@@ -339,16 +339,6 @@ STEN_DEV void block_chan(double& n, double& mean, double& m2, double* scratch) {
 }
 
 // ------------------------------------------------------------------ histograms
-// Lanes of a warp that hit the same bin add once, with their count (smooth data puts
-// neighbouring voxels in the same bin: one atomic per distinct bin per warp).
-STEN_DEV void sten_hist_add(unsigned int* h, int b) {
-  const unsigned peers = __match_any_sync(__activemask(), b);
-  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(h + b, (unsigned)__popc(peers));
-}
-STEN_DEV void sten_hist_add(unsigned long long* h, int b) {
-  const unsigned peers = __match_any_sync(__activemask(), b);
-  if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(h + b, (unsigned long long)__popc(peers));
-}
 // sum over non-empty bins of q log q, q = count / n (the entropy is its negation),
 // clearing the counts for the next run. Fixed bins per thread and a fixed
 // reduction tree: deterministic. Whole block; the result is valid in thread 0.

@@ -156,6 +156,21 @@ def all_sources():
                            ("variance(tanh(f))", "periodic")):
                 g, sink, *_ = S.compile_expression(e, boundary=bnd, field_map={"f": _ph(shape, dt)})
                 src += plan_sources(g, [sink])
+    for dt in (torch.float32, torch.bfloat16):   # entropy bins at edges / with offsets, and their batch
+        ejobs = []
+        for expr in ("entropy_hist(f)", "entropy_hist(f, bins=64)", "entropy_hist(f*f)"):
+            g, sink, *_ = S.compile_expression(expr, boundary="periodic", field_map={"f": _ph((17, 24, 40), dt)})
+            src += plan_sources(g, [sink])
+            ejobs.append(B.BatchJob(g, [sink]))
+        cfg = B.batch_candidates(128)[0]
+        ps, seen = [], set()
+        for j in ejobs * 3:
+            for pp in B.plan_job(j, cfg).passes:
+                k = B.program_key(pp.spec)
+                if k not in seen:
+                    seen.add(k)
+                    ps.append(pp.spec)
+        src.append(emit_batch_module(ps, 128, B.batch_min_blocks(128)))
     # batched executor: per-job runtime plans and the batch modules of the tests
     import test_gpu_batch as TB
     smooth = [(e, torch.float32, [(33, 21, 45), (40, 24, 80)][i % 2], 0) for i, e in

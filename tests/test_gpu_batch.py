@@ -157,3 +157,33 @@ def test_entropy_hist_runtime_against_oracle(dtype):
     c = torch.full((8, 9, 16), 2.5, device=dev, dtype=dtype)
     gc, sc, *_ = S.compile_expression("entropy_hist(f)", field_map={"f": c})
     assert float(S.Runtime(device=dev).run(gc)[sc]) == 0.0
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_entropy_hist_bins_at_edges_and_with_offsets(dtype):
+    """Binning must equal the oracle's FP64 floor exactly: values on bin edges
+    (i/256 patterns, where the FP32 shortcut must defer to FP64), values with a large
+    offset relative to their range (the shortcut is disabled), and both in one batch."""
+    import stenpy_b200 as S
+    from stenpy_b200 import batch as B
+    from stenpy_b200.synth import sinusoid_field
+    dev = _dev()
+    shape = (17, 24, 40)
+    i = torch.arange(shape[0] * shape[1] * shape[2], dtype=torch.float64).reshape(shape)
+    fields = {"edges": ((i % 257) / 256.0).to(dtype),
+              "offset": (sinusoid_field(shape, seed=8).double() * 0.01 + 1000.0).to(dtype),
+              "smooth": sinusoid_field(shape, seed=9).to(dtype)}
+    jobs, host = [], []
+    for name, f in fields.items():
+        for expr in ("entropy_hist(f)", "entropy_hist(f, bins=64)", "entropy_hist(f*f)"):
+            g, sink, *_ = S.compile_expression(expr, boundary="periodic", field_map={"f": f.to(dev)})
+            got = float(S.Runtime(device=dev).run(g)[sink])
+            # the kernel bins the FP32 product: the oracle bins the same rounded values
+            fo = (f.double() * f.double()).float().double() if "f*f" in expr else f.double()
+            g2, s2, *_ = S.compile_expression(expr.replace("f*f", "f"), boundary="periodic", field_map={"f": fo})
+            ref = float(O.evaluate(g2, [s2])[s2])
+            assert abs(got - ref) <= 1e-10 * max(1.0, abs(ref)), (name, expr, got, ref)
+            jobs.append(B.BatchJob(g, [sink]))
+            host.append((name, expr, sink, ref))
+    for (name, expr, sink, ref), res in zip(host, B.run_batch(jobs, dev)):
+        assert abs(float(res[sink]) - ref) <= 1e-10 * max(1.0, abs(ref)), (name, expr, float(res[sink]), ref)

@@ -261,6 +261,43 @@ def conv3d_spectral(a, boundary: str = "periodic"):
     return out / 64.0
 
 
+# ---------------------------------------------------------------- spectral
+def _k(shape, dx):
+    """Angular wavenumbers 2π·fftfreq(n, dx) per axis (stenpy_engine.py:2934-2948): the
+    frequencies are formed in FP32 (torch's default dtype) and widened, as there."""
+    ks = []
+    for d, (n, h) in enumerate(zip(shape, dx)):
+        sh = [1] * len(shape)
+        sh[d] = -1
+        ks.append((torch.fft.fftfreq(n, d=h, dtype=torch.float32).to(F64) * (2 * math.pi)).view(sh))
+    return ks
+
+
+def fft(t, norm="backward"):
+    """fftn of the field as complex128 (stenpy_engine.py:2875-2885), as a graph node sees
+    it: the reference's runtime passes ``alloc`` and the op copies its result into that
+    real FP64 buffer (stenpy_engine.py:2881-2884), keeping the real part."""
+    return torch.fft.fftn(t if t.is_complex() else t.to(torch.complex128), norm=norm).real
+
+
+def ifft(t, norm="backward"):
+    """Real part of ifftn (stenpy_engine.py:2887-2896)."""
+    x = t if t.is_complex() else torch.complex(t, torch.zeros_like(t))
+    return torch.fft.ifftn(x, norm=norm).real
+
+
+def spectral_gradient(t, dx=1.0, dim=0, norm="backward"):
+    """Re ifftn(i·k_dim·fftn(t)) (stenpy_engine.py:2980-2993)."""
+    k = _k(t.shape, _dx_tuple(dx, t.ndim))
+    return torch.fft.ifftn(1j * k[int(dim)] * torch.fft.fftn(t, norm=norm), norm=norm).real
+
+
+def spectral_laplacian(t, dx=1.0, norm="backward"):
+    """Re ifftn(−|k|²·fftn(t)) (stenpy_engine.py:2998-3010)."""
+    k = _k(t.shape, _dx_tuple(dx, t.ndim))
+    return torch.fft.ifftn(-sum(kk * kk for kk in k) * torch.fft.fftn(t, norm=norm), norm=norm).real
+
+
 def grad_mag(t, dx=1.0, boundary="neumann"):
     """|gradient(t)| with gradient's boundary conventions (not in the reference)."""
     return torch.linalg.norm(gradient(t, dx, boundary), dim=-1)
@@ -390,7 +427,8 @@ OPS: Dict[str, Callable] = {
     "hessian": hessian, "jacobian": jacobian, "mean_curvature": mean_curvature,
     "grad_mag": grad_mag, "gradient_nd": gradient_nd, "material_derivative": material_derivative,
     "moving_average": moving_average, "conv3d_spectral": conv3d_spectral,
-    "surface_normals": surface_normals,
+    "surface_normals": surface_normals, "fft": fft, "ifft": ifft,
+    "spectral_gradient": spectral_gradient, "spectral_laplacian": spectral_laplacian,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

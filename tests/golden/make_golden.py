@@ -136,6 +136,11 @@ CASES = [
     ("surfnorm_small", "surface_normals(f*g)", "fg", "neumann", 1.0, (3, 5)),
     ("field2d_reduce", "sum(f*f) + mean(g)", "fg", "periodic", 1.0, (9, 13)),
     ("field2d_pointwise", "tanh(f)*exp(g) + f**2", "fg", "periodic", 1.0, (9, 13)),
+    ("spec_lap", "spectral_laplacian(f)", "f", "periodic", 1.0, S_EVEN),
+    ("spec_grad", "spectral_gradient(f, dim=1)", "f", "periodic", 1.0, S_MIX),
+    ("spec_grad_dx", "spectral_gradient(f, dim=2, dx=0.5)", "f", "periodic", 1.0, S_ODD),
+    ("fft_roundtrip", "ifft(fft(f*g))", "fg", "periodic", 1.0, S_MIX),
+    ("spec_vs_fd", "spectral_laplacian(f) - laplacian(f) + sum(spectral_laplacian(g))", "fg", "periodic", 1.0, S_EVEN),
 ]
 
 # The reference's expression path hands conv3d_spectral a ``dx`` it does not accept

@@ -492,3 +492,17 @@ def test_cooperative_staging_covers_every_box_element_once(es, nc, rule):
                             jg, kg = rm(tj0 - f.halo + r, n1), rm(kg, n2)
                             want = (jg * n2 + kg) * nc + c if (0 <= jg < n1 and 0 <= kg < n2) else None
                             assert g == want, (dst, g, want, tj0, tk0, n1, n2, fb)
+
+def test_spectral_operators_are_registered_and_gpu_only():
+    """FFT operators run outside the fused passes (opaque graph nodes) and, like every
+    operator here, refuse host tensors."""
+    from stenpy_b200.registry import KNOWN_OPS
+    for name in ("fft", "ifft", "fft_complex", "ifft_complex", "spectral_gradient", "spectral_laplacian"):
+        assert name in S.OP_REGISTRY and name not in KNOWN_OPS
+        assert S.OP_METADATA[name]["cost"] == "high"
+        with pytest.raises(ValueError, match="CUDA"):
+            S.OP_REGISTRY[name](torch.zeros(4, 5, 6))
+    g, sink, *_ = S.compile_expression("spectral_gradient(f, dim=2, dx=0.5) + laplacian(f)",
+                                       field_map={"f": torch.zeros(4, 5, 6)})
+    ops = {n.op_name: n.params for n in g.topological_sort()}
+    assert ops["spectral_gradient"] == {"dim": 2, "dx": 0.5}

@@ -261,6 +261,19 @@ def conv3d_spectral(a, boundary: str = "periodic"):
     return out / 64.0
 
 
+# ---------------------------------------------------------------- geometry
+def distance_transform(t, dx=1.0, method="auto"):
+    """The reference's CPU path (stenpy_engine.py:3146-3152): SciPy's
+    ``ndimage.distance_transform_edt`` (SciPy 1.18.1 here; no version is pinned by the
+    reference) of ``t == 0`` with ``sampling`` = dx — for each voxel with t == 0 the
+    Euclidean distance to the nearest voxel with t != 0, else 0."""
+    import numpy as np
+    from scipy.ndimage import distance_transform_edt
+    dxs = _dx_tuple(dx, t.ndim)
+    out = distance_transform_edt((t == 0).numpy(), sampling=list(dxs))
+    return torch.from_numpy(np.asarray(out, dtype=np.float64))
+
+
 # ---------------------------------------------------------------- spectral
 def _k(shape, dx):
     """Angular wavenumbers 2π·fftfreq(n, dx) per axis (stenpy_engine.py:2934-2948): the
@@ -429,6 +442,7 @@ OPS: Dict[str, Callable] = {
     "moving_average": moving_average, "conv3d_spectral": conv3d_spectral,
     "surface_normals": surface_normals, "fft": fft, "ifft": ifft,
     "spectral_gradient": spectral_gradient, "spectral_laplacian": spectral_laplacian,
+    "distance_transform": distance_transform,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

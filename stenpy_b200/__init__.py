@@ -22,6 +22,7 @@ from __future__ import annotations
 from .graph import Graph, GraphNode, _uid
 from .registry import OP_METADATA, OP_REGISTRY, register_operator
 from . import spectral  # noqa: F401  (registers the FFT operators, run outside the fused passes)
+from . import geometry  # noqa: F401  (registers distance_transform)
 from .frontend import compile_expression, compile_expressions, parse_expression
 from .memory_manager import MemoryManager
 from .runtime import Runtime, run_single_op

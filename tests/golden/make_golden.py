@@ -141,6 +141,9 @@ CASES = [
     ("spec_grad_dx", "spectral_gradient(f, dim=2, dx=0.5)", "f", "periodic", 1.0, S_ODD),
     ("fft_roundtrip", "ifft(fft(f*g))", "fg", "periodic", 1.0, S_MIX),
     ("spec_vs_fd", "spectral_laplacian(f) - laplacian(f) + sum(spectral_laplacian(g))", "fg", "periodic", 1.0, S_EVEN),
+    ("edt_clamp", "distance_transform(clamp(f))", "f", "periodic", 1.0, S_MIX),
+    ("edt_even", "distance_transform(clamp(f*g))", "fg", "periodic", 1.0, S_EVEN),
+    ("edt_plus", "distance_transform(clamp(f - 1)) + f", "f", "neumann", 1.0, S_ODD),
 ]
 
 # The reference's expression path hands conv3d_spectral a ``dx`` it does not accept

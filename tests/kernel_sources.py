@@ -173,6 +173,10 @@ def all_sources():
                     seen.add(k)
                     ps.append(pp.spec)
         src.append(emit_batch_module(ps, 128, B.batch_min_blocks(128)))
+    from stenpy_b200.geometry import edt_source   # distance transform (per dtype and longest line)
+    for dt in (torch.float32, torch.float64, torch.bfloat16, torch.float16):
+        src += [edt_source(dt, nmax) for nmax in (16, 32, 64)]
+    src.append(edt_source(torch.float32, 256))
     # batched executor: per-job runtime plans and the batch modules of the tests
     import test_gpu_batch as TB
     smooth = [(e, torch.float32, [(33, 21, 45), (40, 24, 80)][i % 2], 0) for i, e in

@@ -41,6 +41,8 @@ SMEM_LIMIT = 227 * 1024
 _SHAPES = [(32, 128, 4), (32, 128, 8), (64, 128, 2), (64, 128, 4), (64, 256, 4), (64, 256, 8)]
 _SEGS = (32, 128)
 _SHAPES_KV4 = [(64, 128, 4), (64, 128, 2), (64, 256, 2)]   # (TK, threads, rows per thread) with KV = 4
+# KV = 8 (16-byte chunks) is a valid schedule but not a candidate: on B200 at 512^3 the
+# 16-bit passes of the config-1 step ran 3-14 % slower with it than with KV = 4
 _GHOST = (True, False)
 
 
@@ -80,13 +82,14 @@ def candidates(spec: PassSpec) -> List[PassConfig]:
     # 16-bit passes also try four k-adjacent voxels per thread (8-byte chunks, paired
     # 16-bit stores), keeping the rows per thread: measured faster for 16-bit stencils
     if not is_flat(spec) and not spec.has_scan and spec.fields and all(ESIZE[f.dtype] == 2 for f in spec.fields):
-        for tk, nt, vpt in _SHAPES_KV4:
-            for seg in _SEGS:
-                for gh in (_GHOST if uses_ghost else (True,)):
-                    cfg = PassConfig(tj=(nt * 4 // tk) * vpt, tk=tk, threads=nt, prefetch=2, seg_len=seg,
-                                     ghost=gh, kv=4)
-                    if valid_shape(cfg) and _valid(spec, cfg):
-                        out.append(cfg)
+        for kv, shapes in ((4, _SHAPES_KV4),):
+            for tk, nt, vpt in shapes:
+                for seg in _SEGS:
+                    for gh in (_GHOST if uses_ghost else (True,)):
+                        cfg = PassConfig(tj=(nt * kv // tk) * vpt, tk=tk, threads=nt, prefetch=2, seg_len=seg,
+                                         ghost=gh, kv=kv)
+                        if valid_shape(cfg) and _valid(spec, cfg):
+                            out.append(cfg)
     # keep distinct schedules only (scan passes collapse the segment axis)
     seen, uniq = set(), []
     for c in out:

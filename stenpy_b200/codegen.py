@@ -247,7 +247,7 @@ def analyse_ghosts(spec: "PassSpec") -> None:
 def valid_shape(cfg: "PassConfig") -> bool:
     """Thread mapping: TK/KV threads along k (each KV adjacent voxels), the block's
     other threads along j, VPT = TJ / (threads / (TK/KV)) rows each."""
-    if cfg.kv not in (1, 2, 4) or cfg.tk % 32 or cfg.tk % cfg.kv or cfg.prefetch < 1:
+    if cfg.kv not in (1, 2, 4, 8) or cfg.tk % 32 or cfg.tk % cfg.kv or cfg.prefetch < 1:
         return False
     tkt = cfg.tk // cfg.kv
     if cfg.threads % tkt:

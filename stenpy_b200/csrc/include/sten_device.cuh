@@ -133,11 +133,16 @@ STEN_DEV u32 pack2(const bf16_t*, float lo, float hi) {
 template <int KV> STEN_DEV void st_vec(float* p, const float* v) {
   if constexpr (KV == 2) *(float2*)p = make_float2(v[0], v[1]);
   else if constexpr (KV == 4) *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
-  else { for (int q = 0; q < KV; ++q) p[q] = v[q]; }
+  else if constexpr (KV == 8) {
+    *(float4*)p = make_float4(v[0], v[1], v[2], v[3]);
+    *(float4*)(p + 4) = make_float4(v[4], v[5], v[6], v[7]);
+  } else { for (int q = 0; q < KV; ++q) p[q] = v[q]; }
 }
 template <int KV, typename T> STEN_DEV void st_vec(T* p, const float* v) {
   if constexpr (KV == 2) *(u32*)p = pack2(p, v[0], v[1]);
   else if constexpr (KV == 4) *(uint2*)p = make_uint2(pack2(p, v[0], v[1]), pack2(p, v[2], v[3]));
+  else if constexpr (KV == 8)
+    *(uint4*)p = make_uint4(pack2(p, v[0], v[1]), pack2(p, v[2], v[3]), pack2(p, v[4], v[5]), pack2(p, v[6], v[7]));
   else { for (int q = 0; q < KV; ++q) st_from_f32(p + q, v[q]); }
 }
 

@@ -91,7 +91,7 @@ def all_sources():
     for dt in (torch.float32, torch.float16, torch.bfloat16):   # KV chunk parity
         for bnd in ("periodic", "neumann"):
             for shape in [(20, 33, 130), (9, 16, 64), (7, 5, 45)]:
-                for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8)):
+                for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8), (8, 64, 16), (8, 128, 8)):
                     g, sink, *_ = S.compile_expression(expr, boundary=bnd, field_map={
                         "f": _ph(shape, dt), "u": _ph(shape + (3,), dt)})
                     w = [sink, g.add("variance", (sink,), {})]

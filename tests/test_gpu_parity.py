@@ -102,7 +102,7 @@ def test_kv_chunks_match_one_voxel_per_thread(dtype, boundary):
         u = smoothed_vector(shape, seed=5).to(dtype).to(dev)
         expr = "divergence(gradient(f)) + l2norm(curl(u)) + laplacian(f)*tanh(f)"
         outs = {}
-        for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8)):
+        for kv, tk, tj in ((1, 64, 8), (2, 64, 16), (4, 64, 32), (2, 32, 8), (8, 64, 16), (8, 128, 8)):
             cfg = PassConfig(tj=tj, tk=tk, threads=128, seg_len=8, kv=kv)
             g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map={"f": f, "u": u})
             w = [sink, g.add("variance", (sink,), {})]

@@ -173,7 +173,7 @@ def curl(t, dx=1.0, boundary="neumann"):
     raise ValueError("curl: only 2-D or 3-D vector fields")
 
 
-def gradient_nd(t, dx=1.0, boundary="neumann"):
+def gradient_nd(t, dx=1.0, boundary="neumann", dim=None):
     """torch.gradient over all axes, edge order 2 when every axis has ≥3 points,
     boundary ignored (stenpy_engine.py:2037-2083)."""
     order = 2 if min(t.shape) >= 3 else 1
@@ -259,6 +259,67 @@ def conv3d_spectral(a, boundary: str = "periodic"):
             for dk in (-1, 0, 1):
                 out = out + (w1[di] * w1[dj] * w1[dk]) * torch.roll(a, (-di, -dj, -dk), (0, 1, 2))
     return out / 64.0
+
+
+# ---------------------------------------------------------------- tensor and vector helpers
+def determinant(t):
+    """det of each (3, 3), the diagonal lifted by 1e-12 everywhere when any |diagonal|
+    entry of the field is below 1e-12; NaN → 0, ±inf and beyond → ±1e30
+    (stenpy_engine.py:2683-2710)."""
+    eye = torch.eye(t.shape[-1], dtype=F64)
+    diag = torch.diagonal(t, dim1=-2, dim2=-1)
+    tr = t + 1e-12 * eye if bool((diag.abs() < 1e-12).any()) else t
+    det = torch.linalg.det(tr)
+    return torch.nan_to_num(det, nan=0.0, posinf=1e30, neginf=-1e30).clamp(-1e30, 1e30)
+
+
+def inverse(t):
+    """torch.linalg.inv of each matrix (stenpy_engine.py:2724-2728)."""
+    return torch.linalg.inv(t)
+
+
+def deviatoric(t):
+    """t − tr(t)/D · I with NaN and ±inf → 0 (stenpy_engine.py:2852-2867)."""
+    d = t.shape[-1]
+    tr = torch.diagonal(t, dim1=-2, dim2=-1).sum(-1, keepdim=True).unsqueeze(-1)
+    out = t - (tr / max(d, 1e-15)) * torch.eye(d, dtype=F64)
+    return torch.nan_to_num(out, nan=0.0, posinf=0.0, neginf=0.0)
+
+
+def stack_components(*ts, dim=-1):
+    """torch.stack of the fields (stenpy_engine.py:2247-2250)."""
+    return torch.stack(list(ts), dim=dim)
+
+
+def norm_last(t, eps: float = 1e-15):
+    """‖t‖ over the last axis, kept as an axis of 1, at least eps (stenpy_engine.py:2262-2264)."""
+    return torch.linalg.norm(t, dim=-1, keepdim=True).clamp(min=eps)
+
+
+def div_last(a, b):
+    """a / b, b given a trailing axis when it has one fewer (stenpy_engine.py:2269-2274)."""
+    return a / (b.unsqueeze(-1) if b.ndim == a.ndim - 1 else b)
+
+
+def neg_stack3(gx, gy):
+    """(−gx, −gy, 1) / max(‖·‖, 1e-15) (stenpy_engine.py:2279-2288)."""
+    n = torch.stack([-gx, -gy, torch.ones_like(gx)], dim=-1)
+    return n / torch.linalg.norm(n, dim=-1, keepdim=True).clamp(min=1e-15)
+
+
+def scale_eye(scalar_field, D):
+    """s · I_D per voxel (stenpy_engine.py:2293-2300)."""
+    return scalar_field.unsqueeze(-1).unsqueeze(-1) * torch.eye(int(D), dtype=F64)
+
+
+def velocity_dot_grad(v, g):
+    """v · g elementwise (stenpy_engine.py:2305-2311)."""
+    return v * g
+
+
+def surface_integral(t, normals, area_weights):
+    """Σ (t · normals) · area_weights (stenpy_engine.py:2486-2494)."""
+    return ((t * normals).sum(dim=-1) * area_weights).sum()
 
 
 # ---------------------------------------------------------------- geometry
@@ -442,7 +503,10 @@ OPS: Dict[str, Callable] = {
     "moving_average": moving_average, "conv3d_spectral": conv3d_spectral,
     "surface_normals": surface_normals, "fft": fft, "ifft": ifft,
     "spectral_gradient": spectral_gradient, "spectral_laplacian": spectral_laplacian,
-    "distance_transform": distance_transform,
+    "distance_transform": distance_transform, "determinant": determinant, "inverse": inverse,
+    "deviatoric": deviatoric, "stack_components": stack_components, "norm_last": norm_last,
+    "div_last": div_last, "neg_stack3": neg_stack3, "scale_eye": scale_eye,
+    "velocity_dot_grad": velocity_dot_grad, "surface_integral": surface_integral,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

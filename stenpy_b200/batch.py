@@ -281,7 +281,7 @@ class BatchProgram:
                     fptrs.append(t.data_ptr())
                 outs = []
                 for (nid, okind, nc), r in zip(pp.out_nodes, [r for r in spec.roots if r.kind == "out"]):
-                    shape = plan.out_shape(nc)
+                    shape = plan.out_shape(nc, nid)
                     o = job.outputs.get(nid)
                     if o is None or tuple(o.shape) != shape or o.dtype != FC.DT_TORCH[r.out_dtype]:
                         o = torch.empty(shape, dtype=FC.DT_TORCH[r.out_dtype], device=dev)

@@ -402,7 +402,38 @@ class _Emitter:
             out.append(f"{o}[2] = 1.0f / {m};")
         elif op == "norm":
             a = ins[0]
-            out.append(f"{o}[0] = sqrtf({' + '.join(f'{a}[{c}]*{a}[{c}]' for c in range(self.g.nodes[n.ins[0]].nc))});")
+            nrm = f"sqrtf({' + '.join(f'{a}[{c}]*{a}[{c}]' for c in range(self.g.nodes[n.ins[0]].nc))})"
+            eps = n.a("eps")
+            out.append(f"{o}[0] = {nrm};" if eps is None else f"{o}[0] = fmaxf({nrm}, {_lit(eps)});")
+        elif op == "det3":
+            a = ins[0]
+            d = self.t()
+            out.append(f"float {d} = {a}[0] * ({a}[4] * {a}[8] - {a}[5] * {a}[7]) - {a}[1] * ({a}[3] * {a}[8] - {a}[5] * {a}[6])"
+                       f" + {a}[2] * ({a}[3] * {a}[7] - {a}[4] * {a}[6]);")
+            # nan -> 0, then clamped to +-1e30 (infinities included)
+            out.append(f"{o}[0] = ({d} != {d}) ? 0.0f : fminf(fmaxf({d}, -1e30f), 1e30f);")
+        elif op == "inv3":
+            a = ins[0]
+            c = [f"({a}[4] * {a}[8] - {a}[5] * {a}[7])", f"({a}[5] * {a}[6] - {a}[3] * {a}[8])",
+                 f"({a}[3] * {a}[7] - {a}[4] * {a}[6])", f"({a}[2] * {a}[7] - {a}[1] * {a}[8])",
+                 f"({a}[0] * {a}[8] - {a}[2] * {a}[6])", f"({a}[1] * {a}[6] - {a}[0] * {a}[7])",
+                 f"({a}[1] * {a}[5] - {a}[2] * {a}[4])", f"({a}[2] * {a}[3] - {a}[0] * {a}[5])",
+                 f"({a}[0] * {a}[4] - {a}[1] * {a}[3])"]
+            cof = self.t()
+            out.append(f"float {cof}[9] = {{{', '.join(c)}}};")   # cofactor matrix, row-major
+            det = self.t()
+            out.append(f"const float {det} = {a}[0] * {cof}[0] + {a}[1] * {cof}[1] + {a}[2] * {cof}[2];")
+            for i in range(3):
+                for j in range(3):
+                    out.append(f"{o}[{3 * i + j}] = {cof}[{3 * j + i}] / {det};")
+        elif op == "dev3":
+            a = ins[0]
+            q = self.t()
+            out.append(f"const float {q} = ({a}[0] + {a}[4] + {a}[8]) / 3.0f;")
+            for i in range(3):
+                for j in range(3):
+                    v = f"{a}[{3 * i + j}] - {q} * {'1.0f' if i == j else '0.0f'}"
+                    out.append(f"{{ const float v_ = {v}; {o}[{3 * i + j}] = isfinite(v_) ? v_ : 0.0f; }}")
         else:
             raise NotImplementedError(f"codegen: pointwise op {op}")
 

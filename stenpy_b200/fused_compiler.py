@@ -141,10 +141,12 @@ class FusedPlan:
     scalar_module: Optional[int] = None
     hist_size: int = 0
     dims2: bool = False    # 2-D fields: the grid is (1, n0, n1), per-voxel results are (n0, n1, ...)
+    keepdim: Set[str] = dc_field(default_factory=set)   # results with a trailing axis of 1 (norm_last)
 
-    def out_shape(self, nc: int) -> Tuple[int, ...]:
-        """Shape of a per-voxel result with ``nc`` components."""
-        return (self.shape[1:] if self.dims2 else self.shape) + comp_shape(nc)
+    def out_shape(self, nc: int, nid: Optional[str] = None) -> Tuple[int, ...]:
+        """Shape of a per-voxel result with ``nc`` components (of node ``nid``)."""
+        return ((self.shape[1:] if self.dims2 else self.shape) + comp_shape(nc)
+                + ((1,) if nid in self.keepdim else ()))
 
     def kernel_sources(self) -> List[str]:
         return [emit_pass(p.spec) for p in self.passes]
@@ -199,7 +201,7 @@ class Planner:
             if spec.kind == "reduction":
                 if not ins or ins[0].kind in ("scalar", "red"):
                     raise FusionError(f"{op} needs a per-voxel input")
-                p = ins[0].avail
+                p = max(i.avail for i in ins)
                 if op == "entropy_hist":
                     # two phases: min/max of the value, then its histogram over [min, max]
                     self.hist_mm[nid] = p
@@ -264,7 +266,8 @@ class Planner:
         scalar_source = self._scalar_source(scalar_sinks) if scalar_sinks else None
         return FusedPlan(key, self.shape, infos, passes, self.table_size, self.const_index, self.red_index,
                          scalar_sinks, scalar_source, self.wanted, self.out_dtype, list(self.live),
-                         hist_size=self.hist_base, dims2=self.dims2)
+                         hist_size=self.hist_base, dims2=self.dims2,
+                         keepdim={n for n in self.wanted if self.nodes[n].op_name == "norm_last"})
 
     def _build_pass(self, roots: List[Tuple[str, str]]) -> PassPlan:
         pg = PGraph()
@@ -334,6 +337,22 @@ class Planner:
                 reductions.append(RedPlan(nid, nslots, self.red_index[nid] + 1, N.RED_MIN_MAX,
                                           float(n_vox * nc), 0, 0.0))
                 nslots += RED_SLOTS["minmax"]
+            elif node.op_name == "surface_integral":
+                # Σ over voxels of (t · normals) · area_weights (stenpy_engine.py:2486-2494)
+                if len(node.input_ids) != 3:
+                    raise FusionError("surface_integral: (t, normals, area_weights)")
+                t_, n_, w_ = (lower(i) for i in node.input_ids)
+                if pg.nodes[t_].nc != 3 or pg.nodes[n_].nc != 3 or pg.nodes[w_].nc != 1:
+                    raise FusionError("surface_integral: two (*, 3) fields and a scalar weight field")
+
+                def comp_(x, c):
+                    y = low.component(x, c)
+                    return y if y is not None else pg.add("select", (x,), 1, pg.nodes[x].radius, index=c)
+                dots = [low.binop("mul", comp_(t_, c), comp_(n_, c)) for c in range(3)]
+                pn = low.binop("mul", low.binop("add", low.binop("add", dots[0], dots[1]), dots[2]), w_)
+                rspecs.append(RootSpec("red", pn, red="sum", slot=nslots))
+                reductions.append(RedPlan(nid, nslots, self.red_index[nid], N.RED_SUM, float(n_vox), 0, 0.0))
+                nslots += RED_SLOTS["sum"]
             elif node.op_name == "entropy_hist":
                 extra = set(node.params) - {"bins", "alloc", "mm"}
                 if extra:
@@ -650,7 +669,7 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
         for (nid, okind, nc), r in zip(pp.out_nodes, [r for r in spec.roots if r.kind in ("out", "scan")]):
             o = outputs.get(nid) if (outputs and okind == "out") else None
             if o is None:
-                o = torch.empty(plan.out_shape(nc), dtype=DT_TORCH[r.out_dtype], device=device)
+                o = torch.empty(plan.out_shape(nc, nid), dtype=DT_TORCH[r.out_dtype], device=device)
             outs.append(o)
             produced[nid] = o
             if nid in plan.wanted:

@@ -174,7 +174,7 @@ class LazyPipeline:
             outs = []
             for nid, kind, nc in pp.out_nodes:
                 dt = FC.DT_TORCH[[r for r in spec.roots if r.kind in ("out", "scan")][len(outs)].out_dtype]
-                comp = FC.comp_shape(nc)
+                comp = FC.comp_shape(nc) + ((1,) if nid in plan.keepdim else ())
                 host = outputs.get(nid) if outputs else None
                 if host is None:
                     host = torch.empty((self.n0, self.n1, self.n2) + comp, dtype=dt, pin_memory=True)

@@ -213,6 +213,43 @@ class OpLowerer:
                 return self.pg.add("select", (ins[0],), 3, self.r(ins[0]), index=idx)
             raise LoweringError("select_component: index out of range")
 
+        if op in ("determinant", "inverse", "deviatoric"):
+            need(1); no_extra()
+            if self.nc(ins[0]) != 9:
+                raise LoweringError(f"{op}: needs a (*, 3, 3) input")
+            prim = {"determinant": "det3", "inverse": "inv3", "deviatoric": "dev3"}[op]
+            return self.pg.add(prim, (ins[0],), 1 if op == "determinant" else 9, self.r(ins[0]))
+        if op == "stack_components":
+            no_extra("dim")
+            if int(p.get("dim", -1)) not in (-1, 3) or len(ins) != 3 or any(self.nc(x) != 1 for x in ins):
+                raise LoweringError("stack_components: three scalar fields stacked along the last axis")
+            return self.stack(ins)
+        if op == "norm_last":
+            need(1); no_extra("eps")
+            if self.nc(ins[0]) != 3:
+                raise LoweringError("norm_last: (*, 3) vector fields")
+            return self.pg.add("norm", (ins[0],), 1, self.r(ins[0]), eps=float(p.get("eps", 1e-15)))
+        if op == "div_last":
+            need(2); no_extra()
+            if self.nc(ins[1]) not in (1, self.nc(ins[0])):
+                raise LoweringError("div_last: divisor must be scalar or match the components")
+            return self.binop("div", ins[0], ins[1], eps=0.0)
+        if op == "neg_stack3":
+            need(2); no_extra()
+            if self.nc(ins[0]) != 1 or self.nc(ins[1]) != 1:
+                raise LoweringError("neg_stack3: two scalar fields")
+            return self.pg.add("surfnorm", (ins[0], ins[1]), 3, self.r(*ins))
+        if op == "scale_eye":
+            need(1); no_extra("D")
+            if int(p.get("D", 3)) != 3 or self.nc(ins[0]) != 1:
+                raise LoweringError("scale_eye: a scalar field and D=3")
+            s = ins[0]
+            z = self.pg.add("mulk", (s,), 1, self.r(s), k=0.0)   # s·0, as the reference's s·I entries
+            return self.stack([s, z, z, z, s, z, z, z, s])
+        if op == "velocity_dot_grad":
+            need(2); no_extra()
+            return self.binop("mul", ins[0], ins[1])
+
         # ---- stencils
         bnd = str(p.get("boundary", "neumann"))
         if op == "laplacian":
@@ -260,6 +297,14 @@ class OpLowerer:
             return self.stack([self.binop("sub", d(2, 1), d(1, 2)),
                                self.binop("sub", d(0, 2), d(2, 0)),
                                self.binop("sub", d(1, 0), d(0, 1))])
+        if op == "gradient_nd":
+            need(1); no_extra("dx", "boundary", "dim")   # dim is accepted and ignored, as there
+            x = ins[0]
+            if self.nc(x) != 1:
+                raise LoweringError("gradient_nd: scalar fields only")
+            h = dx3(p.get("dx", 1.0))
+            mode = _gnd_mode(self.shape, op)
+            return self.stack([self.d1(x, a, mode, h[a]) for a in range(3)])
         if op in ("hessian", "jacobian", "mean_curvature"):
             no_extra("dx", "boundary", "eps")
             need(1)

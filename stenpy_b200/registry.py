@@ -73,12 +73,17 @@ KNOWN_OPS: Dict[str, OpSpec] = {
     # tensor epilogues (stenpy_engine.py:2674-2721, 2256-2259)
     "trace": OpSpec("pointwise"), "eigenvalues": OpSpec("pointwise"),
     "select_component": OpSpec("pointwise"),
+    # per-voxel tensor and vector helpers (stenpy_engine.py:2247-2313, 2683-2730, 2852-2869)
+    "determinant": OpSpec("pointwise"), "inverse": OpSpec("pointwise"), "deviatoric": OpSpec("pointwise"),
+    "stack_components": OpSpec("pointwise"), "norm_last": OpSpec("pointwise"), "div_last": OpSpec("pointwise"),
+    "neg_stack3": OpSpec("pointwise"), "scale_eye": OpSpec("pointwise"), "velocity_dot_grad": OpSpec("pointwise"),
     # stencils (stenpy_engine.py:1466-2197)
     "laplacian": OpSpec("stencil", 1), "gradient": OpSpec("stencil", 1, True),
     "divergence": OpSpec("stencil", 1, True), "curl": OpSpec("stencil", 1, True),
     "hessian": OpSpec("stencil", 2, True), "mean_curvature": OpSpec("stencil", 2, True),
     "grad_mag": OpSpec("stencil", 1, True), "jacobian": OpSpec("stencil", 1, True),
     "material_derivative": OpSpec("stencil", 1, True), "surface_normals": OpSpec("stencil", 1, True),
+    "gradient_nd": OpSpec("stencil", 1, True),
     # box and Gaussian smoothing (stenpy_engine.py:2385-2408, 2755-2860); the reach of
     # moving_average is window // 2
     "moving_average": OpSpec("stencil", 1), "conv3d_spectral": OpSpec("stencil", 1),
@@ -86,7 +91,7 @@ KNOWN_OPS: Dict[str, OpSpec] = {
     "sum": OpSpec("reduction"), "mean": OpSpec("reduction"), "norm_l2": OpSpec("reduction"),
     "variance": OpSpec("reduction"), "entropy": OpSpec("reduction"),
     "integrate": OpSpec("reduction"), "min_max": OpSpec("reduction"),
-    "entropy_hist": OpSpec("reduction"),
+    "entropy_hist": OpSpec("reduction"), "surface_integral": OpSpec("reduction"),
     # running trapezoid along dim 0 (stenpy_engine.py:2462-2483)
     "cumulative_integral": OpSpec("scan"),
 }
@@ -132,6 +137,10 @@ _BUILTINS: List[Tuple[str, int, str, int, int, int]] = [
     ("grad_mag", 1, "medium", 0, 0, 0), ("jacobian", 1, "high", 0, 0, 0),
     ("material_derivative", 1, "high", 0, 0, 0), ("moving_average", 0, "medium", 0, 0, 0),
     ("conv3d_spectral", 0, "very_high", 2, 8, 8), ("surface_normals", 1, "high", 0, 0, 0),
+    ("gradient_nd", 1, "high", 0, 0, 0), ("determinant", 0, "high", 0, 0, 0), ("inverse", 0, "very_high", 0, 0, 0),
+    ("deviatoric", 0, "medium", 0, 0, 0), ("stack_components", 0, "low", 0, 0, 0), ("norm_last", 0, "low", 0, 0, 0),
+    ("div_last", 0, "low", 0, 0, 0), ("neg_stack3", 0, "low", 0, 0, 0), ("scale_eye", 0, "low", 0, 0, 0),
+    ("velocity_dot_grad", 0, "low", 0, 0, 0), ("surface_integral", 0, "medium", 0, 0, 0),
     ("trace", 0, "low", 0, 0, 0), ("eigenvalues", 0, "very_high", 0, 0, 0),
     ("select_component", 0, "low", 0, 0, 0),
     ("sum", 0, "low", 0, 0, 0), ("mean", 0, "low", 0, 0, 0), ("norm_l2", 0, "low", 0, 0, 0),

@@ -144,6 +144,17 @@ CASES = [
     ("edt_clamp", "distance_transform(clamp(f))", "f", "periodic", 1.0, S_MIX),
     ("edt_even", "distance_transform(clamp(f*g))", "fg", "periodic", 1.0, S_EVEN),
     ("edt_plus", "distance_transform(clamp(f - 1)) + f", "f", "neumann", 1.0, S_ODD),
+    ("det_hess", "determinant(_hessian(f))", "f", "neumann", 1.0, S_MIX),
+    ("dev_hess", "deviatoric(_hessian(f)) * 2", "f", "periodic", 1.0, S_EVEN),
+    ("inv_spd", "inverse(_hessian(f) + scale_eye(f*f + 4, D=3))", "f", "neumann", 1.0, S_MIX),
+    ("gnd", "gradient_nd(f)", "f", "periodic", 0.5, S_ODD),
+    ("stack3", "stack_components(f, g, f*g)", "fg", "periodic", 1.0, S_MIX),
+    ("normlast", "norm_last(gradient(f))", "f", "neumann", 1.0, S_MIX),
+    ("divlast", "div_last(gradient(f), norm_last(gradient(f)))", "f", "periodic", 1.0, S_EVEN),
+    ("divlast_scalar", "div_last(curl(u), f*f + 1)", "fu", "neumann", 1.0, S_MIX),
+    ("negstack", "neg_stack3(f, g)", "fg", "periodic", 1.0, S_ODD),
+    ("vdotg", "velocity_dot_grad(f, g) + 1", "fg", "periodic", 1.0, S_ODD),
+    ("surfint", "surface_integral(gradient(f), curl(u), f*f)", "fu", "neumann", 1.0, S_MIX),
 ]
 
 # The reference's expression path hands conv3d_spectral a ``dx`` it does not accept

@@ -317,6 +317,13 @@ def velocity_dot_grad(v, g):
     return v * g
 
 
+def matmul_batched_custom(a):
+    """A·Aᵀ per matrix (stenpy_engine.py:2735-2742)."""
+    n = a.shape[-1]
+    b = a.reshape(-1, n, n)
+    return (b @ b.transpose(-1, -2)).reshape(*a.shape[:-2], n, n)
+
+
 def surface_integral(t, normals, area_weights):
     """Σ (t · normals) · area_weights (stenpy_engine.py:2486-2494)."""
     return ((t * normals).sum(dim=-1) * area_weights).sum()
@@ -507,6 +514,7 @@ OPS: Dict[str, Callable] = {
     "deviatoric": deviatoric, "stack_components": stack_components, "norm_last": norm_last,
     "div_last": div_last, "neg_stack3": neg_stack3, "scale_eye": scale_eye,
     "velocity_dot_grad": velocity_dot_grad, "surface_integral": surface_integral,
+    "matmul_batched_custom": matmul_batched_custom,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

@@ -426,6 +426,12 @@ class _Emitter:
             for i in range(3):
                 for j in range(3):
                     out.append(f"{o}[{3 * i + j}] = {cof}[{3 * j + i}] / {det};")
+        elif op == "aat3":
+            a = ins[0]   # A·Aᵀ: entry (i, j) = row i · row j
+            for i in range(3):
+                for j in range(3):
+                    out.append(f"{o}[{3 * i + j}] = ({a}[{3 * i}] * {a}[{3 * j}] + {a}[{3 * i + 1}] * {a}[{3 * j + 1}])"
+                               f" + {a}[{3 * i + 2}] * {a}[{3 * j + 2}];")
         elif op == "dev3":
             a = ins[0]
             q = self.t()

@@ -246,6 +246,11 @@ class OpLowerer:
             s = ins[0]
             z = self.pg.add("mulk", (s,), 1, self.r(s), k=0.0)   # s·0, as the reference's s·I entries
             return self.stack([s, z, z, z, s, z, z, z, s])
+        if op == "matmul_batched_custom":
+            need(1); no_extra()
+            if self.nc(ins[0]) != 9:
+                raise LoweringError("matmul_batched_custom: needs a (*, 3, 3) input")
+            return self.pg.add("aat3", (ins[0],), 9, self.r(ins[0]))
         if op == "velocity_dot_grad":
             need(2); no_extra()
             return self.binop("mul", ins[0], ins[1])

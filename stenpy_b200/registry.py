@@ -77,6 +77,7 @@ KNOWN_OPS: Dict[str, OpSpec] = {
     "determinant": OpSpec("pointwise"), "inverse": OpSpec("pointwise"), "deviatoric": OpSpec("pointwise"),
     "stack_components": OpSpec("pointwise"), "norm_last": OpSpec("pointwise"), "div_last": OpSpec("pointwise"),
     "neg_stack3": OpSpec("pointwise"), "scale_eye": OpSpec("pointwise"), "velocity_dot_grad": OpSpec("pointwise"),
+    "matmul_batched_custom": OpSpec("pointwise"),
     # stencils (stenpy_engine.py:1466-2197)
     "laplacian": OpSpec("stencil", 1), "gradient": OpSpec("stencil", 1, True),
     "divergence": OpSpec("stencil", 1, True), "curl": OpSpec("stencil", 1, True),
@@ -108,7 +109,7 @@ NO_STENCIL_OPS = {
     "spectral_laplacian",
     # added (conv3d_spectral accepts no dx: the reference's expression path passes one
     # and fails, here the op is reachable from expressions)
-    "cos", "abs", "entropy_hist", "conv3d_spectral",
+    "cos", "abs", "entropy_hist", "conv3d_spectral", "matmul_batched_custom",
 }
 
 
@@ -141,6 +142,7 @@ _BUILTINS: List[Tuple[str, int, str, int, int, int]] = [
     ("deviatoric", 0, "medium", 0, 0, 0), ("stack_components", 0, "low", 0, 0, 0), ("norm_last", 0, "low", 0, 0, 0),
     ("div_last", 0, "low", 0, 0, 0), ("neg_stack3", 0, "low", 0, 0, 0), ("scale_eye", 0, "low", 0, 0, 0),
     ("velocity_dot_grad", 0, "low", 0, 0, 0), ("surface_integral", 0, "medium", 0, 0, 0),
+    ("matmul_batched_custom", 0, "high", 2, 8, 8),
     ("trace", 0, "low", 0, 0, 0), ("eigenvalues", 0, "very_high", 0, 0, 0),
     ("select_component", 0, "low", 0, 0, 0),
     ("sum", 0, "low", 0, 0, 0), ("mean", 0, "low", 0, 0, 0), ("norm_l2", 0, "low", 0, 0, 0),

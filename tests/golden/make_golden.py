@@ -155,13 +155,15 @@ CASES = [
     ("negstack", "neg_stack3(f, g)", "fg", "periodic", 1.0, S_ODD),
     ("vdotg", "velocity_dot_grad(f, g) + 1", "fg", "periodic", 1.0, S_ODD),
     ("surfint", "surface_integral(gradient(f), curl(u), f*f)", "fu", "neumann", 1.0, S_MIX),
+    ("aat_hess", "matmul_batched_custom(_hessian(f))", "f", "neumann", 1.0, S_MIX),
 ]
 
-# The reference's expression path hands conv3d_spectral a ``dx`` it does not accept
-# (a TypeError at run time), so these cases build the reference graph directly: the
-# inner expression, then the operator node on top (stenpy_engine.py:2800-2860).
+# The reference's expression path hands conv3d_spectral and matmul_batched_custom a
+# ``dx`` they do not accept (a TypeError at run time), so these cases build the
+# reference graph directly: the inner expression, then the operator node on top
+# (stenpy_engine.py:2735-2748, 2800-2860).
 GRAPH_BUILT = {"gauss27": ("f", "conv3d_spectral"), "gauss27_odd": ("g", "conv3d_spectral"),
-               "gauss27_of_expr": ("f*g + 1", "conv3d_spectral")}
+               "gauss27_of_expr": ("f*g + 1", "conv3d_spectral"), "aat_hess": ("_hessian(f)", "matmul_batched_custom")}
 
 
 def main(ref_dir: str) -> None:

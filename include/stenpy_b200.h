@@ -106,6 +106,8 @@ int stenpy_encode_tmap_3d(void* out128, int elem_bytes, const void* base,
 #define STENPY_RED_ENTROPY 4   /* (sum|x|, sum|x|log|x|)        -> entropy    */
 #define STENPY_RED_INTEGRATE 5 /* (sum w x)                     -> sum        */
 #define STENPY_RED_MIN_MAX 6   /* (min, max)                    -> 2 values   */
+#define STENPY_RED_COVARIANCE 7  /* (n, mean a, mean b, C, M2a, M2b) -> C/(n-1)   */
+#define STENPY_RED_CORRELATION 8 /* same co-moments -> C/(sqrt(M2a M2b)+eps)       */
 
 typedef struct StenReduceDesc {
   int32_t kind;      /* STENPY_RED_* */

@@ -317,6 +317,23 @@ def velocity_dot_grad(v, g):
     return v * g
 
 
+def covariance(a, b):
+    """Centred dot product over max(n − 1, 1) (stenpy_engine.py:2575-2590, CPU branch)."""
+    if a.shape != b.shape:
+        raise ValueError(f"covariance: shape mismatch {a.shape} vs {b.shape}")
+    af, bf = (a - a.mean()).flatten(), (b - b.mean()).flatten()
+    return torch.dot(af, bf) / max(af.numel() - 1, 1)
+
+
+def correlation(a, b):
+    """Centred dot product over the product of the centred norms + 1e-15
+    (stenpy_engine.py:2595-2613, CPU branch)."""
+    if a.shape != b.shape:
+        raise ValueError(f"correlation: shape mismatch {a.shape} vs {b.shape}")
+    af, bf = (a - a.mean()).flatten(), (b - b.mean()).flatten()
+    return torch.dot(af, bf) / (af.norm() * bf.norm() + 1e-15)
+
+
 def matmul_batched_custom(a):
     """A·Aᵀ per matrix (stenpy_engine.py:2735-2742)."""
     n = a.shape[-1]
@@ -514,7 +531,7 @@ OPS: Dict[str, Callable] = {
     "deviatoric": deviatoric, "stack_components": stack_components, "norm_last": norm_last,
     "div_last": div_last, "neg_stack3": neg_stack3, "scale_eye": scale_eye,
     "velocity_dot_grad": velocity_dot_grad, "surface_integral": surface_integral,
-    "matmul_batched_custom": matmul_batched_custom,
+    "matmul_batched_custom": matmul_batched_custom, "covariance": covariance, "correlation": correlation,
     "trace": trace, "eigenvalues": eigenvalues, "select_component": select_component,
     "sum": sum_, "mean": mean, "norm_l2": norm_l2, "variance": variance, "entropy": entropy,
     "min_max": min_max, "integrate": integrate, "cumulative_integral": cumulative_integral,

@@ -48,7 +48,8 @@ class LaunchDesc(ctypes.Structure):
 
 NOALLOC_MAX_PARTIALS = 1 << 19
 
-RED_SUM, RED_MEAN, RED_NORM_L2, RED_VARIANCE, RED_ENTROPY, RED_INTEGRATE, RED_MIN_MAX = range(7)
+RED_SUM, RED_MEAN, RED_NORM_L2, RED_VARIANCE, RED_ENTROPY, RED_INTEGRATE, RED_MIN_MAX, RED_COVARIANCE, \
+    RED_CORRELATION = range(9)
 MAX_REDUCTIONS = 32
 
 _lib: Optional[ctypes.CDLL] = None

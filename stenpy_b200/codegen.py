@@ -152,6 +152,7 @@ class PassSpec:
 
 _REMAP_RULES = ("periodic", "replicate", "reflect")
 STENCIL_PRIMS = ("d1", "lap", "taps")   # primitives that read their input at offsets
+RED_SCRATCH_DOUBLES = 6 * 32   # block-reduction scratch: six values per warp (co-moments)
 _EXTRAPOLATED = ("edge2", "edge1", "edge2x2")  # ghost rules that compute a value, not copy one
 
 
@@ -868,7 +869,7 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
             off += plane_bytes(spec, f) * nslot
     off = (off + 127) // 128 * 128
     red_off = off
-    off += 3 * 32 * 8
+    off += RED_SCRATCH_DOUBLES * 8
     off += sum(4 * r.bins for r in spec.roots if r.kind == "red" and r.red == "hist")
     return off, rings, red_off
 
@@ -984,6 +985,15 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
             ri += 1
             if r.red == "sum" and _sum_from_var(spec, r) is not None:
                 continue  # derived from the variance accumulator of the same value
+            if r.red == "cov":
+                h = f"rv{ri_here}"
+                for c in range(nc // 2):
+                    a_, b_ = f"(double)rv[{off + c}]", f"(double)rv[{off + nc // 2 + c}]"
+                    K.append(f"{{ const double a_ = {a_}, b_ = {b_}; if (!{h}_h) {{ {h}_pa = a_; {h}_pb = b_; {h}_h = true; }}"
+                             f" const double da_ = a_ - {h}_pa, db_ = b_ - {h}_pb; {h}_sa += da_; {h}_sb += db_;"
+                             f" {h}_sab = fma(da_, db_, {h}_sab); {h}_saa = fma(da_, da_, {h}_saa);"
+                             f" {h}_sbb = fma(db_, db_, {h}_sbb); ++{h}_n; }}")
+                continue
             if r.red == "sumsq" and nc > 1:
                 terms = " + ".join(f"rv[{off + c}] * rv[{off + c}]" for c in range(nc))
                 K.append(f"rv{ri_here}_a += (double)({terms});")
@@ -1040,7 +1050,7 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
 def hist_offsets(spec: PassSpec, red_off: int) -> Tuple[Dict[int, int], int]:
     """Shared-memory byte offsets of the per-CTA histograms (by reduction-root
     index) placed after the block-reduction scratch, and the end of the region."""
-    off = red_off + 3 * 32 * 8
+    off = red_off + RED_SCRATCH_DOUBLES * 8
     offs: Dict[int, int] = {}
     for ri, r in enumerate([r for r in spec.roots if r.kind == "red"]):
         if r.red == "hist":
@@ -1072,6 +1082,10 @@ def _red_decls(spec: PassSpec, where: str = "main") -> List[str]:
                 K.append(f"unsigned long long* rv{ri}_hs = p.hist + {r.slot};")
         elif r.red == "var":
             K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
+        elif r.red == "cov":
+            # pivot-shifted sums of the pairs (a, b): n, Σda, Σdb, Σda·db, Σda², Σdb²
+            K.append(f"double rv{ri}_pa = 0.0, rv{ri}_pb = 0.0, rv{ri}_sa = 0.0, rv{ri}_sb = 0.0, rv{ri}_sab = 0.0, "
+                     f"rv{ri}_saa = 0.0, rv{ri}_sbb = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
         elif r.red in ("entropy",):
             K.append(f"double rv{ri}_a = 0.0, rv{ri}_b = 0.0;")
         elif r.red == "minmax":
@@ -1106,6 +1120,14 @@ def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
                 K.append("__syncthreads();")
                 K.append(f"for (int b_ = tid; b_ < {r.bins}; b_ += NT) {{ const unsigned int c_ = rv{ri}_hs[b_];"
                          f" if (c_) atomicAdd(p.hist + {r.slot} + b_, (unsigned long long)c_); }}")
+        elif r.red == "cov":
+            h = f"rv{ri}"
+            K.append(f"{{ const double n_ = (double){h}_n; double x_[6] = {{n_, 0.0, 0.0, 0.0, 0.0, 0.0}};")
+            K.append(f"  if (n_ > 0.0) {{ x_[1] = {h}_pa + {h}_sa / n_; x_[2] = {h}_pb + {h}_sb / n_;"
+                     f" x_[3] = {h}_sab - {h}_sa * {h}_sb / n_; x_[4] = fmax({h}_saa - {h}_sa * {h}_sa / n_, 0.0);"
+                     f" x_[5] = fmax({h}_sbb - {h}_sb * {h}_sb / n_, 0.0); }}")
+            K.append("  block_co(x_, red_scratch);")
+            K.append(f"  if (tid == 0) for (int i_ = 0; i_ < 6; ++i_) {base} + i_] = x_[i_]; }}")
         elif r.red == "var":
             K.append(f"{{ double n_ = (double)rv{ri}_n, mu_ = 0.0, q_ = 0.0;")
             K.append(f"  if (n_ > 0.0) {{ mu_ = rv{ri}_piv + rv{ri}_s1 / n_; q_ = rv{ri}_s2 - rv{ri}_s1 * rv{ri}_s1 / n_; if (q_ < 0.0) q_ = 0.0; }}")
@@ -1966,7 +1988,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                      f"sten_shell(const __grid_constant__ Params p) {{")
             K.append("  const Params& pg = p;")
             K.append("  const int bx = blockIdx.x;")
-            K.append(f"  __shared__ double red_scratch[96];")
+            K.append(f"  __shared__ double red_scratch[{RED_SCRATCH_DOUBLES}];")
         K.append("  const int tid = threadIdx.x;")
         K += ["  " + k for k in _red_decls(spec, "shell")]
         K.append("  const long long n0 = p.n0g, n1 = p.n1, n2 = p.n2;")
@@ -2010,7 +2032,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     hists = [r for r in reds if r.red == "hist"]
     if hists and not batch:
         K.append('extern "C" __global__ void __launch_bounds__(256) sten_hist_final(const __grid_constant__ Params p) {')
-        K.append("  __shared__ double red_scratch[96];")
+        K.append(f"  __shared__ double red_scratch[{RED_SCRATCH_DOUBLES}];")
         K.append("  const double nvox = (double)p.n0g * (double)p.n1 * (double)p.n2;")
         for r in hists:
             nc = e.g.nodes[r.node].nc

@@ -294,8 +294,32 @@ STEN_DEV void warp_chan(double& n, double& mean, double& m2) {
   }
 }
 
+// co-moments of two variables: (n, mean a, mean b, C = sum da db, M2 a, M2 b), merged as
+// Chan et al. merge (n, mean, M2) pairs, with C's cross term da db n nb / (n + nb)
+STEN_DEV void co_merge(double* x, const double* y) {
+  const double nt = x[0] + y[0];
+  if (nt == 0.0) return;
+  const double da = y[1] - x[1], db = y[2] - x[2], w = y[0] / nt, f = x[0] * w;
+  x[1] += da * w; x[2] += db * w;
+  x[3] += y[3] + da * db * f;
+  x[4] += y[4] + da * da * f;
+  x[5] += y[5] + db * db * f;
+  x[0] = nt;
+}
+STEN_DEV void warp_co(double* x) {
+  #pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double y[6];
+    #pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] = __shfl_xor_sync(0xffffffffu, x[i], o);
+    // fixed operand order per lane pair keeps the result identical on both lanes
+    if ((threadIdx.x & o) == 0) co_merge(x, y);
+    else { co_merge(y, x); for (int i = 0; i < 6; ++i) x[i] = y[i]; }
+  }
+}
+
 // Block-level reductions through a small shared scratch (one value per warp).
-// All threads of the block must call these; `scratch` holds >= 3*32 doubles.
+// All threads of the block must call these; `scratch` holds >= 6*32 doubles.
 STEN_DEV double block_sum(double v, double* scratch) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   v = warp_sum(v);
@@ -343,6 +367,20 @@ STEN_DEV void block_chan(double& n, double& mean, double& m2, double* scratch) {
   }
 }
 
+STEN_DEV void block_co(double* x, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  warp_co(x);
+  __syncthreads();
+  if (lane == 0) for (int i = 0; i < 6; ++i) scratch[32 * i + warp] = x[i];
+  __syncthreads();
+  if (warp == 0) {
+    double y[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (lane < nw) for (int i = 0; i < 6; ++i) y[i] = scratch[32 * i + lane];
+    warp_co(y);
+    for (int i = 0; i < 6; ++i) x[i] = y[i];
+  }
+}
+
 // ------------------------------------------------------------------ histograms
 // sum over non-empty bins of q log q, q = count / n (the entropy is its negation),
 // clearing the counts for the next run. Fixed bins per thread and a fixed
@@ -366,6 +404,8 @@ STEN_DEV double sten_hist_qlogq(unsigned long long* h, int bins, double n, doubl
 #define STEN_RED_ENTROPY 4
 #define STEN_RED_INTEGRATE 5
 #define STEN_RED_MIN_MAX 6
+#define STEN_RED_COVARIANCE 7
+#define STEN_RED_CORRELATION 8
 // Combine rows part[c * nslots + slot], c < ncta, into the final value(s) at out[0]
 // (out[1] for min/max). Each thread folds rows t, t + blockDim, ... in order and a
 // fixed warp/block tree combines them: deterministic for a given block size.
@@ -373,6 +413,19 @@ STEN_DEV double sten_hist_qlogq(unsigned long long* h, int bins, double n, doubl
 STEN_DEV void sten_reduce_rows(int kind, const double* part, int ncta, int nslots, int slot, int unbiased,
                                double count, double eps, double* out, double* scratch) {
   const int t = threadIdx.x;
+  if (kind == STEN_RED_COVARIANCE || kind == STEN_RED_CORRELATION) {
+    double x[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int c = t; c < ncta; c += blockDim.x) {
+      const double* row = part + (size_t)c * nslots + slot;
+      double y[6];
+      for (int i = 0; i < 6; ++i) y[i] = __ldcg(row + i);
+      co_merge(x, y);
+    }
+    block_co(x, scratch);
+    if (t == 0) out[0] = kind == STEN_RED_COVARIANCE ? x[3] / (x[0] - 1.0 > 1.0 ? x[0] - 1.0 : 1.0)
+                                                    : x[3] / (sqrt(x[4]) * sqrt(x[5]) + eps);
+    return;
+  }
   double x0 = 0.0, x1 = 0.0, x2 = 0.0;
   if (kind == STEN_RED_MIN_MAX) { x0 = __longlong_as_double(0x7ff0000000000000ll); x1 = -x0; }
   for (int c = t; c < ncta; c += blockDim.x) {

@@ -301,6 +301,16 @@ struct FinalizeArgs {
   StenReduceDesc d[STENPY_MAX_REDUCTIONS];
 };
 
+__device__ static void co(double* x, const double* y) {
+  // co-moments (n, mean a, mean b, C, M2 a, M2 b) of two groups merged
+  double nt = x[0] + y[0];
+  if (nt == 0.0) return;
+  double da = y[1] - x[1], db = y[2] - x[2], w = y[0] / nt, f = x[0] * w;
+  x[1] += da * w; x[2] += db * w;
+  x[3] += y[3] + da * db * f; x[4] += y[4] + da * da * f; x[5] += y[5] + db * db * f;
+  x[0] = nt;
+}
+
 __device__ static void chan(double& n, double& m, double& q, double nb, double mb, double qb) {
   double nt = n + nb;
   if (nt == 0.0) return;
@@ -316,8 +326,38 @@ __global__ void __launch_bounds__(256) sten_finalize_kernel(const double* __rest
                                                             int nslots, FinalizeArgs a,
                                                             double* __restrict__ out) {
   __shared__ double s0[256], s1[256], s2[256];
+  __shared__ double sc[6][256];
   const StenReduceDesc d = a.d[blockIdx.x];
   const int t = threadIdx.x;
+  if (d.kind == STENPY_RED_COVARIANCE || d.kind == STENPY_RED_CORRELATION) {
+    // rows folded in order as below, then a fixed tree
+    double x[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int c = t; c < ncta; c += 256) {
+      const double* row = part + (size_t)c * nslots + d.slot;
+      double y[6];
+      for (int i = 0; i < 6; ++i) y[i] = row[i];
+      co(x, y);
+    }
+    for (int i = 0; i < 6; ++i) sc[i][t] = x[i];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (t < w) {
+        double xa[6], yb[6];
+        for (int i = 0; i < 6; ++i) { xa[i] = sc[i][t]; yb[i] = sc[i][t + w]; }
+        co(xa, yb);
+        for (int i = 0; i < 6; ++i) sc[i][t] = xa[i];
+      }
+      __syncthreads();
+    }
+    if (t == 0) {
+      double* o = out + d.out_index;
+      const double n = sc[0][0], c = sc[3][0];
+      // covariance: C / max(n - 1, 1); correlation: C / (|a - mean a| |b - mean b| + eps)
+      o[0] = d.kind == STENPY_RED_COVARIANCE ? c / (n - 1.0 > 1.0 ? n - 1.0 : 1.0)
+                                             : c / (sqrt(sc[4][0]) * sqrt(sc[5][0]) + d.eps);
+    }
+    return;
+  }
   double x0 = 0.0, x1 = 0.0, x2 = 0.0;
   if (d.kind == STENPY_RED_MIN_MAX) { x0 = INFINITY; x1 = -INFINITY; }
   // rows t, t + 256, ... folded in that order; the loads of FOLD_U rows are issued

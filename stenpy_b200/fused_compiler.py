@@ -53,7 +53,7 @@ NVRTC_OPTS = ["--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-l
 
 REDUCTIONS = {"sum": "sum", "mean": "sum", "norm_l2": "sumsq", "variance": "var",
               "entropy": "entropy", "integrate": "integrate", "min_max": "minmax"}
-RED_SLOTS = {"sum": 1, "sumsq": 1, "var": 3, "entropy": 2, "integrate": 1, "minmax": 2}
+RED_SLOTS = {"sum": 1, "sumsq": 1, "var": 3, "entropy": 2, "integrate": 1, "minmax": 2, "cov": 6}
 RED_KIND = {"sum": N.RED_SUM, "mean": N.RED_MEAN, "norm_l2": N.RED_NORM_L2, "variance": N.RED_VARIANCE,
             "entropy": N.RED_ENTROPY, "integrate": N.RED_INTEGRATE, "min_max": N.RED_MIN_MAX}
 
@@ -353,6 +353,21 @@ class Planner:
                 rspecs.append(RootSpec("red", pn, red="sum", slot=nslots))
                 reductions.append(RedPlan(nid, nslots, self.red_index[nid], N.RED_SUM, float(n_vox), 0, 0.0))
                 nslots += RED_SLOTS["sum"]
+            elif node.op_name in ("covariance", "correlation"):
+                # co-moments of the value pairs (stenpy_engine.py:2575-2613, CPU branch: the
+                # centred dot product over n - 1, or over the product of centred norms)
+                extra = set(node.params) - {"alloc", "mm"}
+                if len(node.input_ids) != 2 or extra:
+                    raise FusionError(f"{node.op_name}: two fields and no parameters")
+                a_, b_ = (lower(i) for i in node.input_ids)
+                nc = pg.nodes[a_].nc
+                if pg.nodes[b_].nc != nc:
+                    raise FusionError(f"{node.op_name}: shape mismatch ({nc} vs {pg.nodes[b_].nc} components)")
+                pn = low.stack([a_, b_])
+                rspecs.append(RootSpec("red", pn, red="cov", slot=nslots))
+                kind = N.RED_COVARIANCE if node.op_name == "covariance" else N.RED_CORRELATION
+                reductions.append(RedPlan(nid, nslots, self.red_index[nid], kind, float(n_vox * nc), 0, 1e-15))
+                nslots += RED_SLOTS["cov"]
             elif node.op_name == "entropy_hist":
                 extra = set(node.params) - {"bins", "alloc", "mm"}
                 if extra:

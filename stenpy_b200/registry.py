@@ -93,6 +93,7 @@ KNOWN_OPS: Dict[str, OpSpec] = {
     "variance": OpSpec("reduction"), "entropy": OpSpec("reduction"),
     "integrate": OpSpec("reduction"), "min_max": OpSpec("reduction"),
     "entropy_hist": OpSpec("reduction"), "surface_integral": OpSpec("reduction"),
+    "covariance": OpSpec("reduction"), "correlation": OpSpec("reduction"),
     # running trapezoid along dim 0 (stenpy_engine.py:2462-2483)
     "cumulative_integral": OpSpec("scan"),
 }
@@ -142,7 +143,8 @@ _BUILTINS: List[Tuple[str, int, str, int, int, int]] = [
     ("deviatoric", 0, "medium", 0, 0, 0), ("stack_components", 0, "low", 0, 0, 0), ("norm_last", 0, "low", 0, 0, 0),
     ("div_last", 0, "low", 0, 0, 0), ("neg_stack3", 0, "low", 0, 0, 0), ("scale_eye", 0, "low", 0, 0, 0),
     ("velocity_dot_grad", 0, "low", 0, 0, 0), ("surface_integral", 0, "medium", 0, 0, 0),
-    ("matmul_batched_custom", 0, "high", 2, 8, 8),
+    ("matmul_batched_custom", 0, "high", 2, 8, 8), ("covariance", 0, "medium", 0, 0, 0),
+    ("correlation", 0, "medium", 0, 0, 0),
     ("trace", 0, "low", 0, 0, 0), ("eigenvalues", 0, "very_high", 0, 0, 0),
     ("select_component", 0, "low", 0, 0, 0),
     ("sum", 0, "low", 0, 0, 0), ("mean", 0, "low", 0, 0, 0), ("norm_l2", 0, "low", 0, 0, 0),

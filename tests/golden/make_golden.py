@@ -156,6 +156,9 @@ CASES = [
     ("vdotg", "velocity_dot_grad(f, g) + 1", "fg", "periodic", 1.0, S_ODD),
     ("surfint", "surface_integral(gradient(f), curl(u), f*f)", "fu", "neumann", 1.0, S_MIX),
     ("aat_hess", "matmul_batched_custom(_hessian(f))", "f", "neumann", 1.0, S_MIX),
+    ("cov_fg", "covariance(f, g)", "fg", "periodic", 1.0, S_MIX),
+    ("corr_fg", "correlation(f*g, laplacian(f))", "fg", "periodic", 1.0, S_EVEN),
+    ("cov_vec", "covariance(curl(u), gradient(f)) + correlation(f, f)", "fu", "neumann", 1.0, S_MIX),
 ]
 
 # The reference's expression path hands conv3d_spectral and matmul_batched_custom a

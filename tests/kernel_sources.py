@@ -173,6 +173,13 @@ def all_sources():
                     seen.add(k)
                     ps.append(pp.spec)
         src.append(emit_batch_module(ps, 128, B.batch_min_blocks(128)))
+    for dt in (torch.float32, torch.bfloat16):     # covariance / correlation
+        for shape in [(17, 9, 130), (40, 33, 64), (3, 3, 3)]:
+            exprs = {"c": "covariance(f, g)", "r": "correlation(f, g)", "rr": "correlation(f, f)",
+                     "cl": "covariance(laplacian(f), g)"}
+            g, sinks, *_ = S.compile_expressions(exprs, boundary="periodic",
+                                                 field_map={"f": _ph(shape, dt), "g": _ph(shape, dt)})
+            src += plan_sources(g, list(sinks.values()))
     from stenpy_b200.geometry import edt_source   # distance transform (per dtype and longest line)
     for dt in (torch.float32, torch.float64, torch.bfloat16, torch.float16):
         src += [edt_source(dt, nmax) for nmax in (16, 32, 64)]

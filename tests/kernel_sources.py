@@ -176,7 +176,7 @@ def all_sources():
     for dt in (torch.float32, torch.bfloat16):     # covariance / correlation
         for shape in [(17, 9, 130), (40, 33, 64), (3, 3, 3)]:
             exprs = {"c": "covariance(f, g)", "r": "correlation(f, g)", "rr": "correlation(f, f)",
-                     "cl": "covariance(laplacian(f), g)"}
+                     "cl": "covariance(laplacian(g), f)"}
             g, sinks, *_ = S.compile_expressions(exprs, boundary="periodic",
                                                  field_map={"f": _ph(shape, dt), "g": _ph(shape, dt)})
             src += plan_sources(g, list(sinks.values()))

@@ -188,12 +188,12 @@ def test_covariance_and_correlation(dtype):
         f = (sinusoid_field(shape, seed=41).double() * 0.01 + 100.0).to(dtype)
         g = uniform_field(shape, seed=42).to(dtype)
         exprs = {"c": "covariance(f, g)", "r": "correlation(f, g)", "rr": "correlation(f, f)",
-                 "cl": "covariance(laplacian(f), g)"}
+                 "cl": "covariance(laplacian(g), f)"}
         gr, sinks, *_ = S.compile_expressions(exprs, boundary="periodic", field_map={"f": f.to(dev), "g": g.to(dev)})
         res = S.Runtime(device=dev).run(gr, wanted=list(sinks.values()))
         g2, s2, *_ = S.compile_expressions(exprs, boundary="periodic", field_map={"f": f.double(), "g": g.double()})
         ref = O.evaluate(g2, list(s2.values()))
         for k in exprs:
             a, b = float(res[sinks[k]]), float(ref[s2[k]])
-            tol = 1e-3 if k == "cl" else 1e-9   # cl: the FP32 Laplacian of offset data
+            tol = 1e-5 if k == "cl" else 1e-9   # cl: an FP32 Laplacian
             assert abs(a - b) <= tol * max(abs(b), 1e-6), (k, shape, a, b)

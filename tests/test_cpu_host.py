@@ -102,16 +102,45 @@ def test_generated_kernels_compile_for_sm100a(expr, boundary):
         assert len(cubin) > 1000
 
 
+def _shell_decode(t, shape, R, g_lo, g_hi):
+    """Host model of ``sten_shell``'s voxel decode (regions A, B, C), formula for formula."""
+    n0, n1, n2 = shape
+    a1, a2 = max(n1 - 2 * R, 0), max(n2 - 2 * R, 0)
+    c_low = max(0, min(g_hi, R) - g_lo)
+    hs = max(g_lo, max(n0 - R, R))
+    c_high = max(0, g_hi - hs)
+    ii0 = max(g_lo, R)
+    n_int = max(0, min(g_hi, n0 - R) - ii0)
+    cA, cB = (c_low + c_high) * n1 * n2, n_int * (n1 - a1) * n2
+    if t < cA:
+        q, r = divmod(t, n1 * n2)
+        return (g_lo + q if q < c_low else hs + (q - c_low), r // n2, r % n2)
+    if t < cA + cB:
+        u, w1 = t - cA, n1 - a1
+        q, r = divmod(u, w1 * n2)
+        jr, lo = r // n2, min(R, n1)
+        return ii0 + q, (jr if jr < lo else n1 - (w1 - jr)), r - jr * n2
+    u, w2, per = t - cA - cB, n2 - a2, n_int * a1
+    kr, r = divmod(u, per)
+    q, jr = divmod(r, a1)
+    lo = min(R, n2)
+    return ii0 + q, R + jr, (kr if kr < lo else n2 - (w2 - kr))
+
+
 def test_shell_decode_matches_boundary_shell():
-    """Every global plane range of small grids: count formula == true shell size
-    (the kernel's decode is exercised on the GPU; its count is what the host sizes)."""
-    for shape in [(5, 7, 33), (3, 3, 3), (1, 4, 5), (9, 10, 11), (6, 2, 7)]:
+    """Every global plane range of small grids: the count formula is the true shell
+    size, and the kernel's decode (host model) maps thread indices one to one onto the
+    shell voxels."""
+    for shape in [(5, 7, 33), (3, 3, 3), (1, 4, 5), (9, 10, 11), (6, 2, 7), (12, 11, 9)]:
         for R in (1, 2, 3):
             n0, n1, n2 = shape
             for g_lo, g_hi in [(0, n0), (1, n0), (0, max(1, n0 - 1))]:
-                truth = sum(1 for i in range(g_lo, g_hi) for j in range(n1) for k in range(n2)
-                            if not (R <= i < n0 - R and R <= j < n1 - R and R <= k < n2 - R))
-                assert shell_count(shape, R, g_lo, g_hi) == truth
+                truth = {(i, j, k) for i in range(g_lo, g_hi) for j in range(n1) for k in range(n2)
+                         if not (R <= i < n0 - R and R <= j < n1 - R and R <= k < n2 - R)}
+                cnt = shell_count(shape, R, g_lo, g_hi)
+                assert cnt == len(truth)
+                got = [_shell_decode(t, shape, R, g_lo, g_hi) for t in range(cnt)]
+                assert set(got) == truth and len(set(got)) == cnt, (shape, R, g_lo, g_hi)
 
 
 def test_cpu_device_is_rejected():

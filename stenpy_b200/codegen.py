@@ -2015,11 +2015,11 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("      const long long jr = r / n2, lo = min((long long)RAD, n1);")
         K.append("      i = ii0 + q; j = jr < lo ? jr : n1 - (w1 - jr); k = r - jr * n2;")
         K.append("    } else {                  // interior rows, columns within RAD of a dim-2 face")
-        # column-major: a warp shares one face column (no divergence between the two
-        # faces' one-sided formulas) and walks adjacent rows (their neighbours overlap)
-        K.append("      const long long u = t - cA - cB, w2 = n2 - a2, per = n_int * a1;")
-        K.append("      const long long kr = u / per, r = u - kr * per, q = r / a1, jr = r - q * a1;")
-        K.append("      const long long lo = min((long long)RAD, n2);")
+        # row-major (both faces' columns of a row next to each other): measured faster
+        # on B200 than one face column per warp, which walks rows n2 apart
+        K.append("      const long long u = t - cA - cB, w2 = n2 - a2;")
+        K.append("      const long long q = u / (a1 * w2), r = u - q * a1 * w2;")
+        K.append("      const long long jr = r / w2, kr = r - jr * w2, lo = min((long long)RAD, n2);")
         K.append("      i = ii0 + q; j = RAD + jr; k = kr < lo ? kr : n2 - (w2 - kr);")
         K.append("    }")
         K.append("    const int gi = (int)i;")

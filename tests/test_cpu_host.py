@@ -120,9 +120,9 @@ def _shell_decode(t, shape, R, g_lo, g_hi):
         q, r = divmod(u, w1 * n2)
         jr, lo = r // n2, min(R, n1)
         return ii0 + q, (jr if jr < lo else n1 - (w1 - jr)), r - jr * n2
-    u, w2, per = t - cA - cB, n2 - a2, n_int * a1
-    kr, r = divmod(u, per)
-    q, jr = divmod(r, a1)
+    u, w2 = t - cA - cB, n2 - a2
+    q, r = divmod(u, a1 * w2)
+    jr, kr = divmod(r, w2)
     lo = min(R, n2)
     return ii0 + q, R + jr, (kr if kr < lo else n2 - (w2 - kr))
 

@@ -51,7 +51,7 @@ HEADLINE = "fp16"
 # DRAM bytes (read + write) of one launch of the headline form's dominant pass at
 # 512^3, from an ncu capture of this command's kernels (profiles/ summary of
 # sten_kernel at 512^3, FP16); null for other sizes or forms
-NCU_TRAFFIC = {("fp16", 512): 284129280 + 231270144}
+NCU_TRAFFIC = {("fp16", 512): 284091392 + 230927360}
 
 
 def _peaks():

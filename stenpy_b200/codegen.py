@@ -1277,7 +1277,9 @@ def _lsu_request(spec: "PassSpec", f: "FieldSpec", rings: Dict[int, int], cfg: "
         pre = f"      if ({cond[0]}) {{ " if cond else "      { "
         L.append(pre + " ".join(body) + (" g += rstep;" if k + 1 < nk else "") + " }")
     L.append("    }")
-    L.append("  } else")
+    if v == 2 and es == 2:
+        L += _lsu_odd16(spec, f, cfg, pitch, rp, nk, ncc, tc, u, w, h, guard_rs, guard_r, guard_c)
+    L.append("  } else {")
     L.append(f"  if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{")
     for k in range(nk):
         L.append("    {")
@@ -1340,8 +1342,67 @@ def _lsu_request(spec: "PassSpec", f: "FieldSpec", rings: Dict[int, int], cfg: "
             L.append("        }")
             L.append("    }")
         L.append("  }")
+    L.append("  }")
     L.append("}")
     return L
+
+
+def _lsu_odd16(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", pitch: str, rp: int, nk: int, ncc: int,
+               tc: int, u: int, w: int, h: int, guard_rs: bool, guard_r: bool, guard_c: bool) -> List[str]:
+    """Tiles inside a 16-bit field whose rows have an odd number of elements: row
+    starts alternate between 4-byte alignment and 2 bytes past it. Aligned rows copy
+    their element pairs with asynchronous 4-byte copies; each pair of a misaligned row
+    is cut out of the two aligned words around it (loaded first for every row of the
+    thread, so their latencies overlap) and stored as one aligned word. The words
+    reach 2 bytes before and after the pair: a misaligned row never starts the field,
+    and the plane holding the field's last element is left to the general path."""
+    sl = f.slot
+    hk = spec.hk(f)
+    L = [f"  }} else if (zok && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && tk0 >= {hk} && "
+         f"tk0 + TK + {hk} <= p.n2 && {pitch} % 4 == 2 && ((size_t)fb) % 4 == 0 && "
+         f"!(zq == p.nl - 1 && tj0 + TJ + {f.halo} == p.n1 && tk0 + TK + {hk} == p.n2)) {{",
+         f"    if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{",
+         f"      const long long j0 = (long long)zq * p.n1 + (tj0 - {f.halo} + rs{sl}_);",
+         f"      const char* g = fb + (size_t)j0 * {pitch} + (size_t)((tk0 - {hk}) * {f.nc * 2} + c0{sl}_ * 4);",
+         f"      const size_t rstep = {rp} * {pitch};",
+         f"      pend{sl}_ = true; psb{sl}_ = sb; pj{sl}_ = j0;"]
+    for k in range(nk):
+        cond = [f"rs{sl}_ + {k * rp} < {h}"] if guard_r else []
+        L.append(f"      {{ const bool mis = ((j0 + {k * rp}) & 1) != 0;" + (f" if ({cond[0]}) {{" if cond else " {"))
+        for cc in range(ncc):
+            cc_cond = f"c0{sl}_ + {cc * tc} < {u}" if guard_c and cc == ncc - 1 else "true"
+            sa = f"sb + {(k * rp * w + cc * tc * 2) * 2}u"
+            L.append(f"        if ({cc_cond}) {{ const char* gp = g + {cc * tc * 4};"
+                     f" if (!mis) cp_async_n<4>({sa}, gp, 4u);"
+                     f" else {{ wa{sl}_[{k}][{cc}] = __ldg((const u32*)(gp - 2)); wb{sl}_[{k}][{cc}] = __ldg((const u32*)(gp + 2)); }} }}")
+        L.append("      }" + (" g += rstep;" if k + 1 < nk else "") + " }")
+    L.append("    }")
+    return L
+
+
+def _lsu_odd16_state(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[List[str], List[str]]:
+    """Registers that carry the words of misaligned odd-length 16-bit rows from the
+    plane request that loads them to ``lsu_flush``, which cuts the pairs out and
+    stores them before the barrier that precedes the plane's use (one iteration of
+    the march later: the loads' latency hides behind one plane of compute)."""
+    w, h, es, v, u, tc, ncc, rp, nk = _lsu_geometry(spec, f, cfg)
+    sl = f.slot
+    decl = [f"u32 wa{sl}_[{nk}][{ncc}], wb{sl}_[{nk}][{ncc}], psb{sl}_ = 0u; long long pj{sl}_ = 0; bool pend{sl}_ = false;"]
+    flush = [f"if (pend{sl}_) {{", f"  pend{sl}_ = false;"]
+    guard_rs = rp * tc < cfg.threads
+    if guard_rs:
+        flush.append(f"  if (rs{sl}_ < {rp}) {{")
+    for k in range(nk):
+        cond = f"rs{sl}_ + {k * rp} < {h} && " if nk * rp > h else ""
+        for cc in range(ncc):
+            cc_cond = f"c0{sl}_ + {cc * tc} < {u} && " if ncc * tc > u and cc == ncc - 1 else ""
+            sa = f"psb{sl}_ + {(k * rp * w + cc * tc * 2) * 2}u"
+            flush.append(f"  if ({cond}{cc_cond}((pj{sl}_ + {k * rp}) & 1) != 0) "
+                         f"st_shared_u32({sa}, __byte_perm(wa{sl}_[{k}][{cc}], wb{sl}_[{k}][{cc}], 0x5432));")
+    if guard_rs:
+        flush.append("  }")
+    flush.append("}")
+    return decl, flush
 
 
 def lsu_mapping(w: int, h: int, nt: int) -> Tuple[int, int, int, int]:
@@ -1747,10 +1808,21 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
             K.append("  }")
             K.append("  __syncthreads();")
+        odd16 = [f for f in lsu_fields if f.vec == 2 and ESIZE[f.dtype] == 2]
         for f in lsu_fields:
             K += ["  " + x for x in _lsu_plan(spec, f, cfg, ghost)]
+        if odd16:
+            K.append("  // misaligned odd-length 16-bit rows: words loaded by request(), stored by lsu_flush()")
+            for f in odd16:
+                K += ["  " + x for x in _lsu_odd16_state(spec, f, cfg)[0]]
+            K.append("  auto lsu_flush = [&]() {")
+            for f in odd16:
+                K += ["    " + x for x in _lsu_odd16_state(spec, f, cfg)[1]]
+            K.append("  };")
         if staged:
             K.append("  auto request = [&](int q) {")
+            if odd16:
+                K.append("    lsu_flush();   // the previous request's misaligned rows (back-to-back requests)")
             K.append("    const int s = (q - p_first) % NSLOT;")
             if ghost and spec.i_periodic:
                 K.append("    const int zq = (q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q;")
@@ -1796,6 +1868,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K += ["  " + x for x in _ghost_fill(spec, rings)]
             if async_lsu:
                 K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) { request(q); cp_async_commit(); }")
+                if odd16:
+                    K.append("  lsu_flush();")
                 K.append("  cp_async_wait<0>();")
             else:
                 K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
@@ -1949,6 +2023,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             K.append(f"    cp_async_wait<{cfg.prefetch - 1}>();")
         if lsu_ghost:
             K.append("    if (edge_cta) { __syncthreads(); if (i + 1 < ie) ghost_fill(i + 1 + RAD); }")
+        if staged and odd16:
+            K.append("    lsu_flush();   // misaligned rows of the plane requested last iteration")
         if staged:
             # the ring slot of plane i - RAD is refilled next: every thread must be done with it
             K.append("    ok = __syncthreads_and(ok);")

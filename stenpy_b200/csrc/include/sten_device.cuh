@@ -185,9 +185,6 @@ STEN_DEV void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 // 4-byte asynchronous global->shared copy (completion by commit / wait groups)
-STEN_DEV void cp_async4(void* smem_dst, const void* gsrc) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
-}
 // asynchronous copy of N (4, 8 or 16) bytes to the shared address sdst, of which the
 // first src_bytes come from gsrc and the rest are zero (src_bytes 0: nothing is read;
 // gsrc must still be a mapped, N-aligned address)

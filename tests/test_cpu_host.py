@@ -431,6 +431,30 @@ def _emulate_staging(w, h, es, nc, halo, hk, tk0, tj0, n1, n2, rj, rk, nt, v, fb
                                 put(r * w + (c0 + cc * tc) * v + e, (ga - fb) // es + e)
                 g += rp * pitch
         return out
+    if (v == 2 and es == 2 and tj0 >= halo and tj0 + tj + halo <= n1 and tk0 >= hk and tk0 + tk + hk <= n2
+            and pitch % 4 == 2 and fb % 4 == 0 and not (tj0 + tj + halo == n1 and tk0 + tk + hk == n2)):
+        # odd-length 16-bit rows inside the field: aligned rows by pairs, the others by
+        # the two aligned words around each pair (plane 0 of a one-plane field here)
+        for tid in range(nt):
+            c0, rs = tid % tc, tid // tc
+            if rs >= rp:
+                continue
+            j0 = tj0 - halo + rs
+            g = fb + j0 * pitch + (tk0 - hk) * nc * 2 + c0 * 4
+            for k in range(nk):
+                r = rs + k * rp
+                if r < h:
+                    for cc in range(ncc):
+                        if c0 + cc * tc < u:
+                            gp = g + cc * tc * 4
+                            if (j0 + k * rp) % 2 == 0:
+                                assert gp % 4 == 0
+                            else:
+                                assert (gp - 2) % 4 == 0 and fb <= gp - 2 and gp + 6 <= fb + nbytes
+                            for e in range(2):
+                                put(r * w + (c0 + cc * tc) * 2 + e, (gp - fb) // 2 + e)
+                g += rp * pitch
+        return out
 
     for tid in range(nt):
         c0, rs = tid % tc, tid // tc

@@ -559,3 +559,12 @@ def test_spectral_operators_are_registered_and_gpu_only():
                                        field_map={"f": torch.zeros(4, 5, 6)})
     ops = {n.op_name: n.params for n in g.topological_sort()}
     assert ops["spectral_gradient"] == {"dim": 2, "dx": 0.5}
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64, torch.float16, torch.bfloat16])
+def test_distance_transform_kernels_compile_for_sm100a(dtype):
+    """The distance transform's row, envelope and finalize kernels build for sm_100a
+    for every storage dtype (no GPU needed: NVRTC only)."""
+    from stenpy_b200.geometry import _OPTS, edt_source
+    key, cubin = N.compile_cached(edt_source(dtype, 64), _OPTS)
+    assert len(cubin) > 1000

@@ -398,15 +398,3 @@ def _compile_worker(src: str) -> int:
     from . import fused_compiler as FC
     N.compile_cached(src, FC.NVRTC_OPTS)
     return 1
-
-
-def precompile(sources: Sequence[str], workers: Optional[int] = None) -> int:
-    """Compile kernel sources into the on-disk cache with a spawn-started process
-    pool (safe before or after the parent touches the GPU)."""
-    import multiprocessing as mp
-    todo = list(dict.fromkeys(sources))
-    if not todo:
-        return 0
-    workers = workers or max(1, min(32, (os.cpu_count() or 2) - 1))
-    with mp.get_context("spawn").Pool(workers) as pool:
-        return sum(pool.map(_compile_worker, todo, chunksize=4))

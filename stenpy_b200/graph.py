@@ -131,7 +131,3 @@ class Graph:
             keep.add(nid)
             stack.extend(self._nodes[nid].input_ids)
         return [nid for nid in self._order if nid in keep]
-
-
-def _graph_sinks(graph: Graph) -> List[str]:
-    return graph.sinks()

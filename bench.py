@@ -44,9 +44,17 @@ if HERE not in sys.path:
     sys.path.insert(0, HERE)
 
 EXPR = "divergence(gradient(f)) + l2norm(curl(u))"
+# the reference spells the global L2 norm norm_l2 (it has no l2norm operator)
+REF_EXPR = "divergence(gradient(f)) + norm_l2(curl(u))"
 REDS = ("sum", "mean", "variance")
-FORM_DT = {"fp32": torch.float32, "fp16": torch.float16, "bf16": torch.bfloat16}
-ALG_BYTES = {"fp32": 20, "fp16": 10, "bf16": 10}   # f + u(3) + out, each once
+# the metric both arms report (same string, so their lines compare)
+METRIC = "fused-expr Gvoxel/s & HBM % of roofline, BF16-store vs FP32, err vs FP64"
+# storage form -> (input storage dtype, result storage dtype)
+FORMS = {"fp32": (torch.float32, torch.float32), "fp16": (torch.float16, torch.float16),
+         "bf16": (torch.bfloat16, torch.bfloat16), "bf16in": (torch.bfloat16, torch.float32)}
+FORM_DT = {k: v[0] for k, v in FORMS.items()}
+# f + u(3) + out, each once at storage dtype
+ALG_BYTES = {k: 4 * i.itemsize + o.itemsize for k, (i, o) in FORMS.items()}
 HEADLINE = "fp16"
 # DRAM bytes (read + write) of one launch of the headline form's dominant pass at
 # 512^3, from an ncu capture of this command's kernels (profiles/ summary of
@@ -155,13 +163,13 @@ def build(form, f, u, device, tune=True, schedule=None):
     import stenpy_b200 as S
     from stenpy_b200 import autotune as AT
     from stenpy_b200 import fused_compiler as FC
-    dt = FORM_DT[form]
+    dt, odt = FORMS[form]
     g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
                                        field_map={"f": f.to(dt), "u": u.to(dt)})
     wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
     if schedule is not None:
         tune = False
-    plan = FC.get_plan(g, wanted, out_dtype=dt, config=schedule)
+    plan = FC.get_plan(g, wanted, out_dtype=odt, config=schedule)
     values, back = FC.bind(plan, g, wanted)
     tuned = AT.tune_plan(plan, values, device, tag=f"bench-{form}") if tune else []
     prog = FC.build_program(plan, values, device)
@@ -219,7 +227,7 @@ class E2E:
 
     def __init__(self, f_host, u_host, form, device):
         import stenpy_b200 as S
-        self.dt = FORM_DT[form]
+        self.dt, self.odt = FORMS[form]
         self.g, self.sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
                                                      field_map={"f": f_host, "u": u_host})
         self.wanted = [self.sink] + [self.g.add(r, (self.sink,), {}) for r in REDS]
@@ -232,8 +240,8 @@ class E2E:
                     self.leaf["f"] = nid
                 elif v is u_host:
                     self.leaf["u"] = nid
-        self.rt = S.Runtime(device=device, out_dtype=self.dt, check_errors=False)
-        self.out_host = torch.empty(tuple(f_host.shape), dtype=self.dt, pin_memory=True)
+        self.rt = S.Runtime(device=device, out_dtype=self.odt, check_errors=False)
+        self.out_host = torch.empty(tuple(f_host.shape), dtype=self.odt, pin_memory=True)
         self.scal_host = torch.empty(len(REDS), dtype=torch.float64, pin_memory=True)
 
     def step(self, f_host, u_host):
@@ -276,7 +284,7 @@ def measure_e2e(f, u, form, device, steps, world, dev):
 
 
 def cpu_reference_step(f_sample, u_sample):
-    """The reference algorithm (CPU FP64 oracle) on one bounded sample."""
+    """The reference algorithm (CPU FP64 oracle port) on one bounded sample."""
     from oracle import stenpy_oracle as O
     import stenpy_b200 as S
     g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
@@ -285,38 +293,77 @@ def cpu_reference_step(f_sample, u_sample):
     return O.evaluate(g, wanted), wanted
 
 
+class ReferenceStep:
+    """One step of the reference's own CPU eager path on a sample: its
+    ``compile_expression`` + ``Runtime(MemoryManager(), device="cpu").run`` (FP64),
+    imported unmodified from the ``baseline/_ref`` install. Falls back to the
+    oracle port (a restatement of the same path) when the install is absent;
+    ``kind`` says which ran."""
+
+    def __init__(self):
+        try:
+            from oracle.reference_arm import load_engine
+            self.E = load_engine()
+            self.kind = "reference"
+        except ImportError:
+            self.E = None
+            self.kind = "port"
+
+    def __call__(self, f_sample, u_sample):
+        if self.E is None:
+            return cpu_reference_step(f_sample, u_sample)
+        E = self.E
+        g, sink, *_ = E.compile_expression(REF_EXPR, dx=1.0, boundary="periodic",
+                                           field_map={"f": f_sample.double(), "u": u_sample.double()})
+        wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
+        with torch.no_grad():
+            return E.Runtime(E.MemoryManager(), device="cpu").run(g), wanted
+
+    def describe(self, sample: str) -> str:
+        what = ("the reference's compile_expression + Runtime(MemoryManager(), device='cpu').run, FP64"
+                if self.kind == "reference" else "FP64 torch CPU oracle port of the reference path")
+        return f"{sample}: {what}"
+
+
 def sample_planes(size):
     return max(4, min(size, 32))
 
 
-def run_reference(args):
-    """--impl reference: the reference algorithm on the host cores (oracle port)."""
-    world, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
-    if rank != 0:
-        return
-    torch.set_num_threads(os.cpu_count() or 1)
+def time_reference(size, steps, warmup):
+    """Median seconds per step of the reference CPU path on a 32-plane sample of the
+    workload (bounded so that a run ends within minutes), with every host thread."""
     from stenpy_b200.synth import sinusoid_field, smoothed_vector
-    P = sample_planes(args.size)
-    shape = (P, args.size, args.size)
+    torch.set_num_threads(os.cpu_count() or 1)
+    P = sample_planes(size)
+    shape = (P, size, size)
     f = sinusoid_field(shape, seed=0)
     u = smoothed_vector(shape, seed=2)
-    for _ in range(args.warmup):
-        cpu_reference_step(f, u)
+    step = ReferenceStep()
+    for _ in range(warmup):
+        step(f, u)
     ts = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         t = time.perf_counter()
-        cpu_reference_step(f, u)
+        step(f, u)
         ts.append(time.perf_counter() - t)
-    vox = P * args.size * args.size
-    v = vox / statistics.median(ts) / 1e9
-    line = {"metric": "fused-expr throughput (Gvoxel/s)", "value": v, "unit": "Gvoxel/s", "impl": "reference",
+    return statistics.median(ts), P * size * size, step, f"{P}x{size}x{size} planes per step"
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path on the host cores (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sec, vox, step, sample = time_reference(args.size, args.steps, args.warmup)
+    v = vox / sec / 1e9
+    line = {"metric": METRIC, "value": v, "unit": "Gvoxel/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": statistics.median(ts) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{EXPR} + sum/mean/variance, periodic, {args.size}^3 (sample)",
-                       "sample": f"{P}x{args.size}x{args.size} planes per step"},
-            "cpu_baseline": {"value": v, "unit": "Gvoxel/s", "cores": torch.get_num_threads(), "kind": "port",
-                             "sample": f"{P}x{args.size}x{args.size} voxels per step, FP64 torch CPU oracle"},
+            "config": {"workload": f"{REF_EXPR} + sum/mean/variance, periodic, {args.size}^3 (sample)",
+                       "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "Gvoxel/s", "cores": torch.get_num_threads(), "kind": step.kind,
+                             "sample": step.describe(sample)},
             "e2e": {"value": v, "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -332,11 +379,11 @@ def errors_vs_fp64(f, u, device, forms):
     ref32, wanted = cpu_reference_step(fs.cpu(), us.cpu())
     out = {}
     for form in forms:
-        dt = FORM_DT[form]
+        dt, odt = FORMS[form]
         g, sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
                                            field_map={"f": fs.to(dt), "u": us.to(dt)})
         w = [sink] + [g.add(r, (sink,), {}) for r in REDS]
-        res = S.Runtime(device=device, out_dtype=dt).run(g, wanted=w)
+        res = S.Runtime(device=device, out_dtype=odt).run(g, wanted=w)
         y = res[sink].double().cpu()
         refq, wq = cpu_reference_step(fs.to(dt).cpu(), us.to(dt).cpu())
         d = {}
@@ -703,7 +750,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512)
-    ap.add_argument("--forms", default="fp32,fp16,bf16")
+    ap.add_argument("--forms", default="fp32,fp16,bf16,bf16in")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and error sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default schedules instead of autotuned ones")
@@ -782,9 +829,9 @@ def main():
         main_k = [(op, t) for op, t in kt if op.module in [p.module for p in plan.passes]]
         dom_op, dom_ms = max(main_k, key=lambda x: x[1])
         dom_pass = [p for p in plan.passes if p.module == dom_op.module][0]
-        es = FORM_DT[form].itemsize
-        alg = sum(ESZ * nc for ESZ, nc in ((es, f_.nc) for f_ in dom_pass.spec.fields)) * n_vox
-        alg += sum(es * dom_pass.spec.graph.nodes[r.node].nc for r in dom_pass.spec.roots if r.kind == "out") * n_vox
+        es, oes = FORMS[form][0].itemsize, FORMS[form][1].itemsize
+        alg = sum(es * f_.nc for f_ in dom_pass.spec.fields) * n_vox
+        alg += sum(oes * dom_pass.spec.graph.nodes[r.node].nc for r in dom_pass.spec.roots if r.kind == "out") * n_vox
         results[form] = {
             "gvox_s": n_vox * world / (ms * 1e-3) / 1e9, "ms_per_step": ms,
             "step_GBps": ALG_BYTES[form] * n_vox / (ms * 1e-3) / 1e9,
@@ -798,43 +845,47 @@ def main():
         del cg
     head = results[HEADLINE] if HEADLINE in results else results[forms[0]]
     head_form = HEADLINE if HEADLINE in results else forms[0]
-    line = {"metric": "fused-expr throughput (Gvoxel/s), HBM roofline fraction, error vs FP64",
+    errs, sample = ({}, None)
+    if rank == 0 and not args.no_cpu:
+        errs, sample = errors_vs_fp64(f, u, dev, forms)
+    # per-form summary kept inside roofline (short enough for one JSON line)
+    summary = {}
+    for form, r in results.items():
+        e = errs.get(form, {}).get("vs_fp64_of_stored_inputs", {})
+        summary[form] = {"gvox_s": round(r["gvox_s"], 2), "step_frac": round(r["step_frac_of_peak"], 4),
+                         "dom_frac": round(r["dominant"]["frac_of_peak"], 4),
+                         "B_per_voxel": ALG_BYTES[form],
+                         "err": e.get("max_rel"), "scal_err": max(e["scalars_rel"].values()) if e else None}
+    if "fp32" in results:
+        for form in summary:
+            summary[form]["x_fp32"] = round(results[form]["gvox_s"] / results["fp32"]["gvox_s"], 3)
+    line = {"metric": METRIC,
             "value": head["gvox_s"], "unit": "Gvoxel/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "storage": head_form, "data": "synthetic",
-            "config": {"workload": f"{EXPR} + sum/mean/variance of the result, periodic, dx=1, "
-                                   f"{args.size}^3 f and {args.size}^3x3 u",
-                       "global_voxels": n_vox * world, "l2": "inputs (f, u) larger than L2 (126 MB)",
-                       "step": "one CUDA-graph replay of the fused plan (inputs resident in HBM)",
+            "config": {"workload": f"{EXPR} + sum/mean/variance, periodic, dx=1, {args.size}^3 f, "
+                                   f"{args.size}^3x3 u",
+                       "l2": "inputs larger than L2 (126 MB)", "step": "CUDA-graph replay of the fused plan",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "achieved": head["dominant"]["GBps"], "peak": peak, "unit": "GB/s",
-                         "frac": head["dominant"]["GBps"] / peak, "peak_kind": peak_kind,
+            "roofline": {"bound": "hbm", "achieved": round(head["dominant"]["GBps"], 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(head["dominant"]["GBps"] / peak, 4), "peak_kind": peak_kind,
                          "traffic": NCU_TRAFFIC.get((head_form, args.size)),
                          "kernel": "dominant pass of the headline form",
-                         "step_frac": head["step_frac_of_peak"]},
-            "forms": results, "gpu_launches": head["launches_per_step"] * args.steps, "clocks": clocks}
+                         "step_frac": round(head["step_frac_of_peak"], 4), "forms": summary},
+            "gpu_launches": head["launches_per_step"] * args.steps, "clocks": clocks}
     if not args.no_e2e:
         ms, h2d, d2h = measure_e2e(f, u, head_form, dev, args.steps, world, dev)
         line["e2e"] = {"value": n_vox * world / (ms * 1e-3) / 1e9, "unit": "Gvoxel/s",
                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms}
     if rank == 0 and not args.no_cpu:
-        errs, sample = errors_vs_fp64(f, u, dev, forms)
-        line["error_vs_fp64"] = {"sample": sample, **errs}
-        torch.set_num_threads(os.cpu_count() or 1)
-        P = sample_planes(args.size)
-        fs, us = f[:P].cpu(), u[:P].cpu()
-        cpu_reference_step(fs, us)
-        ts = []
-        for _ in range(3):
-            t = time.perf_counter()
-            cpu_reference_step(fs, us)
-            ts.append(time.perf_counter() - t)
-        line["cpu_baseline"] = {"value": P * args.size ** 2 / statistics.median(ts) / 1e9, "unit": "Gvoxel/s",
-                                "cores": torch.get_num_threads(), "kind": "port",
-                                "sample": f"{P}x{args.size}x{args.size} voxels of the workload, FP64 torch CPU "
-                                          "oracle, median of 3 after 1 warm-up"}
+        sec, vox, step, sample_ref = time_reference(args.size, 3, 1)
+        line["cpu_baseline"] = {"value": vox / sec / 1e9, "unit": "Gvoxel/s", "cores": torch.get_num_threads(),
+                                "kind": step.kind, "sample": step.describe(sample_ref) + ", median of 3"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+        # the long form (schedules, per-launch times, every error figure) goes to stderr
+        print("details: " + json.dumps({"forms": results, "error_vs_fp64": {"sample": sample, **errs}}),
+              file=sys.stderr, flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

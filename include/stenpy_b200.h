@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define STENPY_ABI_VERSION 1
+#define STENPY_ABI_VERSION 2
 
 #define STENPY_OK 0
 #define STENPY_E_INVALID (-1)   /* bad argument */
@@ -163,10 +163,20 @@ int stenpy_adam_step(float* params, const float* grad, float* m, float* v, int n
  * (4 MiB, held by every device that loads the library until exit) instead of a
  * caller-allocated buffer. Each launch's packed parameters are copied and the
  * partials pointer at byte offset `part_offset` is replaced by the static
- * array's device address (looked up per device on the first call, which should
- * therefore precede any stream capture). Requests with ncta_total * nslots above
- * the maximum fail with STENPY_E_INVALID. Calls share the array: every partial
- * row is rewritten each call, but calls that overlap on one GPU race. */
+ * array's device address. That address is looked up on the first call on a
+ * device (so make that call before any stream capture) and kept per device and
+ * context: a call from a different context on the device, for example after a
+ * device reset, looks it up again.
+ *
+ * Sizes: a launch writes partial rows cta_off .. cta_off + gx*gy*gz - 1, where
+ * cta_off is the int32 at byte offset `cta_off_offset` of its params, each row
+ * `nslots` doubles wide. `nslots` must equal the row width the kernels were
+ * generated with (the pass's NSLOTS_RED); every launch's rows must lie below
+ * `ncta_total`, and ncta_total * nslots must not exceed the maximum: otherwise
+ * the call fails with STENPY_E_INVALID before launching anything. The stream
+ * must belong to the current device (STENPY_E_INVALID otherwise). Calls share
+ * the array: every partial row is rewritten each call, but calls that overlap
+ * on one GPU race. */
 #define STENPY_NOALLOC_MAX_PARTIALS (1u << 19)
 
 typedef struct StenLaunchDesc {
@@ -174,8 +184,9 @@ typedef struct StenLaunchDesc {
   uint32_t grid[3];
   uint32_t block[3];
   uint32_t dyn_smem;
-  uint32_t part_offset;   /* byte offset of the partials pointer in params */
-  const void* params;     /* packed kernel parameters (<= 8 KiB) */
+  uint32_t part_offset;    /* byte offset of the partials pointer in params (8-aligned) */
+  uint32_t cta_off_offset; /* byte offset of the int32 first partial row in params */
+  const void* params;      /* packed kernel parameters (<= 8 KiB) */
   size_t params_bytes;
 } StenLaunchDesc;
 

@@ -42,8 +42,8 @@ class ReduceDesc(ctypes.Structure):
 
 class LaunchDesc(ctypes.Structure):
     _fields_ = [("module", ctypes.c_void_p), ("grid", ctypes.c_uint32 * 3), ("block", ctypes.c_uint32 * 3),
-                ("dyn_smem", ctypes.c_uint32), ("part_offset", ctypes.c_uint32), ("params", ctypes.c_void_p),
-                ("params_bytes", ctypes.c_size_t)]
+                ("dyn_smem", ctypes.c_uint32), ("part_offset", ctypes.c_uint32),
+                ("cta_off_offset", ctypes.c_uint32), ("params", ctypes.c_void_p), ("params_bytes", ctypes.c_size_t)]
 
 
 NOALLOC_MAX_PARTIALS = 1 << 19
@@ -101,7 +101,7 @@ def lib() -> ctypes.CDLL:
         for name in ABI_SYMBOLS:
             if not hasattr(L, name):
                 raise NativeUnavailable(f"{LIB_PATH} lacks {name}; rebuild it")
-        if L.stenpy_abi_version() != 1:
+        if L.stenpy_abi_version() != 2:
             raise NativeUnavailable("libstenpy_b200.so ABI version mismatch; rebuild it")
         _lib = L
         return L
@@ -210,10 +210,11 @@ def pass_noalloc(launches, ncta_total: int, nslots: int, descs: Sequence[ReduceD
                  stream: int) -> None:
     """Run one fused reduction pass with the library's static partials array (no
     device allocation). ``launches``: (module, grid, block, dyn_smem, params bytes,
-    byte offset of the partials pointer in params)."""
+    byte offset of the partials pointer in params, byte offset of the int32
+    ``cta_off`` (first partial row) in params)."""
     keep = []
     arr = (LaunchDesc * len(launches))()
-    for d, (module, grid, block, smem, params, part_offset) in zip(arr, launches):
+    for d, (module, grid, block, smem, params, part_offset, cta_off_offset) in zip(arr, launches):
         buf = ctypes.create_string_buffer(params, len(params))
         keep.append(buf)
         d.module = module
@@ -221,6 +222,7 @@ def pass_noalloc(launches, ncta_total: int, nslots: int, descs: Sequence[ReduceD
         d.block[:] = list(block)
         d.dyn_smem = smem
         d.part_offset = part_offset
+        d.cta_off_offset = cta_off_offset
         d.params = ctypes.cast(buf, ctypes.c_void_p)
         d.params_bytes = len(params)
     rd = (ReduceDesc * len(descs))(*descs)

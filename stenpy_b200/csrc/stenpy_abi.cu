@@ -132,6 +132,18 @@ extern "C" {
 // Lets other translation units of the library report errors through stenpy_last_error.
 void sten_internal_set_error(const char* msg) { g_last_error = msg ? msg : ""; }
 
+// The context launches go to (the caller's current one, else the primary context of
+// the runtime's current device, made current), for per-context caches elsewhere.
+int sten_internal_current_context(void** out) {
+  int rc = ensure_context();
+  if (rc) return rc;
+  CUcontext c = nullptr;
+  CUresult r = g_drv.CtxGetCurrent(&c);
+  if (r != CUDA_SUCCESS) return drv_fail(r, "cuCtxGetCurrent");
+  *out = (void*)c;
+  return STENPY_OK;
+}
+
 int stenpy_abi_version(void) { return STENPY_ABI_VERSION; }
 
 const char* stenpy_last_error(void) { return g_last_error.c_str(); }
@@ -437,7 +449,15 @@ extern "C" int stenpy_finalize(const double* partials, int ncta, int nslots, con
   FinalizeArgs a;
   memset(&a, 0, sizeof a);
   for (int i = 0; i < nred; ++i) {
-    if (descs[i].slot < 0 || descs[i].slot >= nslots) return fail(STENPY_E_INVALID, "finalize: slot out of range");
+    // every slot the kernel folds for this kind must lie inside the row
+    const int k = descs[i].kind;
+    if (k < STENPY_RED_SUM || k > STENPY_RED_CORRELATION) return fail(STENPY_E_INVALID, "finalize: kind %d", k);
+    const int width = k == STENPY_RED_VARIANCE ? 3
+                    : (k == STENPY_RED_ENTROPY || k == STENPY_RED_MIN_MAX) ? 2
+                    : (k == STENPY_RED_COVARIANCE || k == STENPY_RED_CORRELATION) ? 6 : 1;
+    if (descs[i].slot < 0 || descs[i].slot + width > nslots)
+      return fail(STENPY_E_INVALID, "finalize: slots %d..%d of kind %d outside rows of %d", descs[i].slot,
+                  descs[i].slot + width - 1, k, nslots);
     a.d[i] = descs[i];
   }
   sten_finalize_kernel<<<nred, 256, 0, (cudaStream_t)stream>>>(partials, ncta, nslots, a, scalars);

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in declared if not hasattr(lib, s)]
     assert not missing, missing
     assert set(N.ABI_SYMBOLS) <= set(declared)
-    assert lib.stenpy_abi_version() == 1
+    assert lib.stenpy_abi_version() == 2
 
 
 def test_abi_rejects_bad_arguments_without_gpu():
@@ -42,6 +42,61 @@ def test_abi_rejects_bad_arguments_without_gpu():
     assert L.stenpy_encode_tmap_3d(buf, 4, ctypes.c_void_p(256), 64, 8, 8, 100, 2048, 72, 10, 1) == -1
     assert L.stenpy_encode_tmap_3d(buf, 4, ctypes.c_void_p(256), 64, 8, 8, 256, 2048, 300, 10, 1) == -1
     assert L.stenpy_finalize(None, 1, 1, None, 1, None, None) == -1
+
+
+def test_finalize_rejects_reductions_wider_than_the_row():
+    """A variance reads 3 slots, entropy/min_max 2, covariance 6: a descriptor whose
+    slots run past the row is refused before anything is launched."""
+    L = N.lib()
+    fake = ctypes.c_void_p(4096)
+    for kind, width in ((N.RED_VARIANCE, 3), (N.RED_ENTROPY, 2), (N.RED_MIN_MAX, 2), (N.RED_COVARIANCE, 6),
+                        (N.RED_SUM, 1)):
+        d = (N.ReduceDesc * 1)(N.ReduceDesc(kind, 8 - width + 1, 0, 0, 1.0, 0.0))
+        assert L.stenpy_finalize(fake, 4, 8, d, 1, fake, None) == -1, kind
+        assert b"outside rows" in L.stenpy_last_error()
+    d = (N.ReduceDesc * 1)(N.ReduceDesc(99, 0, 0, 0, 1.0, 0.0))
+    assert L.stenpy_finalize(fake, 4, 8, d, 1, fake, None) == -1
+
+
+def _noalloc_desc(grid, cta_off, nbytes=64, part_offset=0, cta_off_offset=8):
+    params = bytearray(nbytes)
+    params[cta_off_offset:cta_off_offset + 4] = int(cta_off).to_bytes(4, "little", signed=True)
+    buf = ctypes.create_string_buffer(bytes(params), nbytes)
+    d = N.LaunchDesc()
+    d.module = None
+    d.grid[:] = list(grid)
+    d.block[:] = [128, 1, 1]
+    d.dyn_smem = 0
+    d.part_offset = part_offset
+    d.cta_off_offset = cta_off_offset
+    d.params = ctypes.cast(buf, ctypes.c_void_p)
+    d.params_bytes = nbytes
+    return d, buf
+
+
+@pytest.mark.parametrize("grid,cta_off,ncta,nslots,msg", [
+    ((4, 2, 1), 0, 7, 4, b"exceed ncta_total"),           # 8 rows written, 7 declared
+    ((4, 1, 1), 5, 8, 4, b"exceed ncta_total"),           # rows 5..8 of 8
+    ((4, 1, 1), -1, 8, 4, b"exceed ncta_total"),          # negative first row
+    ((1, 1, 1), 0, N.NOALLOC_MAX_PARTIALS // 4 + 1, 4, b"static scratch"),
+])
+def test_noalloc_rejects_rows_outside_the_static_array(grid, cta_off, ncta, nslots, msg):
+    """stenpy_pass_noalloc checks the rows each launch writes (its cta_off, read
+    from the packed parameters, plus its grid size) against the declared partials
+    before it touches the GPU."""
+    L = N.lib()
+    d, keep = _noalloc_desc(grid, cta_off)
+    rd = (N.ReduceDesc * 1)(N.ReduceDesc(N.RED_SUM, 0, 0, 0, 1.0, 0.0))
+    arr = (N.LaunchDesc * 1)(d)
+    rc = L.stenpy_pass_noalloc(arr, 1, ncta, nslots, rd, 1, ctypes.c_void_p(4096), None)
+    assert rc == -1
+    assert msg in L.stenpy_last_error()
+    # a misplaced cta_off field (past the parameter block) is refused too
+    d2, keep2 = _noalloc_desc((1, 1, 1), 0, cta_off_offset=8)
+    d2.cta_off_offset = 62
+    arr2 = (N.LaunchDesc * 1)(d2)
+    assert L.stenpy_pass_noalloc(arr2, 1, 4, 4, rd, 1, ctypes.c_void_p(4096), None) == -1
+    assert b"bad parameter block" in L.stenpy_last_error()
 
 
 def test_front_end_graph_semantics():

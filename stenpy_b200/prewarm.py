@@ -16,7 +16,9 @@ from typing import Iterable, List, Optional, Sequence
 import torch
 
 EXPR_FIELDS = "divergence(gradient(f)) + l2norm(curl(u))"
-FORM_DT = {"fp32": torch.float32, "fp16": torch.float16, "bf16": torch.bfloat16}
+# storage form -> (field dtype, result dtype)
+FORMS = {"fp32": (torch.float32, torch.float32), "fp16": (torch.float16, torch.float16),
+         "bf16": (torch.bfloat16, torch.bfloat16), "bf16in": (torch.bfloat16, torch.float32)}
 
 
 def _placeholder(shape: Sequence[int], dtype: torch.dtype) -> torch.Tensor:
@@ -38,17 +40,17 @@ def plan_sources(graph, wanted, out_dtype=torch.float32, cfg=None, candidates: b
     return out
 
 
-def sources_fields(size: int = 512, forms: Iterable[str] = ("fp32", "fp16", "bf16")) -> List[str]:
+def sources_fields(size: int = 512, forms: Iterable[str] = tuple(FORMS)) -> List[str]:
     """The 512^3 fused step (default schedule and every tuning candidate), per form."""
     from . import compile_expression
     out = []
     for form in forms:
-        dt = FORM_DT[form]
+        dt, odt = FORMS[form]
         g, sink, *_ = compile_expression(EXPR_FIELDS, dx=1.0, boundary="periodic",
                                          field_map={"f": _placeholder((size,) * 3, dt),
                                                     "u": _placeholder((size,) * 3 + (3,), dt)})
         wanted = [sink] + [g.add(r, (sink,), {}) for r in ("sum", "mean", "variance")]
-        out += plan_sources(g, wanted, dt, candidates=True)
+        out += plan_sources(g, wanted, odt, candidates=True)
     return out
 
 

@@ -944,14 +944,14 @@ __device__ __forceinline__ double sten_simpson_w(int idx, int n, double h, int s
 
 
 def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootSpec] = (),
-              where: str = "main", m: int = 0, kk: int = 0, plane32: bool = False) -> List[str]:
+              where: str = "main", m: int = 0, kk: int = 0, hoisted: bool = False) -> List[str]:
     """Per-voxel root handling (stores, reduction accumulation, scans). Expects
     ``rv`` (root values), ``vox`` (linear voxel index), ``gi, j, k`` and, for scans,
     the register slot ``mq``. Roots in ``skip`` are stored by the caller. With
-    ``plane32`` the reductions of ``plane32_roots`` accumulate into the plane's FP32
-    partials (``_plane32_open`` / ``_plane32_close``)."""
+    ``hoisted`` the variance pivots and counts are kept per plane
+    (``_var_plane_open`` / ``_var_plane_close``)."""
     K: List[str] = []
-    p32 = {id(r) for _, r in plane32_roots(spec)} if plane32 else set()
+    hv = {id(r) for _, r in hoisted_var_roots(spec)} if hoisted else set()
     ri = si = 0
     for r, off in zip(spec.roots, e.offsets):  # noqa: C901
         nc = e.g.nodes[r.node].nc
@@ -988,16 +988,10 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
             ri += 1
             if r.red == "sum" and _sum_from_var(spec, r) is not None:
                 continue  # derived from the variance accumulator of the same value
-            if id(r) in p32:
+            if id(r) in hv:
                 for c in range(nc):
-                    v = f"rv[{off + c}]"
-                    if r.red == "var":
-                        K.append(f"{{ const float d_ = {v} - rv{ri_here}_p32; pp{ri_here}_s1 += d_;"
-                                 f" pp{ri_here}_s2 = fmaf(d_, d_, pp{ri_here}_s2); }}")
-                    elif r.red == "sumsq":
-                        K.append(f"pp{ri_here}_a = fmaf({v}, {v}, pp{ri_here}_a);")
-                    else:
-                        K.append(f"pp{ri_here}_a += {v};")
+                    K.append(f"{{ const double d_ = (double)rv[{off + c}] - rv{ri_here}_piv; rv{ri_here}_s1 += d_;"
+                             f" rv{ri_here}_s2 = fma(d_, d_, rv{ri_here}_s2); }}")
                 continue
             if r.red == "cov":
                 h = f"rv{ri_here}"
@@ -1063,54 +1057,34 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
     return [k.replace("{M}", str(m)).replace("{KK}", str(kk)) for k in K]
 
 
-def plane32_roots(spec: PassSpec) -> List[Tuple[int, RootSpec]]:
-    """Reduction roots (index among reductions, root) whose per-voxel accumulation
-    in the z-march is done in FP32 over one plane of a thread's voxels and added to
-    the FP64 accumulators once per plane: sums, sums of squares and variances of
-    COMPUTED values. Each such value already carries FP32 rounding, so a 16-term FP32
-    partial adds an error of the same order per voxel, random in sign. Reductions of
-    stored field values (exact in FP32) keep FP64 accumulation per voxel."""
-    out = []
-    for ri, r in enumerate([x for x in spec.roots if x.kind == "red"]):
-        if r.red not in ("sum", "sumsq", "var") or spec.graph.nodes[r.node].op == "field":
-            continue
-        if r.red == "sum" and _sum_from_var(spec, r) is not None:
-            continue
-        out.append((ri, r))
-    return out
+def hoisted_var_roots(spec: PassSpec) -> List[Tuple[int, RootSpec]]:
+    """Variance roots (index among reductions, root). In the z-march the pivot of a
+    thread's pivot-shifted sums is taken once, from the first valid voxel of the
+    first plane that has one, and the count grows by the plane's valid voxels, so
+    a voxel adds only d = x - pivot, d and d^2 (FP64). The voxel order and every
+    operation are those of the per-voxel form, so the sums are the same bit for bit."""
+    return [(ri, r) for ri, r in enumerate([x for x in spec.roots if x.kind == "red"]) if r.red == "var"]
 
 
-def _plane32_open(spec: PassSpec, e: "_Emitter") -> List[str]:
-    """Per-plane FP32 partials (declared before a plane's voxels) and, for variances,
-    the thread's pivot: the first valid voxel value of its first plane."""
+def _var_plane_open(spec: PassSpec, e: "_Emitter") -> List[str]:
+    """Before a plane's voxels: the thread's pivot, if it has none yet."""
     K: List[str] = []
-    for ri, r in plane32_roots(spec):
-        if r.red == "var":
-            off = e.offsets[spec.roots.index(r)]
-            K.append(f"float pp{ri}_s1 = 0.0f, pp{ri}_s2 = 0.0f;")
-            K.append(f"if (!rv{ri}_h) {{")
-            K.append("  #pragma unroll")
-            K.append("  for (int m = 0; m < VPT; ++m) {")
-            K.append("    #pragma unroll")
-            K.append("    for (int q = 0; q < KV; ++q) "
-                     f"if (!rv{ri}_h && m_ok[m] && k_ok[q]) {{ rv{ri}_p32 = rvk[m][q][{off}]; rv{ri}_h = true; }}")
-            K.append("  }")
-            K.append("}")
-        else:
-            K.append(f"float pp{ri}_a = 0.0f;")
+    for ri, r in hoisted_var_roots(spec):
+        off = e.offsets[spec.roots.index(r)]
+        K.append(f"if (!rv{ri}_h) {{")
+        K.append("  #pragma unroll")
+        K.append("  for (int m = 0; m < VPT; ++m) {")
+        K.append("    #pragma unroll")
+        K.append("    for (int q = 0; q < KV; ++q) "
+                 f"if (!rv{ri}_h && m_ok[m] && k_ok[q]) {{ rv{ri}_piv = (double)rvk[m][q][{off}]; rv{ri}_h = true; }}")
+        K.append("  }")
+        K.append("}")
     return K
 
 
-def _plane32_close(spec: PassSpec, e: "_Emitter") -> List[str]:
-    """Add this plane's FP32 partials to the FP64 accumulators."""
-    K: List[str] = []
-    for ri, r in plane32_roots(spec):
-        nc = e.g.nodes[r.node].nc
-        if r.red == "var":
-            K.append(f"rv{ri}_s1 += (double)pp{ri}_s1; rv{ri}_s2 += (double)pp{ri}_s2; rv{ri}_n += {nc}u * nvalid_;")
-        else:
-            K.append(f"rv{ri}_a += (double)pp{ri}_a;")
-    return K
+def _var_plane_close(spec: PassSpec, e: "_Emitter") -> List[str]:
+    """After a plane's voxels: its valid voxels join the count."""
+    return [f"rv{ri}_n += {e.g.nodes[r.node].nc}u * nvalid_;" for ri, r in hoisted_var_roots(spec)]
 
 
 def hist_offsets(spec: PassSpec, red_off: int) -> Tuple[Dict[int, int], int]:
@@ -1148,7 +1122,6 @@ def _red_decls(spec: PassSpec, where: str = "main") -> List[str]:
                 K.append(f"unsigned long long* rv{ri}_hs = p.hist + {r.slot};")
         elif r.red == "var":
             K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
-            K.append(f"float rv{ri}_p32 = 0.0f;")
         elif r.red == "cov":
             # pivot-shifted sums of the pairs (a, b): n, Σda, Σdb, Σda·db, Σda², Σdb²
             K.append(f"double rv{ri}_pa = 0.0, rv{ri}_pb = 0.0, rv{ri}_sa = 0.0, rv{ri}_sb = 0.0, rv{ri}_sab = 0.0, "
@@ -2032,7 +2005,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             for m in range(vpt):
                 for kk in range(kvn):
                     K.append(f"    eval_fast<{m}, {kk}>(x, rvk[{m}][{kk}]);")
-            K += ["    " + k for k in _plane32_open(spec, e)]
+            K += ["    " + k for k in _var_plane_open(spec, e)]
         for m in range(vpt):
             K.append(f"    if (m_ok[{m}]) {{")
             K.append(f"      const int j = tj0 + tjb + {m};")
@@ -2055,7 +2028,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                         K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
                         K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
                 K += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk,
-                                                     plane32=eager)]
+                                                     hoisted=eager)]
                 K.append("      }")
             for r in vec_outs:
                 ct = CTYPE[r.out_dtype]
@@ -2070,7 +2043,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K.append("      }")
             K.append("    }")
         if eager:
-            K += ["    " + k for k in _plane32_close(spec, e)]
+            K += ["    " + k for k in _var_plane_close(spec, e)]
         if split:
             K.append("    }")
         for r in spec.roots:
@@ -2116,10 +2089,6 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
         K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
                  % (" false" if batch else ""))
-        if eager:
-            for ri, r in plane32_roots(spec):
-                if r.red == "var":
-                    K.append(f"  rv{ri}_piv = (double)rv{ri}_p32;")
         K += ["  " + k for k in _red_flush(spec, "cta")]
         if batch:
             if async_lsu:

@@ -66,6 +66,14 @@ STEN_DEV void st_from_f64(f16_t* p, double v) { st_from_f32(p, (float)v); }
 template <typename T> struct is_bf16_t { static constexpr bool value = false; };
 template <> struct is_bf16_t<bf16_t> { static constexpr bool value = true; };
 STEN_DEV float f16_bits_to_f32(u16 b) { float f; asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(b)); return f; }
+// The low / high FP16 half of a 32-bit word as FP32: the halves are named as the
+// word's register pair (no shift or mask), so the conversion reads the half directly.
+STEN_DEV float f16_lo_to_f32(u32 w) {
+  float f; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; cvt.f32.f16 %0, l_; }" : "=f"(f) : "r"(w)); return f;
+}
+STEN_DEV float f16_hi_to_f32(u32 w) {
+  float f; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; cvt.f32.f16 %0, h_; }" : "=f"(f) : "r"(w)); return f;
+}
 template <typename T, int CW, int B>
 STEN_DEV float chunk_elem(const unsigned char* row) {
   u32 w;
@@ -81,10 +89,10 @@ STEN_DEV float chunk_elem(const unsigned char* row) {
   }
   if constexpr (sizeof(T) == 4) {
     return __uint_as_float(w);
+  } else if constexpr (is_bf16_t<T>::value) {
+    return __uint_as_float((B % 4) ? (w & 0xffff0000u) : (w << 16));
   } else {
-    const u32 h = (B % 4) ? (w >> 16) : (w & 0xffffu);
-    if constexpr (is_bf16_t<T>::value) return __uint_as_float(h << 16);
-    else return f16_bits_to_f32((u16)h);
+    return (B % 4) ? f16_hi_to_f32(w) : f16_lo_to_f32(w);
   }
 }
 // N consecutive elements from global memory (read-only path) as floats: one 16/8/4-byte
@@ -95,7 +103,7 @@ STEN_DEV void unpack_f32(u32 w, const bf16_t*, float* o) {
   o[0] = __uint_as_float(w << 16); o[1] = __uint_as_float(w & 0xffff0000u);
 }
 STEN_DEV void unpack_f32(u32 w, const f16_t*, float* o) {
-  o[0] = f16_bits_to_f32((u16)(w & 0xffffu)); o[1] = f16_bits_to_f32((u16)(w >> 16));
+  o[0] = f16_lo_to_f32(w); o[1] = f16_hi_to_f32(w);
 }
 template <typename T, int N>
 STEN_DEV void ld_vec_f32(const T* p, float* out) {
@@ -461,13 +469,14 @@ STEN_DEV float m_cos(float x) { return cosf(x); }
 STEN_DEV double m_cos(double x) { return cos(x); }
 // Ascending eigenvalues of the symmetric matrix whose lower triangle is
 // (a00; a10 a11; a20 a21 a22), trigonometric closed form.
+// Returns r = det((A - qI)/p)/2 = cos(3 phi), clamped to [-1, 1] (1 for a multiple of I).
 template <typename T>
-STEN_DEV void eig3_trig(T a00, T a10, T a11, T a20, T a21, T a22, T* w) {
+STEN_DEV T eig3_trig(T a00, T a10, T a11, T a20, T a21, T a22, T* w) {
   const T p1 = a10 * a10 + a20 * a20 + a21 * a21;
   const T q = (a00 + a11 + a22) / T(3);
   const T b00 = a00 - q, b11 = a11 - q, b22 = a22 - q;
   const T p2 = b00 * b00 + b11 * b11 + b22 * b22 + T(2) * p1;
-  if (p2 <= T(0)) { w[0] = q; w[1] = q; w[2] = q; return; }
+  if (p2 <= T(0)) { w[0] = q; w[1] = q; w[2] = q; return T(1); }
   const T p = m_sqrt(p2 / T(6));
   const T ip = T(1) / p;
   const T c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip;
@@ -481,9 +490,14 @@ STEN_DEV void eig3_trig(T a00, T a10, T a11, T a20, T a21, T a22, T* w) {
   const T e_lo = q + T(2) * p * m_cos(phi + two_pi_3);
   const T e_mid = T(3) * q - e_hi - e_lo;
   w[0] = e_lo; w[1] = e_mid; w[2] = e_hi;
+  return r;
 }
-// fp32 evaluation; when the spectrum spread p is below 1e-3 of the matrix scale the
-// fp32 shift A - qI loses digits, so the eigenvalues are re-evaluated in fp64.
+// fp32 evaluation, re-evaluated in fp64 in two cases: (a) the spectrum spread p is
+// below 1e-3 of the matrix scale (the fp32 shift A - qI loses digits); (b) two
+// eigenvalues nearly coincide, |r| > 0.999: acos amplifies the fp32 rounding of r
+// (a few units of 2^-24) by 1/sqrt(1 - r^2), and at |r| = 0.999 the eigenvalue error
+// stays near 1e-6 of the scale (checked against LAPACK on smooth fields, where a few
+// percent of voxels take the fp64 path).
 STEN_DEV void eig3_sym(const float* m, float* w) {
   const float a00 = m[0], a10 = m[3], a11 = m[4], a20 = m[6], a21 = m[7], a22 = m[8];
   const float scale = fmaxf(fmaxf(fabsf(a00), fabsf(a11)), fmaxf(fabsf(a22),
@@ -491,9 +505,9 @@ STEN_DEV void eig3_sym(const float* m, float* w) {
   const float q = (a00 + a11 + a22) * (1.0f / 3.0f);
   const float p2 = (a00 - q) * (a00 - q) + (a11 - q) * (a11 - q) + (a22 - q) * (a22 - q)
                  + 2.0f * (a10 * a10 + a20 * a20 + a21 * a21);
-  if (p2 > 1e-6f * scale * scale) {
-    eig3_trig<float>(a00, a10, a11, a20, a21, a22, w);
-  } else {
+  float r = 1.0f;
+  if (p2 > 1e-6f * scale * scale) r = eig3_trig<float>(a00, a10, a11, a20, a21, a22, w);
+  if (fabsf(r) > 0.999f) {
     double wd[3];
     eig3_trig<double>((double)a00, (double)a10, (double)a11, (double)a20, (double)a21, (double)a22, wd);
     w[0] = (float)wd[0]; w[1] = (float)wd[1]; w[2] = (float)wd[2];

@@ -44,18 +44,60 @@ class Chunk:
     hi: int         # one past the last slab plane (may exceed n0 when wrapped)
 
 
+def chunk_bounds(s: int, e: int, n0: int, halo: int, periodic: bool) -> Chunk:
+    """Slab [lo, hi) that output planes [s, e) read: ``halo`` planes either side,
+    wrapped for periodic runs, clipped to the field otherwise."""
+    if periodic:
+        lo, hi = s - halo, e + halo
+        if hi - lo > n0:           # slab would cover the whole ring twice: take it all
+            lo, hi = s - halo, s - halo + n0
+    else:
+        lo, hi = max(0, s - halo), min(n0, e + halo)
+    return Chunk(s, e, lo, hi)
+
+
 def plan_chunks(n0: int, chunk: int, halo: int, periodic: bool) -> List[Chunk]:
-    out = []
-    for s in range(0, n0, chunk):
-        e = min(n0, s + chunk)
-        if periodic:
-            lo, hi = s - halo, e + halo
-            if hi - lo > n0:           # slab would cover the whole ring twice: take it all
-                lo, hi = s - halo, s - halo + n0
-        else:
-            lo, hi = max(0, s - halo), min(n0, e + halo)
-        out.append(Chunk(s, e, lo, hi))
-    return out
+    return [chunk_bounds(s, min(n0, s + chunk), n0, halo, periodic) for s in range(0, n0, chunk)]
+
+
+def chunk_launches(pp: FC.PassPlan, c: Chunk, shape: Tuple[int, int, int], fptrs: Sequence[int],
+                   optrs: Sequence[int], table_ptr: int, err_ptr: int, part_ptr: int, cta_off: int
+                   ) -> Tuple[FC.Launch, Optional[FC.Launch], int]:
+    """The main (z-march) launch and the shell launch (or None) that compute output
+    planes [c.s, c.e) of pass ``pp`` from a device slab holding planes [c.lo, c.hi)
+    (field pointers ``fptrs``) into outputs holding planes [c.s, c.e) (``optrs``).
+    The kernels keep global coordinates (``i_base`` = c.lo, ``n0g`` = the field's
+    planes), so every voxel is computed exactly as in a whole-field run. Partial rows
+    start at ``cta_off``; returns the launches and the number of rows they write."""
+    n0, n1, n2 = shape
+    spec = pp.spec
+    cfg = spec.cfg
+    n_out = c.e - c.s
+    gx, gy = pass_grid(spec, n1, n2, n_out)
+    grid = (gx, gy, 1)
+    nl = c.hi - c.lo
+    tmaps = FC.encode_tmaps(spec, list(fptrs), nl, n1, n2)
+    vals = dict(fld=list(fptrs), out=list(optrs), scal=table_ptr, part=part_ptr, hist=0, err=err_ptr, n0g=n0,
+                n1=n1, n2=n2, nl=nl, i_base=c.lo, out_lo=c.s - c.lo, n_out=n_out, seg_len=cfg.seg_len,
+                tiles_k=-(-n2 // cfg.tk), cta_off=cta_off)
+    ncta = grid[0] * grid[1]
+    n_shell = shell_count(shape, spec.radius, c.s, c.e, shell_regions(spec)) if FC.has_shell(spec) else 0
+    sh = -(-n_shell // SHELL_THREADS)
+    main = FC.Launch(pp.module, grid, (cfg.threads, 1, 1), pp.smem, FC.pack_params(spec, vals, tmaps))
+    shell = None
+    if sh:
+        shell = FC.Launch(pp.shell_module, (sh, 1, 1), (SHELL_THREADS, 1, 1), 0,
+                          FC.pack_params(spec, dict(vals, cta_off=cta_off + ncta), tmaps))
+    return main, shell, ncta + sh
+
+
+def chunk_rows(pp: FC.PassPlan, c: Chunk, shape: Tuple[int, int, int]) -> int:
+    """Partial rows ``chunk_launches`` writes for chunk ``c`` (no device work)."""
+    n0, n1, n2 = shape
+    spec = pp.spec
+    gx, gy = pass_grid(spec, n1, n2, c.e - c.s)
+    n_shell = shell_count(shape, spec.radius, c.s, c.e, shell_regions(spec)) if FC.has_shell(spec) else 0
+    return gx * gy + -(-n_shell // SHELL_THREADS)
 
 
 def slab_pieces(c: Chunk, n0: int) -> List[Tuple[int, int, int]]:
@@ -180,38 +222,17 @@ class LazyPipeline:
                     host = torch.empty((self.n0, self.n1, self.n2) + comp, dtype=dt, pin_memory=True)
                 self.host_out[nid] = host
                 outs.append([torch.empty((C, self.n1, self.n2) + comp, dtype=dt, device=dev) for _ in range(2)])
-            tiles_k = -(-self.n2 // cfg.tk)
-            tiles_j = -(-self.n1 // cfg.tj)
-            split = FC.has_shell(spec)
-            launches = []
+            total_rows = sum(chunk_rows(pp, c, plan.shape) for c in chunks)
+            part = torch.zeros(max(total_rows * spec.nslots, 1), dtype=torch.float64, device=dev)
+            packed = []
             cta_off = 0
             for ci, c in enumerate(chunks):
                 b = ci % 2
-                n_out = c.e - c.s
-                gx, gy = pass_grid(spec, self.n1, self.n2, n_out)
-                grid = (gx, gy, 1)
-                nl = c.hi - c.lo
-                fptrs = [bufs[b].data_ptr() for bufs in slabs]
-                tmaps = FC.encode_tmaps(spec, fptrs, nl, self.n1, self.n2)
-                vals = dict(fld=fptrs, out=[o[b].data_ptr() for o in outs], scal=self.table.data_ptr(), part=0,
-                            hist=0, err=self.err.data_ptr(), n0g=self.n0, n1=self.n1, n2=self.n2, nl=nl,
-                            i_base=c.lo, out_lo=c.s - c.lo, n_out=n_out, seg_len=cfg.seg_len,
-                            tiles_k=tiles_k, cta_off=cta_off)
-                ncta = grid[0] * grid[1]
-                n_shell = shell_count(plan.shape, spec.radius, c.s, c.e, shell_regions(spec)) if split else 0
-                sh = -(-n_shell // SHELL_THREADS)
-                launches.append((c, b, grid, vals, tmaps, cta_off, ncta, sh))
-                cta_off += ncta + sh
-            part = torch.zeros(max(cta_off * spec.nslots, 1), dtype=torch.float64, device=dev)
-            packed = []
-            for c, b, grid, vals, tmaps, off, ncta, sh in launches:
-                vals = dict(vals, part=part.data_ptr())
-                main = FC.Launch(pp.module, grid, (cfg.threads, 1, 1), pp.smem, FC.pack_params(spec, vals, tmaps))
-                shell = None
-                if sh:
-                    shell = FC.Launch(pp.shell_module, (sh, 1, 1), (SHELL_THREADS, 1, 1), 0,
-                                      FC.pack_params(spec, dict(vals, cta_off=off + ncta), tmaps))
+                main, shell, rows = chunk_launches(pp, c, plan.shape, [bufs[b].data_ptr() for bufs in slabs],
+                                                   [o[b].data_ptr() for o in outs], self.table.data_ptr(),
+                                                   self.err.data_ptr(), part.data_ptr(), cta_off)
                 packed.append((c, b, main, shell))
+                cta_off += rows
             descs = [N.ReduceDesc(r.kind, r.slot, r.table_index, r.unbiased, r.count, r.eps) for r in pp.reductions]
             self.passes.append(dict(pp=pp, chunks=chunks, C=C, H=H, slabs=slabs, outs=outs, launches=packed,
                                     part=part, ncta_total=cta_off, descs=descs))

@@ -828,10 +828,16 @@ def main():
         kt = kernel_times(prog, stream)
         main_k = [(op, t) for op, t in kt if op.module in [p.module for p in plan.passes]]
         dom_op, dom_ms = max(main_k, key=lambda x: x[1])
-        dom_pass = [p for p in plan.passes if p.module == dom_op.module][0]
         es, oes = FORMS[form][0].itemsize, FORMS[form][1].itemsize
-        alg = sum(es * f_.nc for f_ in dom_pass.spec.fields) * n_vox
-        alg += sum(oes * dom_pass.spec.graph.nodes[r.node].nc for r in dom_pass.spec.roots if r.kind == "out") * n_vox
+
+        def pass_bytes(pp_):
+            b = sum(es * f_.nc for f_ in pp_.spec.fields) * n_vox
+            return b + sum(oes * pp_.spec.graph.nodes[r.node].nc for r in pp_.spec.roots if r.kind == "out") * n_vox
+        dom_pass = [p for p in plan.passes if p.module == dom_op.module][0]
+        alg = pass_bytes(dom_pass)
+        # every z-march pass: algorithmic bytes / its own launch time / peak, in plan order
+        pass_frac = [round(pass_bytes(pp_) / (t * 1e-3) / 1e9 / peak, 4)
+                     for pp_ in plan.passes for op, t in main_k if op.module == pp_.module]
         results[form] = {
             "gvox_s": n_vox * world / (ms * 1e-3) / 1e9, "ms_per_step": ms,
             "step_GBps": ALG_BYTES[form] * n_vox / (ms * 1e-3) / 1e9,
@@ -841,6 +847,7 @@ def main():
             "kernels_ms": [round(t, 4) for _, t in kt],
             "dominant": {"ms": dom_ms, "alg_bytes": alg, "GBps": alg / (dom_ms * 1e-3) / 1e9,
                          "frac_of_peak": alg / (dom_ms * 1e-3) / 1e9 / peak},
+            "pass_frac": pass_frac,
         }
         del cg
     head = results[HEADLINE] if HEADLINE in results else results[forms[0]]
@@ -853,7 +860,7 @@ def main():
     for form, r in results.items():
         e = errs.get(form, {}).get("vs_fp64_of_stored_inputs", {})
         summary[form] = {"gvox_s": round(r["gvox_s"], 2), "step_frac": round(r["step_frac_of_peak"], 4),
-                         "dom_frac": round(r["dominant"]["frac_of_peak"], 4),
+                         "dom_frac": round(r["dominant"]["frac_of_peak"], 4), "pass_frac": r["pass_frac"],
                          "B_per_voxel": ALG_BYTES[form],
                          "err": e.get("max_rel"), "scal_err": max(e["scalars_rel"].values()) if e else None}
     if "fp32" in results:

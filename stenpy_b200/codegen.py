@@ -861,7 +861,7 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
     """(total bytes, byte offset of each staged field's ring, offset of the
     block-reduction scratch). Ring slots are 128-byte aligned (TMA destinations)."""
     nslot = 2 * spec.radius + 1 + spec.cfg.prefetch
-    off = 128  # mbarriers: up to 16 slots
+    off = 256  # mbarriers: up to 16 slots "full" (TMA done), then 16 "empty" (warps done)
     rings: Dict[int, int] = {}
     for f in spec.fields:
         if f.staged:
@@ -944,14 +944,14 @@ __device__ __forceinline__ double sten_simpson_w(int idx, int n, double h, int s
 
 
 def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootSpec] = (),
-              where: str = "main", m: int = 0, kk: int = 0, hoisted: bool = False) -> List[str]:
+              where: str = "main", m: int = 0, kk: int = 0, plane: bool = False) -> List[str]:
     """Per-voxel root handling (stores, reduction accumulation, scans). Expects
     ``rv`` (root values), ``vox`` (linear voxel index), ``gi, j, k`` and, for scans,
     the register slot ``mq``. Roots in ``skip`` are stored by the caller. With
-    ``hoisted`` the variance pivots and counts are kept per plane
-    (``_var_plane_open`` / ``_var_plane_close``)."""
+    ``plane`` the roots of ``plane_roots`` accumulate per plane (``_plane_open`` /
+    ``_plane_close``)."""
     K: List[str] = []
-    hv = {id(r) for _, r in hoisted_var_roots(spec)} if hoisted else set()
+    pr = {id(r) for _, r in plane_roots(spec)} if plane else set()
     ri = si = 0
     for r, off in zip(spec.roots, e.offsets):  # noqa: C901
         nc = e.g.nodes[r.node].nc
@@ -988,10 +988,19 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
             ri += 1
             if r.red == "sum" and _sum_from_var(spec, r) is not None:
                 continue  # derived from the variance accumulator of the same value
-            if id(r) in hv:
+            if id(r) in pr:
                 for c in range(nc):
-                    K.append(f"{{ const double d_ = (double)rv[{off + c}] - rv{ri_here}_piv; rv{ri_here}_s1 += d_;"
-                             f" rv{ri_here}_s2 = fma(d_, d_, rv{ri_here}_s2); }}")
+                    v = f"rv[{off + c}]"
+                    if r.red == "var" and _exact_value(spec, r):
+                        K.append(f"{{ const double d_ = (double){v} - rv{ri_here}_piv; rv{ri_here}_s1 += d_;"
+                                 f" rv{ri_here}_s2 = fma(d_, d_, rv{ri_here}_s2); }}")
+                    elif r.red == "var":
+                        K.append(f"{{ const float d_ = {v} - rv{ri_here}_p32; pp{ri_here}_s1 += d_;"
+                                 f" pp{ri_here}_s2 = fmaf(d_, d_, pp{ri_here}_s2); }}")
+                    elif r.red == "sumsq":
+                        K.append(f"pp{ri_here}_a = fmaf({v}, {v}, pp{ri_here}_a);")
+                    else:
+                        K.append(f"pp{ri_here}_a += {v};")
                 continue
             if r.red == "cov":
                 h = f"rv{ri_here}"
@@ -1057,34 +1066,66 @@ def _epilogue(spec: PassSpec, e: "_Emitter", scan_ok: bool, skip: Sequence[RootS
     return [k.replace("{M}", str(m)).replace("{KK}", str(kk)) for k in K]
 
 
-def hoisted_var_roots(spec: PassSpec) -> List[Tuple[int, RootSpec]]:
-    """Variance roots (index among reductions, root). In the z-march the pivot of a
-    thread's pivot-shifted sums is taken once, from the first valid voxel of the
-    first plane that has one, and the count grows by the plane's valid voxels, so
-    a voxel adds only d = x - pivot, d and d^2 (FP64). The voxel order and every
-    operation are those of the per-voxel form, so the sums are the same bit for bit."""
-    return [(ri, r) for ri, r in enumerate([x for x in spec.roots if x.kind == "red"]) if r.red == "var"]
+def plane_roots(spec: PassSpec) -> List[Tuple[int, RootSpec]]:
+    """Reduction roots (index among reductions, root) that the z-march accumulates
+    per plane: the variances of any value, and the sums and sums of squares of
+    COMPUTED values. A thread's voxels of one plane (VPT x KV of them) are summed in
+    FP32 and the plane sums added to its FP64 accumulators; for a variance the
+    pivot of the pivot-shifted sums is the thread's first valid voxel value, taken
+    once. A computed value already carries FP32 rounding, and the FP32 plane sums
+    add errors of that order per voxel, random in sign; against the FP64 oracle the
+    scalars keep their accuracy, and between schedules (which group voxels into
+    threads differently) they agree to FP32 rounding of the plane sums (about 1e-7
+    relative), while per-voxel results stay bit-identical. Variances and sums of stored field values (exact in FP32)
+    are accumulated in FP64 per voxel (plane sums only move the pivot and count)."""
+    out = []
+    for ri, r in enumerate([x for x in spec.roots if x.kind == "red"]):
+        if r.red == "var" or (r.red in ("sum", "sumsq") and spec.graph.nodes[r.node].op != "field"
+                              and _sum_from_var(spec, r) is None):
+            out.append((ri, r))
+    return out
 
 
-def _var_plane_open(spec: PassSpec, e: "_Emitter") -> List[str]:
-    """Before a plane's voxels: the thread's pivot, if it has none yet."""
+def _exact_value(spec: PassSpec, r: RootSpec) -> bool:
+    return spec.graph.nodes[r.node].op == "field"
+
+
+def _plane_open(spec: PassSpec, e: "_Emitter") -> List[str]:
+    """Before a plane's voxels: FP32 plane partials and, for variances, the
+    thread's pivot if it has none yet."""
     K: List[str] = []
-    for ri, r in hoisted_var_roots(spec):
-        off = e.offsets[spec.roots.index(r)]
-        K.append(f"if (!rv{ri}_h) {{")
-        K.append("  #pragma unroll")
-        K.append("  for (int m = 0; m < VPT; ++m) {")
-        K.append("    #pragma unroll")
-        K.append("    for (int q = 0; q < KV; ++q) "
-                 f"if (!rv{ri}_h && m_ok[m] && k_ok[q]) {{ rv{ri}_piv = (double)rvk[m][q][{off}]; rv{ri}_h = true; }}")
-        K.append("  }")
-        K.append("}")
+    for ri, r in plane_roots(spec):
+        if r.red == "var":
+            off = e.offsets[spec.roots.index(r)]
+            if not _exact_value(spec, r):
+                K.append(f"float pp{ri}_s1 = 0.0f, pp{ri}_s2 = 0.0f;")
+            K.append(f"if (!rv{ri}_h) {{")
+            K.append("  #pragma unroll")
+            K.append("  for (int m = 0; m < VPT; ++m) {")
+            K.append("    #pragma unroll")
+            K.append("    for (int q = 0; q < KV; ++q) "
+                     f"if (!rv{ri}_h && m_ok[m] && k_ok[q]) {{ rv{ri}_p32 = rvk[m][q][{off}];"
+                     f" rv{ri}_piv = (double)rv{ri}_p32; rv{ri}_h = true; }}")
+            K.append("  }")
+            K.append("}")
+        else:
+            K.append(f"float pp{ri}_a = 0.0f;")
     return K
 
 
-def _var_plane_close(spec: PassSpec, e: "_Emitter") -> List[str]:
-    """After a plane's voxels: its valid voxels join the count."""
-    return [f"rv{ri}_n += {e.g.nodes[r.node].nc}u * nvalid_;" for ri, r in hoisted_var_roots(spec)]
+def _plane_close(spec: PassSpec, e: "_Emitter") -> List[str]:
+    """After a plane's voxels: plane partials into the FP64 accumulators, and the
+    plane's valid voxels into the variance counts."""
+    K: List[str] = []
+    for ri, r in plane_roots(spec):
+        nc = e.g.nodes[r.node].nc
+        if r.red == "var":
+            if not _exact_value(spec, r):
+                K.append(f"rv{ri}_s1 += (double)pp{ri}_s1; rv{ri}_s2 += (double)pp{ri}_s2;")
+            K.append(f"rv{ri}_n += {nc}u * nvalid_;")
+        else:
+            K.append(f"rv{ri}_a += (double)pp{ri}_a;")
+    return K
 
 
 def hist_offsets(spec: PassSpec, red_off: int) -> Tuple[Dict[int, int], int]:
@@ -1122,6 +1163,7 @@ def _red_decls(spec: PassSpec, where: str = "main") -> List[str]:
                 K.append(f"unsigned long long* rv{ri}_hs = p.hist + {r.slot};")
         elif r.red == "var":
             K.append(f"double rv{ri}_piv = 0.0, rv{ri}_s1 = 0.0, rv{ri}_s2 = 0.0; unsigned int rv{ri}_n = 0u; bool rv{ri}_h = false;")
+            K.append(f"float rv{ri}_p32 = 0.0f;")
         elif r.red == "cov":
             # pivot-shifted sums of the pairs (a, b): n, Σda, Σdb, Σda·db, Σda², Σdb²
             K.append(f"double rv{ri}_pa = 0.0, rv{ri}_pb = 0.0, rv{ri}_sa = 0.0, rv{ri}_sb = 0.0, rv{ri}_sab = 0.0, "
@@ -1840,9 +1882,17 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         tmaps = tmap_specs(spec)
         tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
         K.append("  const int p_first = ib - RAD;")
+        # interior tiles of standalone TMA passes release ring slots per warp through
+        # "empty" mbarriers instead of a block barrier per plane (edge tiles keep the
+        # barrier: their ghost cells are written by every thread)
+        decouple = bool(tma_fields) and not lsu_fields and not batch
+        if decouple:
+            K.append("  u64* ebars = (u64*)(smem + 128);")
         if tma_fields:
             K.append("  if (tid == 0) {")
             K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
+            if decouple:
+                K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&ebars[s], NT / 32);")
             K.append("    fence_mbar_init();")
             for ti in range(len(tmaps)):
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
@@ -1980,111 +2030,155 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K.append(f"  #pragma unroll\n  for (int d = 0; d < 2 * RAD + 1; ++d) "
                          f"x.sb{f.slot}[d] = {rings[f.slot]}u + (unsigned)d * {plane_bytes(spec, f)}u + ob{f.slot};")
         K.append("  int snext = (2 * RAD + 1) % NSLOT;")
-        K.append("  for (int i = ib; i < ie; ++i) {")
-        K.append("    const int gi = i + p.i_base;")
-        if ghost and spec.i_periodic:
-            K.append("    const bool i_in = true;")
-        else:
-            K.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
-        K.append("    const size_t pbase = (size_t)i * plane_n + col;")
-        for ri, r in enumerate(reds):
-            if r.red == "integrate":
-                sm = 1 if r.method == "simpson" else 0
-                K.append(f"    const double rv{ri}_wi = sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm});")
-        if split:
-            K.append("    if (i_in) {")
-        # KV-wide stores for single-component outputs
-        vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1 and kvn > 1
-                    and r.out_dtype in ("f32", "f16", "bf16")]
-        # all voxels of the plane first, stores and accumulation after: with every field
-        # staged the reads stay inside the ring even for voxels beyond the grid, so the
-        # evaluation is unconditional and taps shared by neighbouring voxels load once
+        # computed outside any plane: whether the pass evaluates whole planes before stores
         eager = (split or R == 0) and all(f.staged for f in spec.fields)
-        if eager:
-            K.append(f"    float rvk[VPT][KV][{nroot}];")
+        def plane_body() -> List[str]:
+            B: List[str] = []
+            B.append("    const int gi = i + p.i_base;")
+            if ghost and spec.i_periodic:
+                B.append("    const bool i_in = true;")
+            else:
+                B.append("    const bool i_in = (gi >= RAD) && (gi < p.n0g - RAD);")
+            B.append("    const size_t pbase = (size_t)i * plane_n + col;")
+            for ri, r in enumerate(reds):
+                if r.red == "integrate":
+                    sm = 1 if r.method == "simpson" else 0
+                    B.append(f"    const double rv{ri}_wi = sten_simpson_w(gi, p.n0g, {r.dx[0]!r}, {sm});")
+            if split:
+                B.append("    if (i_in) {")
+            # KV-wide stores for single-component outputs
+            vec_outs = [r for r in spec.roots if r.kind == "out" and e.g.nodes[r.node].nc == 1 and kvn > 1
+                        and r.out_dtype in ("f32", "f16", "bf16")]
+            # all voxels of the plane first, stores and accumulation after: with every field
+            # staged the reads stay inside the ring even for voxels beyond the grid, so the
+            # evaluation is unconditional and taps shared by neighbouring voxels load once
+            eager = (split or R == 0) and all(f.staged for f in spec.fields)
+            if eager:
+                B.append(f"    float rvk[VPT][KV][{nroot}];")
+                for m in range(vpt):
+                    for kk in range(kvn):
+                        B.append(f"    eval_fast<{m}, {kk}>(x, rvk[{m}][{kk}]);")
+                B += ["    " + k for k in _plane_open(spec, e)]
             for m in range(vpt):
-                for kk in range(kvn):
-                    K.append(f"    eval_fast<{m}, {kk}>(x, rvk[{m}][{kk}]);")
-            K += ["    " + k for k in _var_plane_open(spec, e)]
-        for m in range(vpt):
-            K.append(f"    if (m_ok[{m}]) {{")
-            K.append(f"      const int j = tj0 + tjb + {m};")
-            K.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
-            if not eager:
-                K.append(f"      float rvm[KV][{nroot}];")
-            arr = f"rvk[{m}]" if eager else "rvm"
-            for kk in range(kvn):
-                K.append(f"      if (k_ok[{kk}]) {{")
-                K.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
-                K.append(f"        const size_t vox = rowvox + {kk};")
-                K.append(f"        float* rv = {arr}[{kk}];")
+                B.append(f"    if (m_ok[{m}]) {{")
+                B.append(f"      const int j = tj0 + tjb + {m};")
+                B.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
                 if not eager:
-                    for f in spec.fields:
-                        if not f.staged:
-                            K.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
-                    if split or R == 0:
-                        K.append(f"        eval_fast<{m}, {kk}>(x, rv);")
-                    else:
-                        K.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-                        K.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
-                K += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk,
-                                                     hoisted=eager)]
-                K.append("      }")
-            for r in vec_outs:
-                ct = CTYPE[r.out_dtype]
-                off = e.offsets[spec.roots.index(r)]
-                vals = ", ".join(f"{arr}[{q}][{off}]" for q in range(kvn))
-                K.append(f"      {{ {ct}* o_ = orow{r.out_slot} + ro_[{m}];")
-                K.append(f"        if (k_all && (((size_t)o_) & {kvn * ESIZE[r.out_dtype] - 1}) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
-                K.append("        else {")
-                for q in range(kvn):
-                    K.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, {arr}[{q}][{off}]);")
-                K.append("        }")
-                K.append("      }")
-            K.append("    }")
-        if eager:
-            K += ["    " + k for k in _var_plane_close(spec, e)]
-        if split:
-            K.append("    }")
-        for r in spec.roots:
-            if r.kind in ("out", "scan"):
-                K.append(f"    orow{r.out_slot} += plane_n * {e.g.nodes[r.node].nc};")
-        for f in spec.fields:
-            if not f.staged:
-                K.append(f"    frow{f.slot} += plane_n * {f.nc};")
-        # the next plane (i+1+RAD) must be resident and ghosted before the barrier;
-        # ghosts derived from cooperatively staged (asynchronous) rows wait for every
-        # thread's copies: an extra barrier, in edge tiles only
-        lsu_ghost = ghost and any(
-            (spec.ghosts or {}).get((f.slot, ax)) in _EXTRAPOLATED for f in lsu_fields for ax in (1, 2))
-        if tma_fields or (ghost and staged):
-            K.append("    if (i + 1 < ie) {")
-            if tma_fields:
-                K.append("      const int rel = i + 1 + RAD - p_first;")
-                K.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-            if ghost and staged and not lsu_ghost:
-                K.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
-            K.append("    }")
-        if async_lsu:
-            # this thread's copies of plane i+1+RAD (issued PREFETCH iterations ago) are done
-            K.append(f"    cp_async_wait<{cfg.prefetch - 1}>();")
-        if lsu_ghost:
-            K.append("    if (edge_cta) { __syncthreads(); if (i + 1 < ie) ghost_fill(i + 1 + RAD); }")
-        if staged and odd16:
-            K.append("    lsu_flush();   // misaligned rows of the plane requested last iteration")
-        if staged:
-            # the ring slot of plane i - RAD is refilled next: every thread must be done with it
-            K.append("    ok = __syncthreads_and(ok);")
-            K.append("    if (!ok) break;")
-        for f in spec.fields:
-            if f.staged:
-                K.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD; ++d) x.sb{f.slot}[d] = x.sb{f.slot}[d + 1];")
-                K.append(f"    x.sb{f.slot}[2 * RAD] = {rings[f.slot]}u + (unsigned)snext * {plane_bytes(spec, f)}u + ob{f.slot};")
-        K.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
-        if staged:
-            K.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
+                    B.append(f"      float rvm[KV][{nroot}];")
+                arr = f"rvk[{m}]" if eager else "rvm"
+                for kk in range(kvn):
+                    B.append(f"      if (k_ok[{kk}]) {{")
+                    B.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
+                    B.append(f"        const size_t vox = rowvox + {kk};")
+                    B.append(f"        float* rv = {arr}[{kk}];")
+                    if not eager:
+                        for f in spec.fields:
+                            if not f.staged:
+                                B.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
+                        if split or R == 0:
+                            B.append(f"        eval_fast<{m}, {kk}>(x, rv);")
+                        else:
+                            B.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
+                            B.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
+                    B += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk,
+                                                         plane=eager)]
+                    B.append("      }")
+                for r in vec_outs:
+                    ct = CTYPE[r.out_dtype]
+                    off = e.offsets[spec.roots.index(r)]
+                    vals = ", ".join(f"{arr}[{q}][{off}]" for q in range(kvn))
+                    B.append(f"      {{ {ct}* o_ = orow{r.out_slot} + ro_[{m}];")
+                    B.append(f"        if (k_all && (((size_t)o_) & {kvn * ESIZE[r.out_dtype] - 1}) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
+                    B.append("        else {")
+                    for q in range(kvn):
+                        B.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, {arr}[{q}][{off}]);")
+                    B.append("        }")
+                    B.append("      }")
+                B.append("    }")
+            if eager:
+                B += ["    " + k for k in _plane_close(spec, e)]
+            if split:
+                B.append("    }")
+            for r in spec.roots:
+                if r.kind in ("out", "scan"):
+                    B.append(f"    orow{r.out_slot} += plane_n * {e.g.nodes[r.node].nc};")
+            for f in spec.fields:
+                if not f.staged:
+                    B.append(f"    frow{f.slot} += plane_n * {f.nc};")
+            # the next plane (i+1+RAD) must be resident and ghosted before the barrier;
+            # ghosts derived from cooperatively staged (asynchronous) rows wait for every
+            # thread's copies: an extra barrier, in edge tiles only
+            lsu_ghost = ghost and any(
+                (spec.ghosts or {}).get((f.slot, ax)) in _EXTRAPOLATED for f in lsu_fields for ax in (1, 2))
+            if decouple:
+                # edge tiles: every thread may write ghost cells of the next plane, so a
+                # block barrier separates them from the reads; interior tiles: each warp
+                # marks the slot of plane i - RAD free on its "empty" barrier and waits only
+                # for the TMA of plane i + 1 + RAD; thread 0 refills the slot once every
+                # warp has freed it (all waits bounded)
+                B.append("    if (edge_cta) {")
+                B.append("      if (i + 1 < ie) {")
+                B.append("        const int rel = i + 1 + RAD - p_first;")
+                B.append("        ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+                if ghost:
+                    B.append("        ghost_fill(i + 1 + RAD);")
+                B.append("      }")
+                B.append("      ok = __syncthreads_and(ok);")
+                B.append("      if (!ok) break;")
+                B.append("    } else {")
+                B.append("      __syncwarp();")
+                B.append("      if ((tid & 31) == 0) mbar_arrive(&ebars[(i - RAD - p_first) % NSLOT]);")
+                B.append("      if (i + 1 < ie) {")
+                B.append("        const int rel = i + 1 + RAD - p_first;")
+                B.append("        ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+                B.append("      }")
+                B.append("      if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }")
+                B.append("    }")
+                for f in spec.fields:
+                    if f.staged:
+                        B.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD; ++d) x.sb{f.slot}[d] = x.sb{f.slot}[d + 1];")
+                        B.append(f"    x.sb{f.slot}[2 * RAD] = {rings[f.slot]}u + (unsigned)snext * {plane_bytes(spec, f)}u + ob{f.slot};")
+                B.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
+                B.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) {{")
+                B.append("      if (!edge_cta && tid == 0) {")
+                B.append("        const int relq = i - RAD - p_first;")
+                B.append("        ok = ok && mbar_wait_bounded(&ebars[relq % NSLOT], (relq / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+                B.append("      }")
+                B.append(f"      if (ok) request(i + RAD + 1 + {cfg.prefetch});")
+                B.append("    }")
+                return B
+            if tma_fields or (ghost and staged):
+                B.append("    if (i + 1 < ie) {")
+                if tma_fields:
+                    B.append("      const int rel = i + 1 + RAD - p_first;")
+                    B.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+                if ghost and staged and not lsu_ghost:
+                    B.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
+                B.append("    }")
             if async_lsu:
-                K.append("    cp_async_commit();  // one group per plane, empty near the segment end")
+                # this thread's copies of plane i+1+RAD (issued PREFETCH iterations ago) are done
+                B.append(f"    cp_async_wait<{cfg.prefetch - 1}>();")
+            if lsu_ghost:
+                B.append("    if (edge_cta) { __syncthreads(); if (i + 1 < ie) ghost_fill(i + 1 + RAD); }")
+            if staged and odd16:
+                B.append("    lsu_flush();   // misaligned rows of the plane requested last iteration")
+            if staged:
+                # the ring slot of plane i - RAD is refilled next: every thread must be done with it
+                B.append("    ok = __syncthreads_and(ok);")
+                B.append("    if (!ok) break;")
+            for f in spec.fields:
+                if f.staged:
+                    B.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD; ++d) x.sb{f.slot}[d] = x.sb{f.slot}[d + 1];")
+                    B.append(f"    x.sb{f.slot}[2 * RAD] = {rings[f.slot]}u + (unsigned)snext * {plane_bytes(spec, f)}u + ob{f.slot};")
+            B.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
+            if staged:
+                B.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
+                if async_lsu:
+                    B.append("    cp_async_commit();  // one group per plane, empty near the segment end")
+            return B
+
+        K.append("  for (int i = ib; i < ie; ++i) {")
+        K += plane_body()
         K.append("  }")
         K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
         K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"

@@ -89,7 +89,8 @@ def test_config0_shape_against_oracle():
 @pytest.mark.parametrize("boundary", ["periodic", "neumann"])
 def test_kv_chunks_match_one_voxel_per_thread(dtype, boundary):
     """Several k-adjacent voxels per thread (vector shared-memory chunks, paired
-    stores) compute every voxel exactly as one voxel per thread does."""
+    stores) compute every voxel exactly as one voxel per thread does; reductions of
+    computed values agree to FP32 plane-sum rounding."""
     import stenpy_b200 as S
     from stenpy_b200.codegen import PassConfig
     from stenpy_b200.synth import sinusoid_field, smoothed_vector
@@ -104,11 +105,13 @@ def test_kv_chunks_match_one_voxel_per_thread(dtype, boundary):
             g, sink, *_ = S.compile_expression(expr, boundary=boundary, field_map={"f": f, "u": u})
             w = [sink, g.add("variance", (sink,), {})]
             res = S.Runtime(device=dev, out_dtype=dtype, config=cfg).run(g, wanted=w)
-            outs[kv, tk] = (res[w[0]], float(res[w[1]]))
-        ref, vref = outs[1, 64]
+            outs[kv, tk, tj] = (res[w[0]], float(res[w[1]]))
+        ref, vref = outs[1, 64, 8]
         for key, (o, v) in outs.items():
             assert torch.equal(o, ref), (key, shape, (o.float() - ref.float()).abs().max().item())
-            assert abs(v - vref) <= 1e-12 * abs(vref), (key, v, vref)
+            # the variance of a computed value is summed per plane in FP32 over each
+            # thread's voxels, which schedules group differently
+            assert abs(v - vref) <= 1e-6 * abs(vref), (key, v, vref)
 
 
 @pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])

@@ -3,7 +3,8 @@
 process-group driver uses, partial rows are stacked in rank order). Per-voxel
 results reassembled from the ranks' owned planes equal the whole-field run bit
 for bit (every voxel takes the same arithmetic), and the scalars agree with it to
-1e-12 relative (FP64 partial rows folded in another grouping)."""
+1e-12 relative (FP64 partial rows folded in another grouping; variances to 1e-6,
+their FP32 plane sums being pivoted at each thread's first voxel)."""
 import pytest
 import torch
 
@@ -59,6 +60,9 @@ def test_emulated_ranks_equal_whole_field(world, case):
         ref = float(whole[nid])
         for r in range(world):
             v = float(res[r][ids[r][1][i]])
-            assert abs(v - ref) <= 1e-12 * max(abs(ref), 1e-300), (reds[i], r, v, ref)
+            # variances pivot each thread's FP32 plane sums at its first voxel, which
+            # moves with the slab bounds: FP32 rounding of those sums
+            tol = 1e-6 if reds[i] == "variance" else 1e-12
+            assert abs(v - ref) <= tol * max(abs(ref), 1e-300), (reds[i], r, v, ref)
         # every rank holds the same scalar, bit for bit
         assert len({float(res[r][ids[r][1][i]]) for r in range(world)}) == 1

@@ -861,7 +861,7 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
     """(total bytes, byte offset of each staged field's ring, offset of the
     block-reduction scratch). Ring slots are 128-byte aligned (TMA destinations)."""
     nslot = 2 * spec.radius + 1 + spec.cfg.prefetch
-    off = 256  # mbarriers: up to 16 slots "full" (TMA done), then 16 "empty" (warps done)
+    off = 128  # mbarriers: up to 16 slots
     rings: Dict[int, int] = {}
     for f in spec.fields:
         if f.staged:
@@ -1882,17 +1882,9 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         tmaps = tmap_specs(spec)
         tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
         K.append("  const int p_first = ib - RAD;")
-        # interior tiles of standalone TMA passes release ring slots per warp through
-        # "empty" mbarriers instead of a block barrier per plane (edge tiles keep the
-        # barrier: their ghost cells are written by every thread)
-        decouple = bool(tma_fields) and not lsu_fields and not batch
-        if decouple:
-            K.append("  u64* ebars = (u64*)(smem + 128);")
         if tma_fields:
             K.append("  if (tid == 0) {")
             K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
-            if decouple:
-                K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&ebars[s], NT / 32);")
             K.append("    fence_mbar_init();")
             for ti in range(len(tmaps)):
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
@@ -2110,43 +2102,6 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             # thread's copies: an extra barrier, in edge tiles only
             lsu_ghost = ghost and any(
                 (spec.ghosts or {}).get((f.slot, ax)) in _EXTRAPOLATED for f in lsu_fields for ax in (1, 2))
-            if decouple:
-                # edge tiles: every thread may write ghost cells of the next plane, so a
-                # block barrier separates them from the reads; interior tiles: each warp
-                # marks the slot of plane i - RAD free on its "empty" barrier and waits only
-                # for the TMA of plane i + 1 + RAD; thread 0 refills the slot once every
-                # warp has freed it (all waits bounded)
-                B.append("    if (edge_cta) {")
-                B.append("      if (i + 1 < ie) {")
-                B.append("        const int rel = i + 1 + RAD - p_first;")
-                B.append("        ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-                if ghost:
-                    B.append("        ghost_fill(i + 1 + RAD);")
-                B.append("      }")
-                B.append("      ok = __syncthreads_and(ok);")
-                B.append("      if (!ok) break;")
-                B.append("    } else {")
-                B.append("      __syncwarp();")
-                B.append("      if ((tid & 31) == 0) mbar_arrive(&ebars[(i - RAD - p_first) % NSLOT]);")
-                B.append("      if (i + 1 < ie) {")
-                B.append("        const int rel = i + 1 + RAD - p_first;")
-                B.append("        ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-                B.append("      }")
-                B.append("      if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }")
-                B.append("    }")
-                for f in spec.fields:
-                    if f.staged:
-                        B.append(f"    #pragma unroll\n    for (int d = 0; d < 2 * RAD; ++d) x.sb{f.slot}[d] = x.sb{f.slot}[d + 1];")
-                        B.append(f"    x.sb{f.slot}[2 * RAD] = {rings[f.slot]}u + (unsigned)snext * {plane_bytes(spec, f)}u + ob{f.slot};")
-                B.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
-                B.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) {{")
-                B.append("      if (!edge_cta && tid == 0) {")
-                B.append("        const int relq = i - RAD - p_first;")
-                B.append("        ok = ok && mbar_wait_bounded(&ebars[relq % NSLOT], (relq / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-                B.append("      }")
-                B.append(f"      if (ok) request(i + RAD + 1 + {cfg.prefetch});")
-                B.append("    }")
-                return B
             if tma_fields or (ghost and staged):
                 B.append("    if (i + 1 < ie) {")
                 if tma_fields:

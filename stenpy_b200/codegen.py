@@ -93,7 +93,6 @@ class FieldSpec:
     halo: int = 0         # j/k halo of the staged tile (0 for fields read only at the voxel)
     wrap_k: bool = False  # periodic ghosts along dim 2 come from extra TMA strips
     wrap_j: bool = False  # periodic ghosts along dim 1 come from extra TMA strips
-    vec: int = 1          # cooperative staging: elements per asynchronous copy (row alignment)
 
 
 @dataclass
@@ -867,11 +866,26 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
         if f.staged:
             rings[f.slot] = off
             off += plane_bytes(spec, f) * nslot
+    for f in spec.fields:
+        if f.staged and not f.tma:
+            off += rs_stage_bytes(spec, f)     # row staging (stage_offsets)
     off = (off + 127) // 128 * 128
     red_off = off
     off += RED_SCRATCH_DOUBLES * 8
     off += sum(4 * r.bins for r in spec.roots if r.kind == "red" and r.red == "hist")
     return off, rings, red_off
+
+
+def stage_offsets(spec: PassSpec) -> Dict[int, int]:
+    """Byte offsets of the row-staging buffers (fields TMA cannot describe), after the rings."""
+    nslot = 2 * spec.radius + 1 + spec.cfg.prefetch
+    off = 128 + sum(plane_bytes(spec, f) * nslot for f in spec.fields if f.staged)
+    out: Dict[int, int] = {}
+    for f in spec.fields:
+        if f.staged and not f.tma:
+            out[f.slot] = off
+            off += rs_stage_bytes(spec, f)
+    return out
 
 
 def _a128(x: int) -> int:
@@ -1242,26 +1256,6 @@ def _remap_line(var: str, n: str, rule: Optional[str], indent: str) -> List[str]
     return []
 
 
-def lsu_vec(pitch_bytes: int, es: int) -> int:
-    """Elements per asynchronous copy for rows of ``pitch_bytes``: the widest copy
-    (4, 8 or 16 bytes) that every row start is aligned to, so that units inside a
-    row need no per-row alignment (16-bit rows of odd length use element pairs: every
-    other row is then copied element-wise)."""
-    a = 16
-    while a > es and pitch_bytes % a:
-        a //= 2
-    return max(a // es, 2 if es == 2 else 1)
-
-
-def _lsu_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig"):
-    w, h = spec.box(f)
-    es = ESIZE[f.dtype]
-    v = f.vec                        # elements per copy unit
-    u = w // v                       # units per row
-    tc, ncc, rp, nk = lsu_mapping(u, h, cfg.threads)
-    return w, h, es, v, u, tc, ncc, rp, nk
-
-
 def _lsu_elem(spec: "PassSpec", f: "FieldSpec", x: str, rule: Optional[str], ind: str, tag: str) -> List[str]:
     """Global column of box column ``x`` (an element index inside the row): kg{tag},
     component c{tag}, validity ok{tag}, byte offset off{tag} inside the row."""
@@ -1275,228 +1269,146 @@ def _lsu_elem(spec: "PassSpec", f: "FieldSpec", x: str, rule: Optional[str], ind
     return L
 
 
-def _lsu_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -> List[str]:
-    """Per-tile column plan of a cooperatively staged field: for each copy unit
-    (``vec`` adjacent elements of a row) this thread copies in every row, its byte
-    offset inside the row after the dim-2 rule and its size (0: outside the grid, the
-    unit is zero). Units split by the rule (not adjacent in memory, or partly outside)
-    are marked for the element-wise path; ``lsu2`` says whether this thread can have
-    element-wise work at all (split units, or rows not aligned to the unit)."""
-    w, h, es, v, u, tc, ncc, rp, nk = _lsu_geometry(spec, f, cfg)
-    ub = v * es
+def rs_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[int, int, int, int, int, int, int, int, int]:
+    """Row staging of a field whose rows TMA cannot describe: (box width w and height h
+    in elements, element size, box row bytes RB (a multiple of 16), 16-byte chunks C
+    per box row, chunks NCH per run, runs per row, runs, runs per thread). A run is
+    NCH consecutive 16-byte chunks of one box row; thread t stages runs t, t + NT, ..."""
+    w, h = spec.box(f)
+    es = ESIZE[f.dtype]
+    rb = w * es
+    assert rb % 16 == 0, "box rows are whole 16-byte chunks"
+    c = rb // 16
+    nch = next(n for n in (3, 2, 4, 1) if c % n == 0)
+    rpr = c // nch
+    runs = h * rpr
+    return w, h, es, rb, c, nch, rpr, runs, -(-runs // cfg.threads)
+
+
+def rs_stage_bytes(spec: "PassSpec", f: "FieldSpec") -> int:
+    """Shared-memory staging of one plane request: per run NCH + 1 aligned 16-byte
+    units and a 16-byte record (the row's shift and grid row, for the flush)."""
+    _, _, _, _, _, nch, _, runs, _ = rs_geometry(spec, f, spec.cfg)
+    return runs * (nch + 2) * 16
+
+
+def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> List[str]:
+    """The pending request of a row-staged field (plane id and array plane)."""
     sl = f.slot
-    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
-    L = [f"// staging plan of field {sl}: {u} units of {v} element(s) per row, {h} rows",
-         f"const int c0{sl}_ = tid % {tc}, rs{sl}_ = tid / {tc};",
-         f"u32 coff{sl}_[{ncc}], csz{sl}_[{ncc}];"]
-    if v > 1:
-        L.append(f"bool cbad{sl}_[{ncc}];")
-        L.append(f"bool lsu2{sl}_ = ((p.n2 * {f.nc * es}) % {ub}) != 0 || (((size_t)p.fld[{sl}]) % {ub}) != 0;")
-    L.append(f"#pragma unroll\nfor (int cc = 0; cc < {ncc}; ++cc) {{")
-    L.append(f"  const int un = c0{sl}_ + cc * {tc};")
-    for e in range(v):
-        L += _lsu_elem(spec, f, f"un * {v} + {e}", rk, "  ", str(e))
-    if v == 1:
-        L.append(f"  coff{sl}_[cc] = off0; csz{sl}_[cc] = (un < {u} && ok0) ? {es}u : 0u;")
-    else:
-        allok = " && ".join(f"ok{e}" for e in range(v))
-        anyok = " || ".join(f"ok{e}" for e in range(v))
-        contig = " && ".join(f"off{e} == off0 + {e * es}u" for e in range(1, v))
-        L.append(f"  coff{sl}_[cc] = off0; csz{sl}_[cc] = ({allok}) ? {ub}u : 0u;")
-        L.append(f"  cbad{sl}_[cc] = un < {u} && (({anyok}) && !(({allok}) && {contig} && (off0 % {ub}u) == 0u));")
-        L.append(f"  lsu2{sl}_ = lsu2{sl}_ || cbad{sl}_[cc];")
-    L.append("}")
-    return L
+    w, h, es, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, cfg)
+    return [f"// row staging of field {sl}: {runs} runs of {nch} x 16 bytes ({h} box rows of {c} chunks)",
+            f"int rsq{sl}_ = 0, rsz{sl}_ = 0; bool rspend{sl}_ = false;",
+            f"// a field base off 16 bytes would put bytes before it in a copy unit: element-wise then",
+            f"const bool rsal{sl}_ = (((size_t)p.fld[{sl}]) & 15) == 0;"]
 
 
-def _lsu_request(spec: "PassSpec", f: "FieldSpec", rings: Dict[int, int], cfg: "PassConfig",
-                 ghost: bool) -> List[str]:
-    """Staging of plane ``zq`` of a field whose rows TMA cannot describe, into ring
-    slot ``s``: every row (remapped by its dim-1 rule, or zero outside the grid) as
-    asynchronous copies of the planned units. Units that are split by the dim-2 rule
-    or whose global address is not aligned to the unit are copied element-wise after
-    that, loaded in groups before their stores."""
-    w, h, es, v, u, tc, ncc, rp, nk = _lsu_geometry(spec, f, cfg)
+def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool, stage_off: int) -> List[str]:
+    """Request of plane ``zq`` (ring slot of plane ``q``): every run's box row —
+    remapped by the dim-1 rule, or none outside the grid — as 16-byte asynchronous
+    copies from the aligned address at or below the run's first byte into this
+    thread's staging (units outside the field are zero), with a record of the row's
+    shift and grid row; ``rs_flush`` (one march iteration later) shifts them into the
+    ring."""
+    w, h, es, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, cfg)
     sl = f.slot
     rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
-    ct = CTYPE[f.dtype]
-    ub = v * es
+    row_elems = f"((long long)p.n2 * {f.nc})"
+    stride = (nch + 2) * 16
     L = ["{",
-         f"  const u32 sb = smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}) + "
-         f"(u32)((rs{sl}_ * {w} + c0{sl}_ * {v}) * {es});",
-         f"  const char* fb = (const char*)p.fld[{sl}];",
-         "  const bool zok = zq >= 0 && zq < p.nl;"]
-
-    def row(ind: str) -> List[str]:
-        R = [f"{ind}int jg = tj0 - {f.halo} + r;"]
-        R += _remap_line("jg", "p.n1", rj, ind)
-        R.append(f"{ind}const bool rok = zok && jg >= 0 && jg < p.n1;")
-        R.append(f"{ind}const char* rowb = fb + (rok ? ((size_t)zq * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es}) : (size_t)0);")
-        return R
-
-    guard_rs = rp * tc < cfg.threads
-    guard_r = nk * rp > h
-    guard_c = ncc * tc > u
-    zero = {4: "st_shared_u32({sa}, 0u);", 8: "st_shared_u64({sa}, 0ull);", 16: "st_shared_zero16({sa});"}[ub] \
-        if v > 1 else ""
-    # tiles whose box lies inside the field, on rows aligned to the unit: every unit is
-    # one full copy from a row pointer that advances by a fixed stride
-    pitch = f"((size_t)p.n2 * {f.nc * es})"
-    L.append(f"  if (zok && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && tk0 >= {spec.hk(f)} && "
-             f"tk0 + TK + {spec.hk(f)} <= p.n2 && {pitch} % {ub} == 0 && ((size_t)fb) % {ub} == 0) {{")
-    L.append(f"    if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{")
-    L.append(f"      const char* g = fb + ((size_t)zq * p.n1 + (tj0 - {f.halo} + rs{sl}_)) * {pitch} + "
-             f"(size_t)((tk0 - {spec.hk(f)}) * {f.nc * es} + c0{sl}_ * {ub});")
-    L.append(f"      const size_t rstep = {rp} * {pitch};")
-    for k in range(nk):
-        cond = [f"rs{sl}_ + {k * rp} < {h}"] if guard_r else []
-        body = []
-        for cc in range(ncc):
-            cc_cond = f"c0{sl}_ + {cc * tc} < {u}" if guard_c and cc == ncc - 1 else ""
-            st = f"cp_async_n<{ub}>(sb + {(k * rp * w + cc * tc * v) * es}u, g + {cc * tc * ub}, {ub}u);"
-            body.append(("if (" + cc_cond + ") " if cc_cond else "") + st)
-        pre = f"      if ({cond[0]}) {{ " if cond else "      { "
-        L.append(pre + " ".join(body) + (" g += rstep;" if k + 1 < nk else "") + " }")
-    L.append("    }")
-    if v == 2 and es == 2:
-        L += _lsu_odd16(spec, f, cfg, pitch, rp, nk, ncc, tc, u, w, h, guard_rs, guard_r, guard_c)
-    L.append("  } else {")
-    L.append(f"  if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{")
-    for k in range(nk):
-        L.append("    {")
-        L.append(f"      const int r = rs{sl}_ + {k * rp};")
-        if guard_r:
-            L.append(f"      if (r < {h}) {{")
-        ind = "        " if guard_r else "      "
-        L += row(ind)
-        if v == 1:
-            L.append(f"{ind}const u32 rsz = rok ? 0xffffffffu : 0u;")
-        for cc in range(ncc):
-            cond = f"c0{sl}_ + {cc * tc} < {u}" if guard_c and cc == ncc - 1 else ""
-            sa = f"sb + {(k * rp * w + cc * tc * v) * es}u"
-            if v == 1:
-                stmt = f"cp_async_n<{es}>({sa}, rowb + coff{sl}_[{cc}], csz{sl}_[{cc}] & rsz);"
-            else:
-                stmt = (f"{{ const char* gp = rowb + coff{sl}_[{cc}]; "
-                        f"if (!rok || (!cbad{sl}_[{cc}] && csz{sl}_[{cc}] == 0u)) {zero.format(sa=sa)} "
-                        f"else if (!cbad{sl}_[{cc}] && (((size_t)gp) % {ub}u) == 0) cp_async_n<{ub}>({sa}, gp, {ub}u); }}")
-            L.append(f"{ind}{'if (' + cond + ') ' if cond else ''}{stmt}")
-        if guard_r:
-            L.append("      }")
-        L.append("    }")
-    L.append("  }")
-    if v > 1:
-        # element-wise units: split by the dim-2 rule, or on rows not aligned to the unit
-        items = [(k, cc) for k in range(nk) for cc in range(ncc)]
-        G = max(1, 8 // v)
-        conds = [f"lsu2{sl}_"] + ([f"rs{sl}_ < {rp}"] if guard_rs else [])
-        L.append(f"  if ({' && '.join(conds)}) {{")
-        L.append(f"    {ct}* dst = ({ct}*)(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)});")
-        for g0 in range(0, len(items), G):
-            grp = items[g0:g0 + G]
-            L.append("    {")
-            L.append(f"      {ct} v_[{len(grp)}][{v}]; int d_[{len(grp)}];")
-            for t, (k, cc) in enumerate(grp):
-                L.append("      {")
-                L.append(f"        const int r = rs{sl}_ + {k * rp};")
-                L.append(f"        const int un = c0{sl}_ + {cc * tc};")
-                L.append(f"        d_[{t}] = -1;")
-                c2 = (["r < %d" % h] if guard_r else []) + (["un < %d" % u] if guard_c and cc == ncc - 1 else [])
-                L.append(f"        if ({' && '.join(c2) if c2 else 'true'}) {{")
-                L += row("          ")
-                L.append(f"          const char* gp = rowb + coff{sl}_[{cc}];")
-                L.append(f"          if (rok && (cbad{sl}_[{cc}] || (csz{sl}_[{cc}] != 0u && (((size_t)gp) % {ub}u) != 0))) {{")
-                L.append(f"            d_[{t}] = r * {w} + un * {v};")
-                L.append(f"            {ct} z_; " + ("z_.bits = 0;" if es == 2 else f"z_ = ({ct})0;"))
-                for e in range(v):
-                    L.append("            {")
-                    L += _lsu_elem(spec, f, f"un * {v} + {e}", rk, "              ", "")
-                    L.append(f"              v_[{t}][{e}] = ok ? ldg_raw((const {ct}*)(rowb + off)) : z_;")
-                    L.append("            }")
-                L.append("          }")
-                L.append("        }")
-                L.append("      }")
-            L.append(f"      #pragma unroll\n      for (int t_ = 0; t_ < {len(grp)}; ++t_)")
-            L.append("        if (d_[t_] >= 0) {")
-            for e in range(v):
-                L.append(f"          dst[d_[t_] + {e}] = v_[t_][{e}];")
-            L.append("        }")
-            L.append("    }")
-        L.append("  }")
-    L.append("  }")
-    L.append("}")
+         f"  if (rspend{sl}_) rs_flush{sl}();   // back-to-back requests: the previous one first",
+         f"  const unsigned long long fb_ = (unsigned long long)p.fld[{sl}];",
+         f"  const unsigned long long fe_ = fb_ + (unsigned long long)p.nl * p.n1 * {row_elems} * {es};",
+         f"  const bool zok = zq >= 0 && zq < p.nl;",
+         f"  #pragma unroll 1\n  for (int u = tid; u < {runs}; u += NT) {{",
+         f"    const int r = u / {rpr}, c0 = (u % {rpr}) * {nch};",
+         f"    int jg = tj0 - {f.halo} + r;"]
+    L += _remap_line("jg", "p.n1", rj, "    ")
+    L += [f"    const bool ok = zok && jg >= 0 && jg < p.n1;",
+          f"    unsigned char* run_ = smem + {stage_off} + u * {stride};",
+          "    u32 sh = 0u;",
+          "    if (ok) {",
+          f"      const long long e0 = ((long long)zq * p.n1 + jg) * {row_elems} + (long long)(tk0 - {spec.hk(f)}) * {f.nc};",
+          f"      const unsigned long long ai = fb_ + (unsigned long long)(e0 * {es});",
+          "      sh = (u32)(ai & 15ull);",
+          "      const unsigned long long a = (ai & ~15ull) + (unsigned long long)(c0 * 16);",
+          "      const u32 sd = smem_u32(run_);",
+          f"      #pragma unroll\n      for (int v = 0; v <= {nch}; ++v) {{",
+          "        const unsigned long long g = a + (unsigned long long)(v * 16);",
+          "        const u32 nb = (g < fb_ || g >= fe_) ? 0u : (u32)min(16ull, fe_ - g);",
+          "        if (nb) cp_async_n<16>(sd + v * 16, (const void*)g, nb); else st_shared_zero16(sd + v * 16);",
+          "      }",
+          "    }",
+          f"    *(int2*)(run_ + {(nch + 1) * 16}) = make_int2(ok ? jg : -1, (int)sh);",
+          "  }",
+          f"  rsq{sl}_ = q; rsz{sl}_ = zq; rspend{sl}_ = true;",
+          "}"]
     return L
 
 
-def _lsu_odd16(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", pitch: str, rp: int, nk: int, ncc: int,
-               tc: int, u: int, w: int, h: int, guard_rs: bool, guard_r: bool, guard_c: bool) -> List[str]:
-    """Tiles inside a 16-bit field whose rows have an odd number of elements: row
-    starts alternate between 4-byte alignment and 2 bytes past it. Aligned rows copy
-    their element pairs with asynchronous 4-byte copies; each pair of a misaligned row
-    is cut out of the two aligned words around it (loaded first for every row of the
-    thread, so their latencies overlap) and stored as one aligned word. The words
-    reach 2 bytes before and after the pair: a misaligned row never starts the field,
-    and the plane holding the field's last element is left to the general path."""
+def _rs_flush(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[int, int], ghost: bool,
+              stage_off: int) -> List[str]:
+    """``rs_flush{slot}()``: once this thread's copies of the pending request are
+    done, each of its chunks goes to the ring row: the 16 bytes starting at the row's
+    shift into the staging run (five aligned words, funnel-shifted); chunks that
+    cross a dim-2 face element by element from global memory with the dim-2 rule
+    (zero outside the grid); zeros for rows outside the grid."""
+    w, h, es, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, cfg)
     sl = f.slot
-    hk = spec.hk(f)
-    L = [f"  }} else if (zok && tj0 >= {f.halo} && tj0 + TJ + {f.halo} <= p.n1 && tk0 >= {hk} && "
-         f"tk0 + TK + {hk} <= p.n2 && {pitch} % 4 == 2 && ((size_t)fb) % 4 == 0 && "
-         f"!(zq == p.nl - 1 && tj0 + TJ + {f.halo} == p.n1 && tk0 + TK + {hk} == p.n2)) {{",
-         f"    if ({'rs%d_ < %d' % (sl, rp) if guard_rs else 'true'}) {{",
-         f"      const long long j0 = (long long)zq * p.n1 + (tj0 - {f.halo} + rs{sl}_);",
-         f"      const char* g = fb + (size_t)j0 * {pitch} + (size_t)((tk0 - {hk}) * {f.nc * 2} + c0{sl}_ * 4);",
-         f"      const size_t rstep = {rp} * {pitch};",
-         f"      pend{sl}_ = true; psb{sl}_ = sb; pj{sl}_ = j0;"]
-    for k in range(nk):
-        cond = [f"rs{sl}_ + {k * rp} < {h}"] if guard_r else []
-        L.append(f"      {{ const bool mis = ((j0 + {k * rp}) & 1) != 0;" + (f" if ({cond[0]}) {{" if cond else " {"))
-        for cc in range(ncc):
-            cc_cond = f"c0{sl}_ + {cc * tc} < {u}" if guard_c and cc == ncc - 1 else "true"
-            sa = f"sb + {(k * rp * w + cc * tc * 2) * 2}u"
-            L.append(f"        if ({cc_cond}) {{ const char* gp = g + {cc * tc * 4};"
-                     f" if (!mis) cp_async_n<4>({sa}, gp, 4u);"
-                     f" else {{ wa{sl}_[{k}][{cc}] = __ldg((const u32*)(gp - 2)); wb{sl}_[{k}][{cc}] = __ldg((const u32*)(gp + 2)); }} }}")
-        L.append("      }" + (" g += rstep;" if k + 1 < nk else "") + " }")
-    L.append("    }")
+    ct = CTYPE[f.dtype]
+    epc = 16 // es
+    hkn = spec.hk(f) * f.nc
+    stride = (nch + 2) * 16
+    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+    L = [f"auto rs_flush{sl} = [&]() {{",
+         f"  if (!rspend{sl}_) return;",
+         f"  rspend{sl}_ = false;",
+         "  cp_async_wait<0>();",
+         f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((rsq{sl}_ - p_first) % NSLOT) * {plane_bytes(spec, f)};",
+         f"  #pragma unroll 1\n  for (int u = tid; u < {runs}; u += NT) {{",
+         f"    const int r = u / {rpr}, c0 = (u % {rpr}) * {nch};",
+         f"    const unsigned char* run_ = smem + {stage_off} + u * {stride};",
+         f"    const int2 rec = *(const int2*)(run_ + {(nch + 1) * 16});",
+         f"    unsigned char* drow = slot_ + r * {rb};",
+         f"    #pragma unroll\n    for (int ch = 0; ch < {nch}; ++ch) {{",
+         "      const u32 dst = smem_u32(drow + (c0 + ch) * 16);",
+         "      if (rec.x < 0) { st_shared_zero16(dst); continue; }",
+         f"      const int x0 = (c0 + ch) * {epc} - {hkn}, x1 = x0 + {epc - 1};",
+         f"      const int k0 = tk0 + (x0 >= 0 ? x0 / {f.nc} : -((-x0 + {f.nc - 1}) / {f.nc}));",
+         f"      const int k1 = tk0 + x1 / {f.nc};",
+         f"      if (rsal{sl}_ && k0 >= 0 && k1 < p.n2) {{",
+         "        const u32 sh = (u32)rec.y;",
+         "        const u32* wsrc = (const u32*)(run_ + ch * 16 + (sh & ~3u));",
+         "        const u32 b_ = (sh & 3u) * 8u;",
+         "        const u32 w0 = wsrc[0], w1 = wsrc[1], w2 = wsrc[2], w3 = wsrc[3], w4 = wsrc[4];",
+         "        st_shared_u128(dst, __funnelshift_r(w0, w1, b_), __funnelshift_r(w1, w2, b_),",
+         "                       __funnelshift_r(w2, w3, b_), __funnelshift_r(w3, w4, b_));",
+         "      } else {",
+         f"        rs_edge{sl}(rec.x, (c0 + ch) * {epc}, ({ct}*)(drow + (c0 + ch) * 16));",
+         "      }",
+         "    }",
+         "  }",
+         "};"]
     return L
 
 
-def _lsu_odd16_state(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[List[str], List[str]]:
-    """Registers that carry the words of misaligned odd-length 16-bit rows from the
-    plane request that loads them to ``lsu_flush``, which cuts the pairs out and
-    stores them before the barrier that precedes the plane's use (one iteration of
-    the march later: the loads' latency hides behind one plane of compute)."""
-    w, h, es, v, u, tc, ncc, rp, nk = _lsu_geometry(spec, f, cfg)
+def _rs_edge(spec: "PassSpec", f: "FieldSpec", ghost: bool) -> List[str]:
+    """``rs_edge{slot}(jg, x, dst)``: the 16 bytes of box row elements x .. that cross a
+    dim-2 face, element by element from global memory with the dim-2 rule (zero
+    outside the grid); kept out of line (tiles at the dim-2 faces only)."""
     sl = f.slot
-    decl = [f"u32 wa{sl}_[{nk}][{ncc}], wb{sl}_[{nk}][{ncc}], psb{sl}_ = 0u; long long pj{sl}_ = 0; bool pend{sl}_ = false;"]
-    flush = [f"if (pend{sl}_) {{", f"  pend{sl}_ = false;"]
-    guard_rs = rp * tc < cfg.threads
-    if guard_rs:
-        flush.append(f"  if (rs{sl}_ < {rp}) {{")
-    for k in range(nk):
-        cond = f"rs{sl}_ + {k * rp} < {h} && " if nk * rp > h else ""
-        for cc in range(ncc):
-            cc_cond = f"c0{sl}_ + {cc * tc} < {u} && " if ncc * tc > u and cc == ncc - 1 else ""
-            sa = f"psb{sl}_ + {(k * rp * w + cc * tc * 2) * 2}u"
-            flush.append(f"  if ({cond}{cc_cond}((pj{sl}_ + {k * rp}) & 1) != 0) "
-                         f"st_shared_u32({sa}, __byte_perm(wa{sl}_[{k}][{cc}], wb{sl}_[{k}][{cc}], 0x5432));")
-    if guard_rs:
-        flush.append("  }")
-    flush.append("}")
-    return decl, flush
-
-
-def lsu_mapping(w: int, h: int, nt: int) -> Tuple[int, int, int, int]:
-    """Thread mapping of the cooperative staging of a w × h element box: TC threads
-    per row, each owning CC columns (c0 + cc·TC) for every row it copies; RP rows in
-    parallel, each thread K rows (r0 + k·RP). Columns are fixed per thread, so their
-    global offsets and validity are computed once per tile, not per plane."""
-    tc = min(nt, w)
-    cc = -(-w // tc)
-    rp = nt // tc
-    k = -(-h // rp)
-    return tc, cc, rp, k
+    es = ESIZE[f.dtype]
+    ct = CTYPE[f.dtype]
+    epc = 16 // es
+    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+    L = [f"auto rs_edge{sl} = [&](int jg, int xb, {ct}* de) {{",
+         f"  const char* rowb = (const char*)p.fld[{sl}] + ((size_t)rsz{sl}_ * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es});",
+         f"  #pragma unroll 1\n  for (int e = 0; e < {epc}; ++e) {{"]
+    L += _lsu_elem(spec, f, "xb + e", rk, "    ", "")
+    L += [f"    {ct} z_; " + ("z_.bits = 0;" if es == 2 else f"z_ = ({ct})0;"),
+          f"    de[e] = ok ? ldg_raw((const {ct}*)(rowb + off)) : z_;",
+          "  }",
+          "};"]
+    return L
 
 
 def _ghost_expr2(at, n: str, side: str) -> str:
@@ -1838,8 +1750,9 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     L.append(_simpson_fn())
     tma_fields = [f for f in spec.fields if f.tma]
     lsu_fields = [f for f in spec.fields if f.staged and not f.tma]
-    # cooperative staging of 4-byte fields is asynchronous: one commit group per plane
-    async_lsu = any(ESIZE[f.dtype] in (2, 4, 8) for f in lsu_fields)
+    # row staging (fields TMA cannot describe) is asynchronous: one commit group per request
+    async_lsu = bool(lsu_fields)
+    stage_off = stage_offsets(spec)
     total_smem, rings, red_off = smem_layout(spec)
     tma_bytes = sum(spec.box(f)[0] * spec.box(f)[1] * ESIZE[f.dtype] for f in tma_fields)
     reds = [r for r in spec.roots if r.kind == "red"]
@@ -1890,21 +1803,15 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
             K.append("  }")
             K.append("  __syncthreads();")
-        odd16 = [f for f in lsu_fields if f.vec == 2 and ESIZE[f.dtype] == 2]
         for f in lsu_fields:
-            K += ["  " + x for x in _lsu_plan(spec, f, cfg, ghost)]
-        if odd16:
-            K.append("  // misaligned odd-length 16-bit rows: words loaded by request(), stored by lsu_flush()")
-            for f in odd16:
-                K += ["  " + x for x in _lsu_odd16_state(spec, f, cfg)[0]]
-            K.append("  auto lsu_flush = [&]() {")
-            for f in odd16:
-                K += ["    " + x for x in _lsu_odd16_state(spec, f, cfg)[1]]
-            K.append("  };")
+            K += ["  " + x for x in _rs_plan(spec, f, cfg)]
+            K += ["  " + x for x in _rs_edge(spec, f, ghost)]
+            K += ["  " + x for x in _rs_flush(spec, f, cfg, rings, ghost, stage_off[f.slot])]
+        if lsu_fields:
+            K.append("  // staged rows of the last request into the ring (before the barrier that publishes them)")
+            K.append("  auto lsu_flush = [&]() { " + " ".join(f"rs_flush{f.slot}();" for f in lsu_fields) + " };")
         if staged:
             K.append("  auto request = [&](int q) {")
-            if odd16:
-                K.append("    lsu_flush();   // the previous request's misaligned rows (back-to-back requests)")
             K.append("    const int s = (q - p_first) % NSLOT;")
             if ghost and spec.i_periodic:
                 K.append("    const int zq = (q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q;")
@@ -1944,14 +1851,13 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                                  f"(tk0 - {hk}) * {f.nc}, 0, zq);")
                 K.append("    }")
             for f in lsu_fields:
-                K += ["    " + x for x in _lsu_request(spec, f, rings, cfg, ghost)]
+                K += ["    " + x for x in _rs_request(spec, f, cfg, ghost, stage_off[f.slot])]
             K.append("  };")
             if ghost:
                 K += ["  " + x for x in _ghost_fill(spec, rings)]
             if async_lsu:
                 K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) { request(q); cp_async_commit(); }")
-                if odd16:
-                    K.append("  lsu_flush();")
+                K.append("  lsu_flush();")
                 K.append("  cp_async_wait<0>();")
             else:
                 K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
@@ -2110,13 +2016,11 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 if ghost and staged and not lsu_ghost:
                     B.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
                 B.append("    }")
-            if async_lsu:
-                # this thread's copies of plane i+1+RAD (issued PREFETCH iterations ago) are done
-                B.append(f"    cp_async_wait<{cfg.prefetch - 1}>();")
+            if lsu_fields:
+                # the plane requested last iteration goes from staging into its ring slot
+                B.append("    lsu_flush();")
             if lsu_ghost:
                 B.append("    if (edge_cta) { __syncthreads(); if (i + 1 < ie) ghost_fill(i + 1 + RAD); }")
-            if staged and odd16:
-                B.append("    lsu_flush();   // misaligned rows of the plane requested last iteration")
             if staged:
                 # the ring slot of plane i - RAD is refilled next: every thread must be done with it
                 B.append("    ok = __syncthreads_and(ok);")
@@ -2138,10 +2042,13 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
         K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
                  % (" false" if batch else ""))
+        if async_lsu:
+            # a request past the last plane may still be copying into staging
+            K.append("  cp_async_wait<0>();")
         K += ["  " + k for k in _red_flush(spec, "cta")]
         if batch:
-            if async_lsu:
-                K.append("  cp_async_wait<0>();")
+            if async_lsu and not tma_fields:
+                K.append("  __syncthreads();   // every thread's staging copies are done before the next item")
             if tma_fields:
                 # every requested plane was waited on: retire the barriers before the
                 # next item re-initialises this shared memory

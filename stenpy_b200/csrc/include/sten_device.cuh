@@ -202,6 +202,9 @@ template <int N> STEN_DEV void cp_async_n(u32 sdst, const void* gsrc, u32 src_by
 }
 STEN_DEV void st_shared_u32(u32 saddr, u32 v) { asm volatile("st.shared.u32 [%0], %1;" :: "r"(saddr), "r"(v) : "memory"); }
 STEN_DEV void st_shared_u64(u32 saddr, u64 v) { asm volatile("st.shared.u64 [%0], %1;" :: "r"(saddr), "l"(v) : "memory"); }
+STEN_DEV void st_shared_u128(u32 saddr, u32 a, u32 b, u32 c, u32 d) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" :: "r"(saddr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
 STEN_DEV void st_shared_zero16(u32 saddr) {
   asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" :: "r"(saddr), "r"(0u) : "memory");
 }

@@ -34,7 +34,7 @@ import torch
 
 from . import _native as N
 from .codegen import (ESIZE, SHELL_THREADS, STENCIL_PRIMS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec,
-                      analyse_ghosts, emit_pass, lsu_vec, param_layout, pass_grid, shell_count, shell_regions,
+                      analyse_ghosts, emit_pass, param_layout, pass_grid, shell_count, shell_regions,
                       smem_layout, tmap_specs)
 from .graph import Graph
 from .lowering import LoweringError, OpLowerer, dx3
@@ -433,7 +433,6 @@ class Planner:
             es = ESIZE[f.dtype]
             f.tma = (n2 * f.nc * es) % 16 == 0 and (w * es) % 16 == 0 and w <= 256 and h <= 256
             f.staged = f.tma or f.slot in offset_read
-            f.vec = lsu_vec(n2 * f.nc * es, es)
             if radius == 0 and not has_scan:
                 f.tma = f.staged = False     # flat pass: vector loads straight from HBM
         if self.ghosts:

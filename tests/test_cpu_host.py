@@ -429,12 +429,18 @@ def test_2d_fields_plan_as_one_plane_grids():
         FC.Planner(g, list(sinks.values())).plan()
 
 
-def _emulate_staging(w, h, es, nc, halo, hk, tk0, tj0, n1, n2, rj, rk, nt, v, fb=0):
-    """Host model of the cooperative staging of one plane (the generated plan and
-    request code, formula for formula, both copy loops): returns {box element: global
-    element, or None for zero}, checking that every element is written once, every
-    global read is inside the field and every asynchronous copy is aligned."""
-    from stenpy_b200.codegen import lsu_mapping
+def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
+    """Host model of the row staging of one plane (the generated request and flush,
+    formula for formula, on a one-plane field starting at byte ``fb``): returns {box
+    element: global element, or None for zero}, checking that every element is written
+    once, every copy unit is 16-byte aligned and reads only bytes of the field, and
+    every shifted read stays inside its staging run."""
+    from stenpy_b200.codegen import ESIZE, rs_geometry
+    es, nc = ESIZE[f.dtype], f.nc
+    hk = spec.hk(f)
+    w, h, _, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, spec.cfg)
+    epc = 16 // es
+    fe = fb + n1 * n2 * nc * es
 
     def remap(x, n, rule):
         if rule == "periodic":
@@ -447,126 +453,71 @@ def _emulate_staging(w, h, es, nc, halo, hk, tk0, tj0, n1, n2, rj, rk, nt, v, fb
             return min(max(x, 0), n - 1)
         return x
 
-    def elem(x):
-        xr = x - hk * nc
-        kg = tk0 + xr // nc
-        c = xr - (kg - tk0) * nc
-        kg = remap(kg, n2, rk)
-        ok = 0 <= kg < n2
-        return ok, ((kg * nc + c) * es if ok else 0)
-
-    ub = v * es
-    u = w // v
-    tc, ncc, rp, nk = lsu_mapping(u, h, nt)
-    pitch = n2 * nc * es
-    nbytes = n1 * pitch
     out = {}
 
     def put(dst, g):
         assert dst not in out, ("written twice", dst)
         out[dst] = g
 
-    tj, tk = h - 2 * halo, w // nc - 2 * hk
-    if (tj0 >= halo and tj0 + tj + halo <= n1 and tk0 >= hk and tk0 + tk + hk <= n2
-            and pitch % ub == 0 and fb % ub == 0):
-        # box inside the field: full units from a row pointer advancing by RP rows
-        for tid in range(nt):
-            c0, rs = tid % tc, tid // tc
-            if rs >= rp:
-                continue
-            g = fb + (tj0 - halo + rs) * pitch + (tk0 - hk) * nc * es + c0 * ub
-            for k in range(nk):
-                r = rs + k * rp
-                if r < h:
-                    for cc in range(ncc):
-                        if c0 + cc * tc < u:
-                            ga = g + cc * tc * ub
-                            assert ga % ub == 0 and fb <= ga and ga + ub <= fb + nbytes
-                            for e in range(v):
-                                put(r * w + (c0 + cc * tc) * v + e, (ga - fb) // es + e)
-                g += rp * pitch
-        return out
-    if (v == 2 and es == 2 and tj0 >= halo and tj0 + tj + halo <= n1 and tk0 >= hk and tk0 + tk + hk <= n2
-            and pitch % 4 == 2 and fb % 4 == 0 and not (tj0 + tj + halo == n1 and tk0 + tk + hk == n2)):
-        # odd-length 16-bit rows inside the field: aligned rows by pairs, the others by
-        # the two aligned words around each pair (plane 0 of a one-plane field here)
-        for tid in range(nt):
-            c0, rs = tid % tc, tid // tc
-            if rs >= rp:
-                continue
-            j0 = tj0 - halo + rs
-            g = fb + j0 * pitch + (tk0 - hk) * nc * 2 + c0 * 4
-            for k in range(nk):
-                r = rs + k * rp
-                if r < h:
-                    for cc in range(ncc):
-                        if c0 + cc * tc < u:
-                            gp = g + cc * tc * 4
-                            if (j0 + k * rp) % 2 == 0:
-                                assert gp % 4 == 0
-                            else:
-                                assert (gp - 2) % 4 == 0 and fb <= gp - 2 and gp + 6 <= fb + nbytes
-                            for e in range(2):
-                                put(r * w + (c0 + cc * tc) * 2 + e, (gp - fb) // 2 + e)
-                g += rp * pitch
-        return out
-
     for tid in range(nt):
-        c0, rs = tid % tc, tid // tc
-        plan = []
-        lsu2 = pitch % ub != 0 or fb % ub != 0
-        for cc in range(ncc):
-            un = c0 + cc * tc
-            els = [elem(un * v + e) for e in range(v)]
-            csz = ub if all(ok for ok, _ in els) else 0
-            contig = all(els[e][1] == els[0][1] + e * es for e in range(v))
-            bad = un < u and any(ok for ok, _ in els) and not (csz and contig and els[0][1] % ub == 0)
-            lsu2 = lsu2 or bad
-            plan.append((un, els, csz, bad))
-        if rs >= rp:
-            continue
-        for k in range(nk):
-            r = rs + k * rp
-            if r >= h:
-                continue
-            jg = remap(tj0 - halo + r, n1, rj)
-            rok = 0 <= jg < n1
-            rowb = fb + (jg * pitch if rok else 0)
-            for un, els, csz, bad in plan:
-                if un >= u:
-                    continue
-                dst0 = r * w + un * v
-                gp = rowb + els[0][1]
-                if v == 1:
-                    n = csz if rok else 0
-                    assert gp % es == 0 and fb <= gp < fb + nbytes
-                    put(dst0, (gp - fb) // es if n else None)
-                    continue
-                if not rok or (not bad and csz == 0):
-                    for e in range(v):
+        for u in range(tid, runs, nt):
+            r, c0 = u // rpr, (u % rpr) * nch
+            jg = remap(tj0 - f.halo + r, n1, rj)
+            ok = 0 <= jg < n1
+            stage = {}                      # byte of the staging run -> global byte or None
+            sh = 0
+            if ok:
+                e0 = (jg * n2 + (tk0 - hk)) * nc
+                ai = fb + e0 * es
+                sh = ai % 16
+                a = ai - sh + c0 * 16
+                for v in range(nch + 1):
+                    g = a + 16 * v
+                    assert g % 16 == 0
+                    nb = 0 if (g < fb or g >= fe) else min(16, fe - g)
+                    for t in range(16):
+                        stage[16 * v + t] = g + t if t < nb else None
+            for ch in range(nch):
+                dst0 = r * w + (c0 + ch) * epc
+                if not ok:
+                    for e in range(epc):
                         put(dst0 + e, None)
-                elif not bad and gp % ub == 0:
-                    assert fb <= gp and gp + ub <= fb + nbytes
-                    for e in range(v):
-                        put(dst0 + e, (gp - fb) // es + e)
+                    continue
+                x0 = (c0 + ch) * epc - hk * nc
+                x1 = x0 + epc - 1
+                k0 = tk0 + x0 // nc
+                k1 = tk0 + x1 // nc
+                if fb % 16 == 0 and k0 >= 0 and k1 < n2:
+                    base = ch * 16 + (sh & ~3)
+                    assert base + 20 <= (nch + 1) * 16       # five words inside the run
+                    for e in range(epc):
+                        bytes_ = [stage[ch * 16 + sh + e * es + t] for t in range(es)]
+                        assert all(x is not None for x in bytes_), ("zero-filled byte used", e)
+                        assert all(bytes_[t] == bytes_[0] + t for t in range(es))
+                        put(dst0 + e, (bytes_[0] - fb) // es)
                 else:
-                    assert lsu2          # the element-wise loop runs for this thread
-                    for e in range(v):
-                        ok, off = els[e]
-                        if ok:
-                            assert fb <= rowb + off < fb + nbytes
-                        put(dst0 + e, (rowb + off - fb) // es if ok else None)
+                    rowb = fb + jg * n2 * nc * es
+                    for e in range(epc):
+                        xr = (c0 + ch) * epc + e - hk * nc
+                        kg = tk0 + xr // nc
+                        cc = xr - (kg - tk0) * nc
+                        kg = remap(kg, n2, rk)
+                        okk = 0 <= kg < n2
+                        if okk:
+                            assert fb <= rowb + (kg * nc + cc) * es < fe
+                        put(dst0 + e, (rowb + (kg * nc + cc) * es - fb) // es if okk else None)
     return out
 
 
 @pytest.mark.parametrize("es,nc", [(4, 1), (4, 3), (2, 1), (2, 3), (8, 1)])
 @pytest.mark.parametrize("rule", [None, "periodic", "replicate", "reflect"])
-def test_cooperative_staging_covers_every_box_element_once(es, nc, rule):
-    """Every element of a staged box is written exactly once — with the element its
-    axis rules map it to, or zero outside the grid — every global read is inside the
-    field and every asynchronous copy aligned, for interior, face and corner tiles of
-    ragged grids, with 16-byte-aligned and merely element-aligned field bases."""
-    from stenpy_b200.codegen import PassConfig, PassSpec, FieldSpec, PGraph, lsu_vec
+def test_row_staging_covers_every_box_element_once(es, nc, rule):
+    """Row staging (fields whose rows TMA cannot describe): every element of a staged
+    box is written exactly once — with the element its axis rules map it to, or zero
+    outside the grid — from aligned 16-byte copies that read only the field, for
+    interior, face and corner tiles of ragged grids, with 16-byte-aligned and merely
+    element-aligned field bases."""
+    from stenpy_b200.codegen import PassConfig, PassSpec, FieldSpec, PGraph
 
     def rm(x_, n_):
         if rule == "periodic":
@@ -582,16 +533,15 @@ def test_cooperative_staging_covers_every_box_element_once(es, nc, rule):
     dt = {4: "f32", 2: "bf16", 8: "f64"}[es]
     for tk, tj, nt in ((64, 8, 128), (32, 16, 128), (64, 16, 256)):
         cfg = PassConfig(tj=tj, tk=tk, threads=nt)
-        for n1, n2 in ((37, 45), (9, 33), (40, 130), (5, 7), (12, 34), (11, 510), (6, 22)):
-            f = FieldSpec(0, dt, nc, staged=True, halo=2, vec=lsu_vec(n2 * nc * es, es))
+        for n1, n2 in ((37, 45), (9, 33), (40, 130), (5, 7), (12, 34), (11, 509), (6, 22)):
+            f = FieldSpec(0, dt, nc, staged=True, halo=2)
             spec = PassSpec(PGraph(), [f], [], 1, 1, 2, cfg)
             hk = spec.hk(f)
             w, h = spec.box(f)
             for tj0 in range(0, n1, tj):
                 for tk0 in range(0, n2, tk):
-                    for fb in (0, es):
-                        got = _emulate_staging(w, h, es, nc, f.halo, hk, tk0, tj0, n1, n2, rule, rule, nt,
-                                               f.vec, fb)
+                    for fb in (0, es, 16 * 1000 + es * 3):
+                        got = _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rule, rule, nt, fb)
                         assert len(got) == w * h
                         for dst, g in got.items():
                             r, x = divmod(dst, w)
@@ -600,6 +550,7 @@ def test_cooperative_staging_covers_every_box_element_once(es, nc, rule):
                             jg, kg = rm(tj0 - f.halo + r, n1), rm(kg, n2)
                             want = (jg * n2 + kg) * nc + c if (0 <= jg < n1 and 0 <= kg < n2) else None
                             assert g == want, (dst, g, want, tj0, tk0, n1, n2, fb)
+
 
 def test_spectral_operators_are_registered_and_gpu_only():
     """FFT operators run outside the fused passes (opaque graph nodes) and, like every

@@ -1905,6 +1905,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 K.append(f"  double rv{ri}_wj[VPT], rv{ri}_wk[KV];")
                 K.append(f"  #pragma unroll\n  for (int m = 0; m < VPT; ++m) rv{ri}_wj[m] = sten_simpson_w(tj0 + tjb + m, p.n1, {r.dx[1]!r}, {sm});")
                 K.append(f"  #pragma unroll\n  for (int q = 0; q < KV; ++q) rv{ri}_wk[q] = sten_simpson_w(kt0 + q, p.n2, {r.dx[2]!r}, {sm});")
+        K.append("  const bool full_ = k_all" + "".join(f" && m_ok[{m}]" for m in range(vpt)) + ";")
         K.append("  unsigned int nvalid_ = 0u;  // voxels of a plane this thread owns inside the grid")
         K.append("  #pragma unroll\n  for (int m = 0; m < VPT; ++m) {\n    #pragma unroll\n"
                  "    for (int q = 0; q < KV; ++q) nvalid_ += (m_ok[m] && k_ok[q]) ? 1u : 0u;\n  }")
@@ -1957,42 +1958,57 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                     for kk in range(kvn):
                         B.append(f"    eval_fast<{m}, {kk}>(x, rvk[{m}][{kk}]);")
                 B += ["    " + k for k in _plane_open(spec, e)]
-            for m in range(vpt):
-                B.append(f"    if (m_ok[{m}]) {{")
-                B.append(f"      const int j = tj0 + tjb + {m};")
-                B.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
-                if not eager:
-                    B.append(f"      float rvm[KV][{nroot}];")
-                arr = f"rvk[{m}]" if eager else "rvm"
-                for kk in range(kvn):
-                    B.append(f"      if (k_ok[{kk}]) {{")
-                    B.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
-                    B.append(f"        const size_t vox = rowvox + {kk};")
-                    B.append(f"        float* rv = {arr}[{kk}];")
+            def voxel_loop(pred: bool) -> List[str]:
+                V: List[str] = []
+                for m in range(vpt):
+                    V.append(f"    if (m_ok[{m}]) {{" if pred else "    {")
+                    V.append(f"      const int j = tj0 + tjb + {m};")
+                    V.append(f"      const size_t rowvox = pbase + (size_t){m} * p.n2;")
                     if not eager:
-                        for f in spec.fields:
-                            if not f.staged:
-                                B.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
-                        if split or R == 0:
-                            B.append(f"        eval_fast<{m}, {kk}>(x, rv);")
-                        else:
-                            B.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
-                            B.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
-                    B += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk,
-                                                         plane=eager)]
-                    B.append("      }")
-                for r in vec_outs:
-                    ct = CTYPE[r.out_dtype]
-                    off = e.offsets[spec.roots.index(r)]
-                    vals = ", ".join(f"{arr}[{q}][{off}]" for q in range(kvn))
-                    B.append(f"      {{ {ct}* o_ = orow{r.out_slot} + ro_[{m}];")
-                    B.append(f"        if (k_all && (((size_t)o_) & {kvn * ESIZE[r.out_dtype] - 1}) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
-                    B.append("        else {")
-                    for q in range(kvn):
-                        B.append(f"          if (k_ok[{q}]) st_from_f32(o_ + {q}, {arr}[{q}][{off}]);")
-                    B.append("        }")
-                    B.append("      }")
+                        V.append(f"      float rvm[KV][{nroot}];")
+                    arr = f"rvk[{m}]" if eager else "rvm"
+                    for kk in range(kvn):
+                        V.append(f"      if (k_ok[{kk}]) {{" if pred else "      {")
+                        V.append(f"        const int k = kt0 + {kk}, mq = {m * kvn + kk};")
+                        V.append(f"        const size_t vox = rowvox + {kk};")
+                        V.append(f"        float* rv = {arr}[{kk}];")
+                        if not eager:
+                            for f in spec.fields:
+                                if not f.staged:
+                                    V.append(f"        x.gp{f.slot} = frow{f.slot} + ro_[{m}] * {f.nc} + {kk * f.nc};")
+                            if split or R == 0:
+                                V.append(f"        eval_fast<{m}, {kk}>(x, rv);")
+                            else:
+                                V.append("        const bool inter = i_in && j >= RAD && j < p.n1 - RAD && k >= RAD && k < p.n2 - RAD;")
+                                V.append(f"        if (inter) eval_fast<{m}, {kk}>(x, rv); else eval_slow(pg, gi, j, k, rv);")
+                        V += ["        " + k for k in _epilogue(spec, e, scan_ok=True, skip=vec_outs, m=m, kk=kk,
+                                                             plane=eager)]
+                        V.append("      }")
+                    for r in vec_outs:
+                        ct = CTYPE[r.out_dtype]
+                        off = e.offsets[spec.roots.index(r)]
+                        vals = ", ".join(f"{arr}[{q}][{off}]" for q in range(kvn))
+                        allk = "k_all && " if pred else ""
+                        V.append(f"      {{ {ct}* o_ = orow{r.out_slot} + ro_[{m}];")
+                        V.append(f"        if ({allk}(((size_t)o_) & {kvn * ESIZE[r.out_dtype] - 1}) == 0) {{ const float v_[KV] = {{{vals}}}; st_vec<KV>(o_, v_); }}")
+                        V.append("        else {")
+                        for q in range(kvn):
+                            cond = f"if (k_ok[{q}]) " if pred else ""
+                            V.append(f"          {cond}st_from_f32(o_ + {q}, {arr}[{q}][{off}]);")
+                        V.append("        }")
+                        V.append("      }")
+                    V.append("    }")
+                return V
+
+            if eager:
+                # tiles whose voxels all lie inside the grid skip the per-voxel predicates
+                B.append("    if (full_) {")
+                B += ["  " + v for v in voxel_loop(False)]
+                B.append("    } else {")
+                B += ["  " + v for v in voxel_loop(True)]
                 B.append("    }")
+            else:
+                B += voxel_loop(True)
             if eager:
                 B += ["    " + k for k in _plane_close(spec, e)]
             if split:

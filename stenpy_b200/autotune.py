@@ -55,7 +55,7 @@ def _valid(spec: PassSpec, cfg: PassConfig) -> bool:
         if f.tma and (w > 256 or h > 256 or (w * ESIZE[f.dtype]) % 16):
             return False
     total, _, _ = smem_layout(trial)
-    return total <= SMEM_LIMIT and 2 * spec.radius + 1 + cfg.prefetch <= 16
+    return total <= SMEM_LIMIT and 2 * spec.radius + 1 + cfg.prefetch <= FC.MAX_RING_SLOTS
 
 
 def default_kv(spec: PassSpec) -> int:
@@ -96,6 +96,10 @@ def candidates(spec: PassSpec) -> List[PassConfig]:
                             capped = dataclasses.replace(cfg, min_blocks=6)
                             if valid_shape(capped) and _valid(spec, capped):
                                 out.append(capped)
+    # row-staged fields land in their ring slot one iteration after the request: one
+    # plane of prefetch suffices, and the slot it saves can buy a resident CTA
+    if any(f.staged and not f.tma for f in spec.fields):
+        out += [c for c in (dataclasses.replace(c, prefetch=1) for c in out) if _valid(spec, c)]
     # keep distinct schedules only (scan passes collapse the segment axis)
     seen, uniq = set(), []
     for c in out:

@@ -866,26 +866,11 @@ def smem_layout(spec: PassSpec) -> Tuple[int, Dict[int, int], int]:
         if f.staged:
             rings[f.slot] = off
             off += plane_bytes(spec, f) * nslot
-    for f in spec.fields:
-        if f.staged and not f.tma:
-            off += rs_stage_bytes(spec, f)     # row staging (stage_offsets)
     off = (off + 127) // 128 * 128
     red_off = off
     off += RED_SCRATCH_DOUBLES * 8
     off += sum(4 * r.bins for r in spec.roots if r.kind == "red" and r.red == "hist")
     return off, rings, red_off
-
-
-def stage_offsets(spec: PassSpec) -> Dict[int, int]:
-    """Byte offsets of the row-staging buffers (fields TMA cannot describe), after the rings."""
-    nslot = 2 * spec.radius + 1 + spec.cfg.prefetch
-    off = 128 + sum(plane_bytes(spec, f) * nslot for f in spec.fields if f.staged)
-    out: Dict[int, int] = {}
-    for f in spec.fields:
-        if f.staged and not f.tma:
-            out[f.slot] = off
-            off += rs_stage_bytes(spec, f)
-    return out
 
 
 def _a128(x: int) -> int:
@@ -903,10 +888,10 @@ def strip_boxes(spec: PassSpec, f: FieldSpec) -> Tuple[Tuple[int, int], Tuple[in
 def slot_layout(spec: PassSpec, f: FieldSpec) -> Dict[str, int]:
     """Byte offsets inside one ring slot: the plane box, then wrap strips
     (left/right along dim 2, top/bottom along dim 1) when the field has them."""
-    w, h = spec.box(f)
+    h = spec.box(f)[1]
     es = ESIZE[f.dtype]
     off = {"box": 0}
-    o = _a128(w * h * es)
+    o = _a128(ring_w(spec, f) * h * es)
     (kw, kh), (jw, jh) = strip_boxes(spec, f)
     if f.wrap_k:
         off["kl"], off["kr"] = o, o + _a128(kw * kh * es)
@@ -1269,143 +1254,136 @@ def _lsu_elem(spec: "PassSpec", f: "FieldSpec", x: str, rule: Optional[str], ind
     return L
 
 
-def rs_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[int, int, int, int, int, int, int, int, int]:
+RS_SHIFT = 17                                   # chunk table: slot offset below, row offset mod 16 from here
+RS_VALID, RS_ROWOK, RS_KX = 1 << 21, 1 << 22, 1 << 23
+
+
+def ring_w(spec: "PassSpec", f: "FieldSpec") -> int:
+    """Row pitch of a staged field's ring slot, in elements: the box row, plus one
+    16-byte unit for row-staged fields (a row lands there as the 16-byte units that
+    cover it, and is shifted into place within that pitch)."""
+    w = spec.box(f)[0]
+    return w if f.tma else w + 16 // ESIZE[f.dtype]
+
+
+def rs_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[int, int, int, int, int, int, int, int]:
     """Row staging of a field whose rows TMA cannot describe: (box width w and height h
-    in elements, element size, box row bytes RB (a multiple of 16), 16-byte chunks C
-    per box row, chunks NCH per run, runs per row, runs, runs per thread). A run is
-    NCH consecutive 16-byte chunks of one box row; thread t stages runs t, t + NT, ..."""
+    in elements, element size es, box row bytes RB (a multiple of 16), 16-byte chunks
+    C per box row, ring row pitch SR = RB + 16 bytes, box rows per warp, chunks per
+    thread). Box row r is bulk-copied into ring row r as the 16-byte units that cover
+    it; warp r % (NT / 32) then shifts it into place, 32 chunks at a time."""
     w, h = spec.box(f)
     es = ESIZE[f.dtype]
     rb = w * es
     assert rb % 16 == 0, "box rows are whole 16-byte chunks"
     c = rb // 16
-    nch = next(n for n in (3, 2, 4, 1) if c % n == 0)
-    rpr = c // nch
-    runs = h * rpr
-    return w, h, es, rb, c, nch, rpr, runs, -(-runs // cfg.threads)
+    assert h * (rb + 16) <= 1 << RS_SHIFT, "slot offsets are packed in 17 bits"
+    rpw = -(-h // (cfg.threads // 32))
+    return w, h, es, rb, c, rb + 16, rpw, -(-(rpw * c) // 32)
 
 
-def rs_stage_bytes(spec: "PassSpec", f: "FieldSpec") -> int:
-    """Shared-memory staging of one plane request: per run NCH + 1 aligned 16-byte
-    units and a 16-byte record (the row's shift and grid row, for the flush)."""
-    _, _, _, _, _, nch, _, runs, _ = rs_geometry(spec, f, spec.cfg)
-    return runs * (nch + 2) * 16
-
-
-def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> List[str]:
-    """The pending request of a row-staged field (plane id and array plane)."""
+def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -> List[str]:
+    """Per-thread chunk table of a row-staged field, fixed for the whole march (one
+    word per chunk: its byte offset in the ring slot, the row's byte offset mod 16, and
+    flags: chunk exists / row inside the grid / chunk crosses a dim-2 face). Warp v owns box rows
+    v, v + NT/32, ...; its lanes take that list's chunks in order, 32 at a time."""
     sl = f.slot
-    w, h, es, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, cfg)
-    return [f"// row staging of field {sl}: {runs} runs of {nch} x 16 bytes ({h} box rows of {c} chunks)",
-            f"int rsq{sl}_ = 0, rsz{sl}_ = 0; bool rspend{sl}_ = false;",
-            f"// a field base off 16 bytes would put bytes before it in a copy unit: element-wise then",
-            f"const bool rsal{sl}_ = (((size_t)p.fld[{sl}]) & 15) == 0;"]
-
-
-def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool, stage_off: int) -> List[str]:
-    """Request of plane ``zq`` (ring slot of plane ``q``): every run's box row —
-    remapped by the dim-1 rule, or none outside the grid — as 16-byte asynchronous
-    copies from the aligned address at or below the run's first byte into this
-    thread's staging (units outside the field are zero), with a record of the row's
-    shift and grid row; ``rs_flush`` (one march iteration later) shifts them into the
-    ring."""
-    w, h, es, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, cfg)
-    sl = f.slot
+    w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
+    epc = 16 // es
+    hkn = spec.hk(f) * f.nc
     rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-    row_elems = f"((long long)p.n2 * {f.nc})"
-    stride = (nch + 2) * 16
-    L = ["{",
-         f"  if (rspend{sl}_) rs_flush{sl}();   // back-to-back requests: the previous one first",
-         f"  const unsigned long long fb_ = (unsigned long long)p.fld[{sl}];",
-         f"  const unsigned long long fe_ = fb_ + (unsigned long long)p.nl * p.n1 * {row_elems} * {es};",
-         f"  const bool zok = zq >= 0 && zq < p.nl;",
-         f"  #pragma unroll 1\n  for (int u = tid; u < {runs}; u += NT) {{",
-         f"    const int r = u / {rpr}, c0 = (u % {rpr}) * {nch};",
-         f"    int jg = tj0 - {f.halo} + r;"]
-    L += _remap_line("jg", "p.n1", rj, "    ")
-    L += [f"    const bool ok = zok && jg >= 0 && jg < p.n1;",
-          f"    unsigned char* run_ = smem + {stage_off} + u * {stride};",
-          "    u32 sh = 0u;",
-          "    if (ok) {",
-          f"      const long long e0 = ((long long)zq * p.n1 + jg) * {row_elems} + (long long)(tk0 - {spec.hk(f)}) * {f.nc};",
-          f"      const unsigned long long ai = fb_ + (unsigned long long)(e0 * {es});",
-          "      sh = (u32)(ai & 15ull);",
-          "      const unsigned long long a = (ai & ~15ull) + (unsigned long long)(c0 * 16);",
-          "      const u32 sd = smem_u32(run_);",
-          f"      #pragma unroll\n      for (int v = 0; v <= {nch}; ++v) {{",
-          "        const unsigned long long g = a + (unsigned long long)(v * 16);",
-          "        const u32 nb = (g < fb_ || g >= fe_) ? 0u : (u32)min(16ull, fe_ - g);",
-          "        if (nb) cp_async_n<16>(sd + v * 16, (const void*)g, nb); else st_shared_zero16(sd + v * 16);",
-          "      }",
-          "    }",
-          f"    *(int2*)(run_ + {(nch + 1) * 16}) = make_int2(ok ? jg : -1, (int)sh);",
-          "  }",
-          f"  rsq{sl}_ = q; rsz{sl}_ = zq; rspend{sl}_ = true;",
+    L = [f"// row staging of field {sl}: {h} box rows of {c} chunks, {ni} chunks per thread",
+         f"const u32 rsB{sl}_ = (u32)p.n2 * {f.nc * es}u;  // bytes of a grid row (mod 2^32)",
+         f"u32 rsit{sl}_[{ni}];",
+         f"#pragma unroll\nfor (int i = 0; i < {ni}; ++i) {{",
+         f"  const int ix = i * 32 + (tid & 31), m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
+         f"  int jg = tj0 - {f.halo} + r;"]
+    L += _remap_line("jg", "p.n1", rj, "  ")
+    L += [f"  const int xl = cc * {epc} - {hkn}, xh = xl + {epc - 1};",
+          f"  const int kl = tk0 + (xl >= 0 ? xl / {f.nc} : -((-xl + {f.nc - 1}) / {f.nc})), kh = tk0 + xh / {f.nc};",
+          f"  rsit{sl}_[i] = (m < {rpw} && r < {h}) ? ((u32)(r * {sr} + cc * 16) | ((((u32)jg * rsB{sl}_) & 15u) << {RS_SHIFT})"
+          f" | {RS_VALID}u | (jg >= 0 && jg < p.n1 ? {RS_ROWOK}u : 0u) | (kl < 0 || kh >= p.n2 ? {RS_KX}u : 0u)) : 0u;",
           "}"]
     return L
 
 
-def _rs_flush(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[int, int], ghost: bool,
-              stage_off: int) -> List[str]:
-    """``rs_flush{slot}()``: once this thread's copies of the pending request are
-    done, each of its chunks goes to the ring row: the 16 bytes starting at the row's
-    shift into the staging run (five aligned words, funnel-shifted); chunks that
-    cross a dim-2 face element by element from global memory with the dim-2 rule
-    (zero outside the grid); zeros for rows outside the grid."""
-    w, h, es, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, cfg)
+def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool, rings: Dict[int, int],
+                phase: str) -> List[str]:
+    """Request of plane ``zq`` into ring slot ``s`` by warp 0, one lane per box row: the
+    16-byte units covering the row — remapped by the dim-1 rule, none outside the
+    grid — less those that do not overlap the field, as one bulk copy onto the slot's
+    barrier. ``phase`` "size" adds the bytes to ``tot_``; "issue" copies."""
+    w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     sl = f.slot
-    ct = CTYPE[f.dtype]
-    epc = 16 // es
-    hkn = spec.hk(f) * f.nc
-    stride = (nch + 2) * 16
-    rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
-    L = [f"auto rs_flush{sl} = [&]() {{",
-         f"  if (!rspend{sl}_) return;",
-         f"  rspend{sl}_ = false;",
-         "  cp_async_wait<0>();",
-         f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((rsq{sl}_ - p_first) % NSLOT) * {plane_bytes(spec, f)};",
-         f"  #pragma unroll 1\n  for (int u = tid; u < {runs}; u += NT) {{",
-         f"    const int r = u / {rpr}, c0 = (u % {rpr}) * {nch};",
-         f"    const unsigned char* run_ = smem + {stage_off} + u * {stride};",
-         f"    const int2 rec = *(const int2*)(run_ + {(nch + 1) * 16});",
-         f"    unsigned char* drow = slot_ + r * {rb};",
-         f"    #pragma unroll\n    for (int ch = 0; ch < {nch}; ++ch) {{",
-         "      const u32 dst = smem_u32(drow + (c0 + ch) * 16);",
-         "      if (rec.x < 0) { st_shared_zero16(dst); continue; }",
-         f"      const int x0 = (c0 + ch) * {epc} - {hkn}, x1 = x0 + {epc - 1};",
-         f"      const int k0 = tk0 + (x0 >= 0 ? x0 / {f.nc} : -((-x0 + {f.nc - 1}) / {f.nc}));",
-         f"      const int k1 = tk0 + x1 / {f.nc};",
-         f"      if (rsal{sl}_ && k0 >= 0 && k1 < p.n2) {{",
-         "        const u32 sh = (u32)rec.y;",
-         "        const u32* wsrc = (const u32*)(run_ + ch * 16 + (sh & ~3u));",
-         "        const u32 b_ = (sh & 3u) * 8u;",
-         "        const u32 w0 = wsrc[0], w1 = wsrc[1], w2 = wsrc[2], w3 = wsrc[3], w4 = wsrc[4];",
-         "        st_shared_u128(dst, __funnelshift_r(w0, w1, b_), __funnelshift_r(w1, w2, b_),",
-         "                       __funnelshift_r(w2, w3, b_), __funnelshift_r(w3, w4, b_));",
-         "      } else {",
-         f"        rs_edge{sl}(rec.x, (c0 + ch) * {epc}, ({ct}*)(drow + (c0 + ch) * 16));",
-         "      }",
-         "    }",
-         "  }",
-         "};"]
+    rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
+    L = [f"#pragma unroll\nfor (int r = tid; r < {h}; r += 32) {{",
+         f"  int jg = tj0 - {f.halo} + r;"]
+    L += _remap_line("jg", "p.n1", rj, "  ")
+    L += [f"  if (zok && jg >= 0 && jg < p.n1) {{",
+          f"    const unsigned long long fb_ = (unsigned long long)p.fld[{sl}];",
+          f"    const unsigned long long fe_ = fb_ + (unsigned long long)p.nl * p.n1 * p.n2 * {f.nc * es}ull;",
+          f"    const long long e0 = ((long long)zq * p.n1 + jg) * ((long long)p.n2 * {f.nc})"
+          f" + (long long)(tk0 - {spec.hk(f)}) * {f.nc};",
+          f"    const unsigned long long a0 = fb_ + (unsigned long long)(e0 * {es}), al = a0 & ~15ull;",
+          f"    const unsigned long long s_ = max(al, fb_ & ~15ull), e_ = min((a0 + {rb + 15}ull) & ~15ull, (fe_ + 15ull) & ~15ull);"]
+    if phase == "size":
+        L.append("    if (e_ > s_) tot_ += (u32)(e_ - s_);")
+    else:
+        L.append(f"    if (e_ > s_) bulk_load(smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)} + r * {sr})"
+                 f" + (u32)(s_ - al), (const void*)s_, (u32)(e_ - s_), &bars[s]);")
+    L += ["  }", "}"]
     return L
 
 
-def _rs_edge(spec: "PassSpec", f: "FieldSpec", ghost: bool) -> List[str]:
-    """``rs_edge{slot}(jg, x, dst)``: the 16 bytes of box row elements x .. that cross a
-    dim-2 face, element by element from global memory with the dim-2 rule (zero
-    outside the grid); kept out of line (tiles at the dim-2 faces only)."""
+def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[int, int], ghost: bool,
+              zexpr: str) -> List[str]:
+    """``rs_shift{slot}(q)``, once plane q's copies landed in its ring slot: each ring
+    chunk becomes the 16 bytes that start ``shift`` bytes into it (the row's byte
+    offset mod 16), in place — a warp loads all its chunks of an iteration before it
+    stores any, and a row's chunks go in order — zero for rows outside the grid.
+    Chunks that cross a dim-2 face then get their out-of-grid elements from the dim-2
+    rule, element by element from global memory, or zero (tiles at the dim-2 faces
+    only: one loop after the shift keeps that code out of the unrolled chunks)."""
+    w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     sl = f.slot
-    es = ESIZE[f.dtype]
     ct = CTYPE[f.dtype]
     epc = 16 // es
+    rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
     rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
-    L = [f"auto rs_edge{sl} = [&](int jg, int xb, {ct}* de) {{",
-         f"  const char* rowb = (const char*)p.fld[{sl}] + ((size_t)rsz{sl}_ * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es});",
-         f"  #pragma unroll 1\n  for (int e = 0; e < {epc}; ++e) {{"]
-    L += _lsu_elem(spec, f, "xb + e", rk, "    ", "")
-    L += [f"    {ct} z_; " + ("z_.bits = 0;" if es == 2 else f"z_ = ({ct})0;"),
-          f"    de[e] = ok ? ldg_raw((const {ct}*)(rowb + off)) : z_;",
+    L = [f"auto rs_shift{sl} = [&](int q) {{",
+         f"  const int zq = {zexpr};",
+         "  const bool zok_ = zq >= 0 && zq < p.nl;",
+         f"  const u32 sz_ = (u32)(unsigned long long)p.fld[{sl}] + (u32)zq * ((u32)p.n1 * rsB{sl}_)"
+         f" + (u32)((tk0 - {spec.hk(f)}) * {f.nc * es});",
+         f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((q - p_first) % NSLOT) * {plane_bytes(spec, f)};",
+         "  u32 kx_ = 0u;   // chunks that cross a dim-2 face"]
+    for i in range(ni):
+        L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
+              f"    unsigned char* d_ = slot_ + (m_ & {(1 << RS_SHIFT) - 1}u);",
+              f"    const bool cp_ = zok_ && (m_ & {RS_ROWOK}u);",
+              "    uint4 v_ = make_uint4(0u, 0u, 0u, 0u);",
+              f"    if (cp_) v_ = shifted16<{es}>(d_, (sz_ + (m_ >> {RS_SHIFT})) & 15u);",
+              "    __syncwarp();   // every lane has read the chunks it needs before any is overwritten",
+              f"    if (m_ & {RS_VALID}u) *(uint4*)d_ = v_;",
+              f"    if (cp_ && (m_ & {RS_KX}u)) kx_ |= {1 << i}u;",
+              "  }"]
+    L += ["  #pragma unroll 1",
+          "  for (; kx_ != 0u; kx_ &= kx_ - 1u) {",
+          "    const int ix = (__ffs(kx_) - 1) * 32 + (tid & 31);",
+          f"    const int m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
+          f"    int jg = tj0 - {f.halo} + r;"]
+    L += _remap_line("jg", "p.n1", rj, "    ")
+    L += [f"    const char* rowb = (const char*)p.fld[{sl}] + ((size_t)zq * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es});",
+          f"    {ct}* d = ({ct}*)(slot_ + r * {sr} + cc * 16);",
+          f"    #pragma unroll 1\n    for (int e = 0; e < {epc}; ++e) {{",
+          f"      const int x0_ = cc * {epc} + e - {spec.hk(f) * f.nc};",
+          f"      const int k0_ = tk0 + (x0_ >= 0 ? x0_ / {f.nc} : -((-x0_ + {f.nc - 1}) / {f.nc}));",
+          "      if (k0_ >= 0 && k0_ < p.n2) continue;   // inside the grid: the shifted copy holds it"]
+    L += _lsu_elem(spec, f, f"cc * {epc} + e", rk, "      ", "")
+    L += [f"      {ct} v_; " + ("v_.bits = 0;" if es == 2 else f"v_ = ({ct})0;"),
+          f"      if (ok) v_ = ldg_raw((const {ct}*)(rowb + off));",
+          "      d[e] = v_;",
+          "    }",
           "  }",
           "};"]
     return L
@@ -1461,7 +1439,7 @@ def _ghost_fill(spec: PassSpec, rings: Dict[int, int]) -> List[str]:
         if not (todo_k or todo_j):
             continue
         ct = CTYPE[f.dtype]
-        w = spec.box(f)[0]
+        w = ring_w(spec, f)
         hk = spec.hk(f)
         nc = f.nc
         lay = slot_layout(spec, f)
@@ -1736,7 +1714,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         chunk = es in (2, 4) and cw % 4 == 0
         L.append(f"template <int DI, int DJ, int E> __device__ __forceinline__ float LDF{f.slot}(const FCtx& x) {{")
         L.append(f"  // element E of row DJ (relative to the thread's chunk) in the plane at offset DI")
-        L.append(f"  const unsigned char* row_ = sten_smem + x.sb{f.slot}[DI + RAD] + DJ * {spec.box(f)[0] * es};")
+        L.append(f"  const unsigned char* row_ = sten_smem + x.sb{f.slot}[DI + RAD] + DJ * {ring_w(spec, f) * es};")
         if chunk:
             L.append(f"  if constexpr (E >= 0 && E < {cfg.kv * f.nc}) return chunk_elem<{ct}, {cw}, E * {es}>(row_);")
             L.append(f"  else return ld_as_f32((const {ct}*)row_ + E);")
@@ -1750,9 +1728,6 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
     L.append(_simpson_fn())
     tma_fields = [f for f in spec.fields if f.tma]
     lsu_fields = [f for f in spec.fields if f.staged and not f.tma]
-    # row staging (fields TMA cannot describe) is asynchronous: one commit group per request
-    async_lsu = bool(lsu_fields)
-    stage_off = stage_offsets(spec)
     total_smem, rings, red_off = smem_layout(spec)
     tma_bytes = sum(spec.box(f)[0] * spec.box(f)[1] * ESIZE[f.dtype] for f in tma_fields)
     reds = [r for r in spec.roots if r.kind == "red"]
@@ -1795,7 +1770,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         tmaps = tmap_specs(spec)
         tidx = {(sl, kind): i for i, (sl, kind, _) in enumerate(tmaps)}
         K.append("  const int p_first = ib - RAD;")
-        if tma_fields:
+        zexpr = ("(q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q" if ghost and spec.i_periodic else "q")
+        if staged:
             K.append("  if (tid == 0) {")
             K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
             K.append("    fence_mbar_init();")
@@ -1804,73 +1780,82 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             K.append("  }")
             K.append("  __syncthreads();")
         for f in lsu_fields:
-            K += ["  " + x for x in _rs_plan(spec, f, cfg)]
-            K += ["  " + x for x in _rs_edge(spec, f, ghost)]
-            K += ["  " + x for x in _rs_flush(spec, f, cfg, rings, ghost, stage_off[f.slot])]
-        if lsu_fields:
-            K.append("  // staged rows of the last request into the ring (before the barrier that publishes them)")
-            K.append("  auto lsu_flush = [&]() { " + " ".join(f"rs_flush{f.slot}();" for f in lsu_fields) + " };")
+            K += ["  " + x for x in _rs_plan(spec, f, cfg, ghost)]
+            K += ["  " + x for x in _rs_shift(spec, f, cfg, rings, ghost, zexpr)]
         if staged:
             K.append("  auto request = [&](int q) {")
             K.append("    const int s = (q - p_first) % NSLOT;")
-            if ghost and spec.i_periodic:
-                K.append("    const int zq = (q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q;")
-            else:
-                K.append("    const int zq = q;")
-            if tma_fields:
-                K.append("    if (tid == 0) {")
+            K.append(f"    const int zq = {zexpr};")
+            K.append("    if (tid < 32) {")
+            if lsu_fields:
+                # warp 0 sizes the row copies first: the slot's barrier expects every byte
+                K.append("      const bool zok = zq >= 0 && zq < p.nl;")
+                K.append("      u32 tot_ = 0u;")
+                for f in lsu_fields:
+                    K += ["      " + x for x in _rs_request(spec, f, cfg, ghost, rings, "size")]
+                K.append("      tot_ = __reduce_add_sync(0xffffffffu, tot_);")
+            if lsu_fields:
+                # the lanes that issue copies order this CTA's earlier generic writes of
+                # the slot (the previous plane's shift) before them
                 K.append("      fence_proxy_async();")
-                K.append(f"      unsigned int bytes_ = {tma_bytes}u;")
-                for f in tma_fields:
-                    (kw, kh), (jw, jh) = strip_boxes(spec, f)
-                    es = ESIZE[f.dtype]
-                    if f.wrap_k:
-                        K.append(f"      if (tk0 == 0) bytes_ += {kw * kh * es}u;")
-                        K.append(f"      if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
-                    if f.wrap_j:
-                        K.append(f"      if (tj0 == 0) bytes_ += {jw * jh * es}u;")
-                        K.append(f"      if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
-                K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
-                for f in tma_fields:
-                    base = f"smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}"
-                    lay = slot_layout(spec, f)
-                    hk = spec.hk(f)
-                    K.append(f"      tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
-                             f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
-                    if f.wrap_k:
-                        ti = tidx[(f.slot, "kstrip")]
-                        K.append(f"      if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
-                                 f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
-                        K.append(f"      if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
-                                 f"0, tj0, zq);")
-                    if f.wrap_j:
-                        ti = tidx[(f.slot, "jstrip")]
-                        K.append(f"      if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
-                                 f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
-                        K.append(f"      if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
-                                 f"(tk0 - {hk}) * {f.nc}, 0, zq);")
-                K.append("    }")
-            for f in lsu_fields:
-                K += ["    " + x for x in _rs_request(spec, f, cfg, ghost, stage_off[f.slot])]
+            K.append("      if (tid == 0) {")
+            if not lsu_fields:
+                K.append("        fence_proxy_async();")
+            K.append(f"        unsigned int bytes_ = {tma_bytes}u{' + tot_' if lsu_fields else ''};")
+            for f in tma_fields:
+                (kw, kh), (jw, jh) = strip_boxes(spec, f)
+                es = ESIZE[f.dtype]
+                if f.wrap_k:
+                    K.append(f"        if (tk0 == 0) bytes_ += {kw * kh * es}u;")
+                    K.append(f"        if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
+                if f.wrap_j:
+                    K.append(f"        if (tj0 == 0) bytes_ += {jw * jh * es}u;")
+                    K.append(f"        if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
+            K.append("        mbar_arrive_expect_tx(&bars[s], bytes_);")
+            for f in tma_fields:
+                base = f"smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}"
+                lay = slot_layout(spec, f)
+                hk = spec.hk(f)
+                K.append(f"        tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
+                         f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
+                if f.wrap_k:
+                    ti = tidx[(f.slot, "kstrip")]
+                    K.append(f"        if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
+                             f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
+                    K.append(f"        if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
+                             f"0, tj0, zq);")
+                if f.wrap_j:
+                    ti = tidx[(f.slot, "jstrip")]
+                    K.append(f"        if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
+                             f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
+                    K.append(f"        if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
+                             f"(tk0 - {hk}) * {f.nc}, 0, zq);")
+            K.append("      }")
+            if lsu_fields:
+                K.append("      __syncwarp();")
+                for f in lsu_fields:
+                    K += ["      " + x for x in _rs_request(spec, f, cfg, ghost, rings, "issue")]
+            K.append("    }")
             K.append("  };")
+            if lsu_fields:
+                K.append("  // plane q resident: its row-staged fields shifted into place (published by the")
+                K.append("  // barrier that follows)")
+                K.append("  auto shift_rows = [&](int q) { " + " ".join(f"rs_shift{f.slot}(q);" for f in lsu_fields) + " };")
             if ghost:
                 K += ["  " + x for x in _ghost_fill(spec, rings)]
-            if async_lsu:
-                K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) { request(q); cp_async_commit(); }")
-                K.append("  lsu_flush();")
-                K.append("  cp_async_wait<0>();")
-            else:
-                K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
-            if lsu_fields:
-                K.append("  __syncthreads();")
+            K.append("  for (int q = p_first; q < p_first + NSLOT && q < ie + RAD; ++q) request(q);")
         K.append("  bool ok = true;")
         # planes p_first .. ib+RAD must be resident (and ghosted) before the first plane
-        if tma_fields:
+        if staged:
             K.append("  for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) {")
             K.append("    const int rel = q - p_first;")
             K.append("    ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+            if lsu_fields:
+                K.append("    shift_rows(q);")
             K.append("  }")
         if ghost and staged:
+            if lsu_fields:
+                K.append("  __syncthreads();  // shifted rows visible to the ghost fill")
             K.append("  if (edge_cta) { for (int q = p_first; q <= ib + RAD && q < ie + RAD; ++q) ghost_fill(q); }")
         if staged:
             K.append("  __syncthreads();")
@@ -1897,7 +1882,7 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  }")
         for f in spec.fields:
             if f.staged:
-                K.append(f"  const unsigned int ob{f.slot} = ((tjb + {f.halo}) * {spec.box(f)[0]} + (tk + {spec.hk(f)}) * {f.nc})"
+                K.append(f"  const unsigned int ob{f.slot} = ((tjb + {f.halo}) * {ring_w(spec, f)} + (tk + {spec.hk(f)}) * {f.nc})"
                          f" * {ESIZE[f.dtype]};")
         for ri, r in enumerate(reds):
             if r.red == "integrate":
@@ -2024,17 +2009,15 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             # thread's copies: an extra barrier, in edge tiles only
             lsu_ghost = ghost and any(
                 (spec.ghosts or {}).get((f.slot, ax)) in _EXTRAPOLATED for f in lsu_fields for ax in (1, 2))
-            if tma_fields or (ghost and staged):
+            if staged:
                 B.append("    if (i + 1 < ie) {")
-                if tma_fields:
-                    B.append("      const int rel = i + 1 + RAD - p_first;")
-                    B.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
-                if ghost and staged and not lsu_ghost:
+                B.append("      const int rel = i + 1 + RAD - p_first;")
+                B.append("      ok = ok && mbar_wait_bounded(&bars[rel % NSLOT], (rel / NSLOT) & 1, STEN_WAIT_LIMIT_NS);")
+                if lsu_fields:
+                    B.append("      shift_rows(i + 1 + RAD);")
+                if ghost and not lsu_ghost:
                     B.append("      if (edge_cta) ghost_fill(i + 1 + RAD);")
                 B.append("    }")
-            if lsu_fields:
-                # the plane requested last iteration goes from staging into its ring slot
-                B.append("    lsu_flush();")
             if lsu_ghost:
                 B.append("    if (edge_cta) { __syncthreads(); if (i + 1 < ie) ghost_fill(i + 1 + RAD); }")
             if staged:
@@ -2048,8 +2031,6 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             B.append("    snext = (snext + 1 == NSLOT) ? 0 : snext + 1;")
             if staged:
                 B.append(f"    if (i + RAD + 1 + {cfg.prefetch} < ie + RAD) request(i + RAD + 1 + {cfg.prefetch});")
-                if async_lsu:
-                    B.append("    cp_async_commit();  // one group per plane, empty near the segment end")
             return B
 
         K.append("  for (int i = ib; i < ie; ++i) {")
@@ -2058,14 +2039,9 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         K.append("  ok = __syncthreads_and(ok);  // uniform even when the march ran no plane")
         K.append("  if (!ok) { if (tid == 0) atomicExch(p.err, STEN_ERR_TMA_TIMEOUT); return%s; }"
                  % (" false" if batch else ""))
-        if async_lsu:
-            # a request past the last plane may still be copying into staging
-            K.append("  cp_async_wait<0>();")
         K += ["  " + k for k in _red_flush(spec, "cta")]
         if batch:
-            if async_lsu and not tma_fields:
-                K.append("  __syncthreads();   // every thread's staging copies are done before the next item")
-            if tma_fields:
+            if tma_fields or lsu_fields:
                 # every requested plane was waited on: retire the barriers before the
                 # next item re-initialises this shared memory
                 K.append("  __syncthreads();")

@@ -208,6 +208,30 @@ STEN_DEV void st_shared_u128(u32 saddr, u32 a, u32 b, u32 c, u32 d) {
 STEN_DEV void st_shared_zero16(u32 saddr) {
   asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" :: "r"(saddr), "r"(0u) : "memory");
 }
+// The 16 bytes that start `sh` (0..15, a multiple of ES) bytes into the 32 bytes at
+// the 16-byte aligned shared src: the word offset sh / 4 picked in two select steps,
+// the byte offset sh % 4 by funnel shifts.
+template <int ES> STEN_DEV uint4 shifted16(const unsigned char* src, u32 sh) {
+  const uint4 a = *(const uint4*)src, b = *(const uint4*)(src + 16);
+  const u32 w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  const bool s8 = (sh & 8u) != 0u, s4 = (sh & 4u) != 0u;
+  u32 x[6], y[5];
+  #pragma unroll
+  for (int j = 0; j < 6; ++j) x[j] = s8 ? w[j + 2] : w[j];
+  if constexpr (ES >= 8) return make_uint4(x[0], x[1], x[2], x[3]);
+  #pragma unroll
+  for (int j = 0; j < 5; ++j) y[j] = s4 ? x[j + 1] : x[j];
+  if constexpr (ES == 4) return make_uint4(y[0], y[1], y[2], y[3]);
+  const u32 bs = (sh & 3u) * 8u;
+  return make_uint4(__funnelshift_r(y[0], y[1], bs), __funnelshift_r(y[1], y[2], bs),
+                    __funnelshift_r(y[2], y[3], bs), __funnelshift_r(y[3], y[4], bs));
+}
+// Untiled bulk copy of `bytes` (a multiple of 16) from the 16-byte aligned global
+// address gsrc to the 16-byte aligned shared address sdst; completion counted on `bar`.
+STEN_DEV void bulk_load(u32 sdst, const void* gsrc, u32 bytes, u64* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :: "r"(sdst), "l"(gsrc), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
 STEN_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> STEN_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 STEN_DEV void fence_proxy_async() {

@@ -430,17 +430,22 @@ def test_2d_fields_plan_as_one_plane_grids():
 
 
 def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
-    """Host model of the row staging of one plane (the generated request and flush,
-    formula for formula, on a one-plane field starting at byte ``fb``): returns {box
-    element: global element, or None for zero}, checking that every element is written
-    once, every copy unit is 16-byte aligned and reads only bytes of the field, and
-    every shifted read stays inside its staging run."""
+    """Host model of the row staging of one plane (the generated request and in-place
+    shift, formula for formula, on a one-plane field starting at byte ``fb``): returns
+    {box element: global element, or None for zero}, checking that every bulk copy is
+    16-byte aligned, fits its ring row and reads only 16-byte units that overlap the
+    field; that a warp reads all chunks of an iteration before it writes any, with
+    every read inside its row; and that no element takes a byte that was not copied
+    from the field."""
     from stenpy_b200.codegen import ESIZE, rs_geometry
     es, nc = ESIZE[f.dtype], f.nc
     hk = spec.hk(f)
-    w, h, _, rb, c, nch, rpr, runs, rpt = rs_geometry(spec, f, spec.cfg)
+    w, h, _, rb, c, sr, rpw, ni = rs_geometry(spec, f, spec.cfg)
+    nw = nt // 32
+    assert rpw * nw >= h and ni * 32 >= rpw * c
     epc = 16 // es
     fe = fb + n1 * n2 * nc * es
+    rbg = n2 * nc * es
 
     def remap(x, n, rule):
         if rule == "periodic":
@@ -453,59 +458,82 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
             return min(max(x, 0), n - 1)
         return x
 
-    out = {}
+    slot = [None] * (h * sr)               # ring slot byte -> global byte ("outside": not the field)
+    for r in range(h):                      # request: one bulk copy per box row inside the grid
+        jg = remap(tj0 - f.halo + r, n1, rj)
+        if not 0 <= jg < n1:
+            continue
+        a0 = fb + ((jg * n2 + (tk0 - hk)) * nc) * es
+        al = a0 - a0 % 16
+        s_ = max(al, fb - fb % 16)
+        e_ = min((a0 + rb + 15) // 16 * 16, (fe + 15) // 16 * 16)
+        if e_ <= s_:
+            continue
+        assert s_ % 16 == 0 and e_ % 16 == 0
+        assert e_ - al <= sr, "copy fits the ring row"
+        for u in range(s_, e_, 16):
+            assert u < fe and u + 16 > fb, "a copied unit overlaps the field"
+        for g in range(s_, e_):
+            slot[r * sr + (g - al)] = g if fb <= g < fe else "outside"
 
-    def put(dst, g):
-        assert dst not in out, ("written twice", dst)
-        out[dst] = g
-
-    for tid in range(nt):
-        for u in range(tid, runs, nt):
-            r, c0 = u // rpr, (u % rpr) * nch
-            jg = remap(tj0 - f.halo + r, n1, rj)
-            ok = 0 <= jg < n1
-            stage = {}                      # byte of the staging run -> global byte or None
-            sh = 0
-            if ok:
-                e0 = (jg * n2 + (tk0 - hk)) * nc
-                ai = fb + e0 * es
-                sh = ai % 16
-                a = ai - sh + c0 * 16
-                for v in range(nch + 1):
-                    g = a + 16 * v
-                    assert g % 16 == 0
-                    nb = 0 if (g < fb or g >= fe) else min(16, fe - g)
-                    for t in range(16):
-                        stage[16 * v + t] = g + t if t < nb else None
-            for ch in range(nch):
-                dst0 = r * w + (c0 + ch) * epc
-                if not ok:
-                    for e in range(epc):
-                        put(dst0 + e, None)
+    sz = fb + (tk0 - hk) * nc * es            # plane 0
+    fixes = []
+    for v in range(nw):                      # warps touch disjoint rows: one at a time
+        for i in range(ni):
+            lanes = []
+            for lane in range(32):
+                ix = i * 32 + lane
+                m, cc = divmod(ix, c)
+                r = v + nw * m
+                if m >= rpw or r >= h:
                     continue
-                x0 = (c0 + ch) * epc - hk * nc
-                x1 = x0 + epc - 1
-                k0 = tk0 + x0 // nc
-                k1 = tk0 + x1 // nc
-                if fb % 16 == 0 and k0 >= 0 and k1 < n2:
-                    base = ch * 16 + (sh & ~3)
-                    assert base + 20 <= (nch + 1) * 16       # five words inside the run
-                    for e in range(epc):
-                        bytes_ = [stage[ch * 16 + sh + e * es + t] for t in range(es)]
-                        assert all(x is not None for x in bytes_), ("zero-filled byte used", e)
-                        assert all(bytes_[t] == bytes_[0] + t for t in range(es))
-                        put(dst0 + e, (bytes_[0] - fb) // es)
+                jg = remap(tj0 - f.halo + r, n1, rj)
+                off = r * sr + cc * 16
+                if 0 <= jg < n1:
+                    sh = (sz + (jg * rbg) % 16) % 16
+                    assert sh == (fb + ((jg * n2 + (tk0 - hk)) * nc) * es) % 16
+                    assert r * sr <= off and off + 32 <= (r + 1) * sr, "shifted read inside the row"
+                    val = slot[off + sh:off + sh + 16]          # every lane reads ...
+                    xl = cc * epc - hk * nc
+                    if tk0 + xl // nc < 0 or tk0 + (xl + epc - 1) // nc >= n2:
+                        fixes.append((r, cc, jg))
                 else:
-                    rowb = fb + jg * n2 * nc * es
-                    for e in range(epc):
-                        xr = (c0 + ch) * epc + e - hk * nc
-                        kg = tk0 + xr // nc
-                        cc = xr - (kg - tk0) * nc
-                        kg = remap(kg, n2, rk)
-                        okk = 0 <= kg < n2
-                        if okk:
-                            assert fb <= rowb + (kg * nc + cc) * es < fe
-                        put(dst0 + e, (rowb + (kg * nc + cc) * es - fb) // es if okk else None)
+                    val = [None] * 16
+                lanes.append((off, val))
+            for off, val in lanes:                             # ... before any lane writes
+                slot[off:off + 16] = val
+    zero = object()
+    for r in range(h):                       # rows outside the grid were written as zeros
+        if not 0 <= remap(tj0 - f.halo + r, n1, rj) < n1:
+            slot[r * sr:r * sr + rb] = [zero] * rb
+    fixed = {}
+    for r, cc, jg in fixes:                  # the dim-2 fix-up after the shift
+        rowb = fb + jg * rbg
+        for e in range(epc):
+            xr = cc * epc + e - hk * nc
+            kg = tk0 + xr // nc
+            if 0 <= kg < n2:
+                continue
+            ccomp = xr - (kg - tk0) * nc
+            kg = remap(kg, n2, rk)
+            okk = 0 <= kg < n2
+            if okk:
+                assert fb <= rowb + (kg * nc + ccomp) * es < fe
+            fixed[r * w + cc * epc + e] = (rowb + (kg * nc + ccomp) * es - fb) // es if okk else None
+    out = {}
+    for r in range(h):
+        for x in range(w):
+            dst = r * w + x
+            if dst in fixed:
+                out[dst] = fixed[dst]
+                continue
+            bytes_ = slot[r * sr + x * es:r * sr + (x + 1) * es]
+            if all(b_ is zero for b_ in bytes_):
+                out[dst] = None
+                continue
+            assert all(isinstance(b_, int) for b_ in bytes_), ("byte not copied from the field", r, x, bytes_)
+            assert all(bytes_[t] == bytes_[0] + t for t in range(es)) and (bytes_[0] - fb) % es == 0
+            out[dst] = (bytes_[0] - fb) // es
     return out
 
 

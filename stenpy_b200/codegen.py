@@ -1254,8 +1254,8 @@ def _lsu_elem(spec: "PassSpec", f: "FieldSpec", x: str, rule: Optional[str], ind
     return L
 
 
-RS_SHIFT = 17                                   # chunk table: slot offset below, row offset mod 16 from here
-RS_VALID, RS_ROWOK, RS_KX = 1 << 21, 1 << 22, 1 << 23
+RS_SHIFT = 13                       # chunk table: slot offset / 16 below, row offset mod 16 from here
+RS_VALID, RS_ROWOK, RS_KX = 1 << 17, 1 << 18, 1 << 19
 
 
 def ring_w(spec: "PassSpec", f: "FieldSpec") -> int:
@@ -1277,16 +1277,17 @@ def rs_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[in
     rb = w * es
     assert rb % 16 == 0, "box rows are whole 16-byte chunks"
     c = rb // 16
-    assert h * (rb + 16) <= 1 << RS_SHIFT, "slot offsets are packed in 17 bits"
+    assert h * (c + 1) < 1 << RS_SHIFT, "slot offsets are packed in 13 bits of 16-byte units"
     rpw = -(-h // (cfg.threads // 32))
     return w, h, es, rb, c, rb + 16, rpw, -(-(rpw * c) // 32)
 
 
 def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -> List[str]:
     """Per-thread chunk table of a row-staged field, fixed for the whole march (one
-    word per chunk: its byte offset in the ring slot, the row's byte offset mod 16, and
-    flags: chunk exists / row inside the grid / chunk crosses a dim-2 face). Warp v owns box rows
-    v, v + NT/32, ...; its lanes take that list's chunks in order, 32 at a time."""
+    word per chunk: its 16-byte unit in the ring slot, the row's byte offset mod 16,
+    and flags: chunk exists / row inside the grid / chunk crosses a dim-2 face). Warp
+    v owns box rows v,
+    v + NT/32, ...; its lanes take that list's chunks in order, 32 at a time."""
     sl = f.slot
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     epc = 16 // es
@@ -1299,24 +1300,25 @@ def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -
          f"  const int ix = i * 32 + (tid & 31), m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
          f"  int jg = tj0 - {f.halo} + r;"]
     L += _remap_line("jg", "p.n1", rj, "  ")
-    L += [f"  const int xl = cc * {epc} - {hkn}, xh = xl + {epc - 1};",
-          f"  const int kl = tk0 + (xl >= 0 ? xl / {f.nc} : -((-xl + {f.nc - 1}) / {f.nc})), kh = tk0 + xh / {f.nc};",
-          f"  rsit{sl}_[i] = (m < {rpw} && r < {h}) ? ((u32)(r * {sr} + cc * 16) | ((((u32)jg * rsB{sl}_) & 15u) << {RS_SHIFT})"
-          f" | {RS_VALID}u | (jg >= 0 && jg < p.n1 ? {RS_ROWOK}u : 0u) | (kl < 0 || kh >= p.n2 ? {RS_KX}u : 0u)) : 0u;",
+    L += [f"  const int x0 = cc * {epc} - {hkn};  // box element of the chunk's first element, from column tk0",
+          f"  const bool kx = x0 < -tk0 * {f.nc} || x0 + {epc} > (p.n2 - tk0) * {f.nc};",
+          f"  rsit{sl}_[i] = (m < {rpw} && r < {h}) ? ((u32)(r * {c + 1} + cc) | ((((u32)jg * rsB{sl}_) & 15u) << {RS_SHIFT})"
+          f" | {RS_VALID}u | (jg >= 0 && jg < p.n1 ? {RS_ROWOK}u : 0u) | (kx ? {RS_KX}u : 0u)) : 0u;",
           "}"]
     return L
 
 
 def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool, rings: Dict[int, int],
                 phase: str) -> List[str]:
-    """Request of plane ``zq`` into ring slot ``s`` by warp 0, one lane per box row: the
-    16-byte units covering the row — remapped by the dim-1 rule, none outside the
-    grid — less those that do not overlap the field, as one bulk copy onto the slot's
-    barrier. ``phase`` "size" adds the bytes to ``tot_``; "issue" copies."""
+    """Request of plane ``zq`` into ring slot ``s``, warp v for box rows v, v + NT/32, ...
+    (one lane per row): the 16-byte units covering the row — remapped by the dim-1
+    rule, none outside the grid — less those that do not overlap the field, as one
+    bulk copy onto the slot's barrier. ``phase`` "size" adds the bytes to ``tot_``;
+    "issue" copies."""
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     sl = f.slot
     rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-    L = [f"#pragma unroll\nfor (int r = tid; r < {h}; r += 32) {{",
+    L = [f"#pragma unroll 1\nfor (int r = (tid >> 5) + (tid & 31) * (NT / 32); r < {h}; r += NT) {{",
          f"  int jg = tj0 - {f.halo} + r;"]
     L += _remap_line("jg", "p.n1", rj, "  ")
     L += [f"  if (zok && jg >= 0 && jg < p.n1) {{",
@@ -1341,25 +1343,26 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
     chunk becomes the 16 bytes that start ``shift`` bytes into it (the row's byte
     offset mod 16), in place — a warp loads all its chunks of an iteration before it
     stores any, and a row's chunks go in order — zero for rows outside the grid.
-    Chunks that cross a dim-2 face then get their out-of-grid elements from the dim-2
-    rule, element by element from global memory, or zero (tiles at the dim-2 faces
-    only: one loop after the shift keeps that code out of the unrolled chunks)."""
+    Elements of chunks at a dim-2 face that lie outside the grid are zeroed, or, under
+    a dim-2 rule that copies values, fetched by that rule from global memory (one loop
+    after the shift keeps that code out of the unrolled chunks)."""
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     sl = f.slot
     ct = CTYPE[f.dtype]
     epc = 16 // es
     rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
     rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
+    gather = rk in _REMAP_RULES
     L = [f"auto rs_shift{sl} = [&](int q) {{",
          f"  const int zq = {zexpr};",
          "  const bool zok_ = zq >= 0 && zq < p.nl;",
          f"  const u32 sz_ = (u32)(unsigned long long)p.fld[{sl}] + (u32)zq * ((u32)p.n1 * rsB{sl}_)"
          f" + (u32)((tk0 - {spec.hk(f)}) * {f.nc * es});",
          f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((q - p_first) % NSLOT) * {plane_bytes(spec, f)};",
-         "  u32 kx_ = 0u;   // chunks that cross a dim-2 face"]
+         "  u32 kx_ = 0u;   // chunks at a dim-2 face"]
     for i in range(ni):
         L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
-              f"    unsigned char* d_ = slot_ + (m_ & {(1 << RS_SHIFT) - 1}u);",
+              f"    unsigned char* d_ = slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4);",
               f"    const bool cp_ = zok_ && (m_ & {RS_ROWOK}u);",
               "    uint4 v_ = make_uint4(0u, 0u, 0u, 0u);",
               f"    if (cp_) v_ = shifted16<{es}>(d_, (sz_ + (m_ >> {RS_SHIFT})) & 15u);",
@@ -1371,21 +1374,26 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
           "  for (; kx_ != 0u; kx_ &= kx_ - 1u) {",
           "    const int ix = (__ffs(kx_) - 1) * 32 + (tid & 31);",
           f"    const int m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
-          f"    int jg = tj0 - {f.halo} + r;"]
-    L += _remap_line("jg", "p.n1", rj, "    ")
-    L += [f"    const char* rowb = (const char*)p.fld[{sl}] + ((size_t)zq * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es});",
-          f"    {ct}* d = ({ct}*)(slot_ + r * {sr} + cc * 16);",
-          f"    #pragma unroll 1\n    for (int e = 0; e < {epc}; ++e) {{",
-          f"      const int x0_ = cc * {epc} + e - {spec.hk(f) * f.nc};",
-          f"      const int k0_ = tk0 + (x0_ >= 0 ? x0_ / {f.nc} : -((-x0_ + {f.nc - 1}) / {f.nc}));",
-          "      if (k0_ >= 0 && k0_ < p.n2) continue;   // inside the grid: the shifted copy holds it"]
-    L += _lsu_elem(spec, f, f"cc * {epc} + e", rk, "      ", "")
-    L += [f"      {ct} v_; " + ("v_.bits = 0;" if es == 2 else f"v_ = ({ct})0;"),
-          f"      if (ok) v_ = ldg_raw((const {ct}*)(rowb + off));",
-          "      d[e] = v_;",
-          "    }",
-          "  }",
-          "};"]
+          f"    unsigned char* d_ = slot_ + r * {sr} + cc * 16;"]
+    if gather:
+        L += [f"    int jg = tj0 - {f.halo} + r;"]
+        L += _remap_line("jg", "p.n1", rj, "    ")
+        L += [f"    const char* rowb = (const char*)p.fld[{sl}] + ((size_t)zq * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es});",
+              f"    {ct}* d = ({ct}*)d_;",
+              f"    #pragma unroll 1\n    for (int e = 0; e < {epc}; ++e) {{",
+              f"      const int x0_ = cc * {epc} + e - {spec.hk(f) * f.nc};",
+              f"      const int k0_ = tk0 + (x0_ >= 0 ? x0_ / {f.nc} : -((-x0_ + {f.nc - 1}) / {f.nc}));",
+              "      if (k0_ >= 0 && k0_ < p.n2) continue;   // inside the grid: the shifted copy holds it"]
+        L += _lsu_elem(spec, f, f"cc * {epc} + e", rk, "      ", "")
+        L += [f"      {ct} v_; " + ("v_.bits = 0;" if es == 2 else f"v_ = ({ct})0;"),
+              f"      if (ok) v_ = ldg_raw((const {ct}*)(rowb + off));",
+              "      d[e] = v_;",
+              "    }"]
+    else:
+        L += [f"    const int x0 = cc * {epc} - {spec.hk(f) * f.nc};",
+              f"    const int elo = min(max(-tk0 * {f.nc} - x0, 0), {epc}), ehi = min(max((p.n2 - tk0) * {f.nc} - x0, 0), {epc});",
+              f"    *(uint4*)d_ = keep_bytes16(*(const uint4*)d_, (u32)elo * {es}u, (u32)ehi * {es}u);"]
+    L += ["  }", "};"]
     return L
 
 
@@ -1773,7 +1781,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         zexpr = ("(q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q" if ghost and spec.i_periodic else "q")
         if staged:
             K.append("  if (tid == 0) {")
-            K.append("    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], 1);")
+            # with row-staged fields every warp arrives once per plane (its rows' copies)
+            K.append(f"    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], {'NT / 32' if lsu_fields else '1'});")
             K.append("    fence_mbar_init();")
             for ti in range(len(tmaps)):
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
@@ -1786,56 +1795,63 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             K.append("  auto request = [&](int q) {")
             K.append("    const int s = (q - p_first) % NSLOT;")
             K.append(f"    const int zq = {zexpr};")
-            K.append("    if (tid < 32) {")
-            if lsu_fields:
-                # warp 0 sizes the row copies first: the slot's barrier expects every byte
-                K.append("      const bool zok = zq >= 0 && zq < p.nl;")
-                K.append("      u32 tot_ = 0u;")
-                for f in lsu_fields:
-                    K += ["      " + x for x in _rs_request(spec, f, cfg, ghost, rings, "size")]
-                K.append("      tot_ = __reduce_add_sync(0xffffffffu, tot_);")
-            if lsu_fields:
-                # the lanes that issue copies order this CTA's earlier generic writes of
-                # the slot (the previous plane's shift) before them
-                K.append("      fence_proxy_async();")
-            K.append("      if (tid == 0) {")
-            if not lsu_fields:
-                K.append("        fence_proxy_async();")
-            K.append(f"        unsigned int bytes_ = {tma_bytes}u{' + tot_' if lsu_fields else ''};")
-            for f in tma_fields:
-                (kw, kh), (jw, jh) = strip_boxes(spec, f)
-                es = ESIZE[f.dtype]
-                if f.wrap_k:
-                    K.append(f"        if (tk0 == 0) bytes_ += {kw * kh * es}u;")
-                    K.append(f"        if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
-                if f.wrap_j:
-                    K.append(f"        if (tj0 == 0) bytes_ += {jw * jh * es}u;")
-                    K.append(f"        if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
-            K.append("        mbar_arrive_expect_tx(&bars[s], bytes_);")
+            tma_issue = []
             for f in tma_fields:
                 base = f"smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}"
                 lay = slot_layout(spec, f)
                 hk = spec.hk(f)
-                K.append(f"        tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
-                         f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
+                tma_issue.append(f"tma_load_3d({base}, &p.tmap[{tidx[(f.slot, 'box')]}], &bars[s], "
+                                 f"(tk0 - {hk}) * {f.nc}, tj0 - {f.halo}, zq);")
                 if f.wrap_k:
                     ti = tidx[(f.slot, "kstrip")]
-                    K.append(f"        if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
-                             f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
-                    K.append(f"        if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
-                             f"0, tj0, zq);")
+                    tma_issue.append(f"if (tk0 == 0) tma_load_3d({base} + {lay['kl']}, &p.tmap[{ti}], &bars[s], "
+                                     f"(p.n2 - {hk}) * {f.nc}, tj0, zq);")
+                    tma_issue.append(f"if (tk0 + TK >= p.n2) tma_load_3d({base} + {lay['kr']}, &p.tmap[{ti}], &bars[s], "
+                                     f"0, tj0, zq);")
                 if f.wrap_j:
                     ti = tidx[(f.slot, "jstrip")]
-                    K.append(f"        if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
-                             f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
-                    K.append(f"        if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
-                             f"(tk0 - {hk}) * {f.nc}, 0, zq);")
-            K.append("      }")
+                    tma_issue.append(f"if (tj0 == 0) tma_load_3d({base} + {lay['jt']}, &p.tmap[{ti}], &bars[s], "
+                                     f"(tk0 - {hk}) * {f.nc}, p.n1 - {f.halo}, zq);")
+                    tma_issue.append(f"if (tj0 + TJ >= p.n1) tma_load_3d({base} + {lay['jb']}, &p.tmap[{ti}], &bars[s], "
+                                     f"(tk0 - {hk}) * {f.nc}, 0, zq);")
+            tma_size = []
+            for f in tma_fields:
+                (kw, kh), (jw, jh) = strip_boxes(spec, f)
+                es = ESIZE[f.dtype]
+                if f.wrap_k:
+                    tma_size.append(f"if (tk0 == 0) bytes_ += {kw * kh * es}u;")
+                    tma_size.append(f"if (tk0 + TK >= p.n2) bytes_ += {kw * kh * es}u;")
+                if f.wrap_j:
+                    tma_size.append(f"if (tj0 == 0) bytes_ += {jw * jh * es}u;")
+                    tma_size.append(f"if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
             if lsu_fields:
-                K.append("      __syncwarp();")
+                # every warp sizes the copies of its rows, arrives once with their bytes
+                # (warp 0 also with the TMA boxes), then its lanes issue them
+                K.append("    const bool zok = zq >= 0 && zq < p.nl;")
+                K.append("    u32 tot_ = 0u;")
                 for f in lsu_fields:
-                    K += ["      " + x for x in _rs_request(spec, f, cfg, ghost, rings, "issue")]
-            K.append("    }")
+                    K += ["    " + x for x in _rs_request(spec, f, cfg, ghost, rings, "size")]
+                K.append("    tot_ = __reduce_add_sync(0xffffffffu, tot_);")
+                K.append("    fence_proxy_async();   // this CTA's earlier generic writes of the slot come first")
+                K.append("    if ((tid & 31) == 0) {")
+                K.append("      unsigned int bytes_ = tot_;")
+                if tma_fields:
+                    K.append(f"      if (tid == 0) {{ bytes_ += {tma_bytes}u; " + " ".join(tma_size) + " }")
+                K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
+                if tma_fields:
+                    K.append("      if (tid == 0) { " + " ".join(tma_issue) + " }")
+                K.append("    }")
+                K.append("    __syncwarp();")
+                for f in lsu_fields:
+                    K += ["    " + x for x in _rs_request(spec, f, cfg, ghost, rings, "issue")]
+            else:
+                K.append("    if (tid == 0) {")
+                K.append("      fence_proxy_async();")
+                K.append(f"      unsigned int bytes_ = {tma_bytes}u;")
+                K += ["      " + x for x in tma_size]
+                K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
+                K += ["      " + x for x in tma_issue]
+                K.append("    }")
             K.append("  };")
             if lsu_fields:
                 K.append("  // plane q resident: its row-staged fields shifted into place (published by the")

@@ -226,6 +226,18 @@ template <int ES> STEN_DEV uint4 shifted16(const unsigned char* src, u32 sh) {
   return make_uint4(__funnelshift_r(y[0], y[1], bs), __funnelshift_r(y[1], y[2], bs),
                     __funnelshift_r(y[2], y[3], bs), __funnelshift_r(y[3], y[4], bs));
 }
+// The 16 bytes of v with bytes outside [lo, hi) zeroed.
+STEN_DEV uint4 keep_bytes16(uint4 v, u32 lo, u32 hi) {
+  u32 w[4] = {v.x, v.y, v.z, v.w};
+  #pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int l = min(max((int)lo - 4 * i, 0), 4), h = min(max((int)hi - 4 * i, 0), 4);
+    const u32 below_h = h >= 4 ? 0xffffffffu : ((1u << (8 * h)) - 1u);
+    const u32 below_l = l >= 4 ? 0xffffffffu : ((1u << (8 * l)) - 1u);
+    w[i] &= below_h & ~below_l;
+  }
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
 // Untiled bulk copy of `bytes` (a multiple of 16) from the 16-byte aligned global
 // address gsrc to the 16-byte aligned shared address sdst; completion counted on `bar`.
 STEN_DEV void bulk_load(u32 sdst, const void* gsrc, u32 bytes, u64* bar) {

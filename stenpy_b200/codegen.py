@@ -1270,8 +1270,9 @@ def rs_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[in
     """Row staging of a field whose rows TMA cannot describe: (box width w and height h
     in elements, element size es, box row bytes RB (a multiple of 16), 16-byte chunks
     C per box row, ring row pitch SR = RB + 16 bytes, box rows per warp, chunks per
-    thread). Box row r is bulk-copied into ring row r as the 16-byte units that cover
-    it; warp r % (NT / 32) then shifts it into place, 32 chunks at a time."""
+    thread). Box row r lands in ring row r as the C + 1 16-byte units that cover it
+    (unit q of the slot, q = r (C + 1) + u, copied by thread q % NT); warp
+    r % (NT / 32) then shifts it into place, 32 chunks at a time."""
     w, h = spec.box(f)
     es = ESIZE[f.dtype]
     rb = w * es
@@ -1282,23 +1283,41 @@ def rs_geometry(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[in
     return w, h, es, rb, c, rb + 16, rpw, -(-(rpw * c) // 32)
 
 
+def rs_units(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[int, int]:
+    """(16-byte copy units of one row-staged plane, units per thread)."""
+    _, h, _, _, c, _, _, _ = rs_geometry(spec, f, cfg)
+    return h * (c + 1), -(-(h * (c + 1)) // cfg.threads)
+
+
 def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -> List[str]:
-    """Per-thread chunk table of a row-staged field, fixed for the whole march (one
-    word per chunk: its 16-byte unit in the ring slot, the row's byte offset mod 16,
-    and flags: chunk exists / row inside the grid / chunk crosses a dim-2 face). Warp
-    v owns box rows v,
-    v + NT/32, ...; its lanes take that list's chunks in order, 32 at a time."""
+    """Per-thread tables of a row-staged field, fixed for the whole march. Copy units:
+    for unit q = tid + i NT (unit u of box row r), its byte offset from a plane's start
+    (row start at column tk0 - hk, plus 16 u; the rows' dim-1 rule applied) and a bit
+    for rows inside the grid. Shift chunks: one word per chunk — its 16-byte unit in
+    the ring slot, the row's byte offset mod 16, and flags: chunk exists / row inside
+    the grid / chunk crosses a dim-2 face. Warp v owns box rows v, v + NT/32, ...; its
+    lanes take that list's chunks in order, 32 at a time."""
     sl = f.slot
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
+    units, nu = rs_units(spec, f, cfg)
     epc = 16 // es
     hkn = spec.hk(f) * f.nc
     rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-    L = [f"// row staging of field {sl}: {h} box rows of {c} chunks, {ni} chunks per thread",
+    L = [f"// row staging of field {sl}: {h} box rows of {c} chunks; {nu} copy units and {ni} chunks per thread",
          f"const u32 rsB{sl}_ = (u32)p.n2 * {f.nc * es}u;  // bytes of a grid row (mod 2^32)",
-         f"u32 rsit{sl}_[{ni}];",
-         f"#pragma unroll\nfor (int i = 0; i < {ni}; ++i) {{",
-         f"  const int ix = i * 32 + (tid & 31), m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
+         f"int rsw{sl}_[{nu}];",
+         f"u32 rsok{sl}_ = 0u;",
+         f"#pragma unroll\nfor (int i = 0; i < {nu}; ++i) {{",
+         f"  const int q = tid + i * NT, r = q / {c + 1}, u = q - r * {c + 1};",
          f"  int jg = tj0 - {f.halo} + r;"]
+    L += _remap_line("jg", "p.n1", rj, "  ")
+    L += [f"  rsw{sl}_[i] = (int)((u32)jg * rsB{sl}_ + (u32)((tk0 - {spec.hk(f)}) * {f.nc * es}) + 16u * (u32)u);",
+          f"  if (q < {units} && jg >= 0 && jg < p.n1) rsok{sl}_ |= 1u << i;",
+          "}",
+          f"u32 rsit{sl}_[{ni}];",
+          f"#pragma unroll\nfor (int i = 0; i < {ni}; ++i) {{",
+          f"  const int ix = i * 32 + (tid & 31), m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
+          f"  int jg = tj0 - {f.halo} + r;"]
     L += _remap_line("jg", "p.n1", rj, "  ")
     L += [f"  const int x0 = cc * {epc} - {hkn};  // box element of the chunk's first element, from column tk0",
           f"  const bool kx = x0 < -tk0 * {f.nc} || x0 + {epc} > (p.n2 - tk0) * {f.nc};",
@@ -1308,31 +1327,28 @@ def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -
     return L
 
 
-def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool, rings: Dict[int, int],
-                phase: str) -> List[str]:
-    """Request of plane ``zq`` into ring slot ``s``, warp v for box rows v, v + NT/32, ...
-    (one lane per row): the 16-byte units covering the row — remapped by the dim-1
-    rule, none outside the grid — less those that do not overlap the field, as one
-    bulk copy onto the slot's barrier. ``phase`` "size" adds the bytes to ``tot_``;
-    "issue" copies."""
+def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[int, int]) -> List[str]:
+    """Copies of plane ``zq`` into ring slot ``s`` by every thread, its units only: 16
+    bytes from the aligned address at or below the unit's offset from the plane
+    start; in the field's first and last planes, units outside the field are zero."""
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
+    units, nu = rs_units(spec, f, cfg)
     sl = f.slot
-    rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
-    L = [f"#pragma unroll 1\nfor (int r = (tid >> 5) + (tid & 31) * (NT / 32); r < {h}; r += NT) {{",
-         f"  int jg = tj0 - {f.halo} + r;"]
-    L += _remap_line("jg", "p.n1", rj, "  ")
-    L += [f"  if (zok && jg >= 0 && jg < p.n1) {{",
-          f"    const unsigned long long fb_ = (unsigned long long)p.fld[{sl}];",
-          f"    const unsigned long long fe_ = fb_ + (unsigned long long)p.nl * p.n1 * p.n2 * {f.nc * es}ull;",
-          f"    const long long e0 = ((long long)zq * p.n1 + jg) * ((long long)p.n2 * {f.nc})"
-          f" + (long long)(tk0 - {spec.hk(f)}) * {f.nc};",
-          f"    const unsigned long long a0 = fb_ + (unsigned long long)(e0 * {es}), al = a0 & ~15ull;",
-          f"    const unsigned long long s_ = max(al, fb_ & ~15ull), e_ = min((a0 + {rb + 15}ull) & ~15ull, (fe_ + 15ull) & ~15ull);"]
-    if phase == "size":
-        L.append("    if (e_ > s_) tot_ += (u32)(e_ - s_);")
-    else:
-        L.append(f"    if (e_ > s_) bulk_load(smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)} + r * {sr})"
-                 f" + (u32)(s_ - al), (const void*)s_, (u32)(e_ - s_), &bars[s]);")
+    L = ["if (zok) {",
+         f"  const unsigned long long fb_ = (unsigned long long)p.fld[{sl}];",
+         f"  const unsigned long long bz_ = fb_ + (unsigned long long)zq * p.n1 * rsB{sl}_;   // plane start",
+         f"  const u32 dst_ = smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}) + (u32)tid * 16u;",
+         "  if (zq > 0 && zq < p.nl - 1) {   // every unit lies inside the field"]
+    for i in range(nu):
+        L.append(f"    if (rsok{sl}_ & {1 << i}u) {{ const int w_ = rsw{sl}_[{i}];"
+                 f" cp_async16_cg(dst_ + {i * cfg.threads * 16}u, (const void*)(bz_ + (long long)(w_ - (int)(((u32)bz_ + (u32)w_) & 15u))), 16u); }}")
+    L += ["  } else {",
+          f"    const unsigned long long lo_ = fb_ & ~15ull, hi_ = (fb_ + (unsigned long long)p.nl * p.n1 * rsB{sl}_ + 15ull) & ~15ull;"]
+    for i in range(nu):
+        L += [f"    if (rsok{sl}_ & {1 << i}u) {{ const int w_ = rsw{sl}_[{i}];",
+              f"      const unsigned long long g_ = bz_ + (long long)(w_ - (int)(((u32)bz_ + (u32)w_) & 15u));",
+              f"      const bool in_ = g_ >= lo_ && g_ < hi_;",
+              f"      cp_async16_cg(dst_ + {i * cfg.threads * 16}u, (const void*)(in_ ? g_ : lo_), in_ ? 16u : 0u); }}"]
     L += ["  }", "}"]
     return L
 
@@ -1343,9 +1359,11 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
     chunk becomes the 16 bytes that start ``shift`` bytes into it (the row's byte
     offset mod 16), in place — a warp loads all its chunks of an iteration before it
     stores any, and a row's chunks go in order — zero for rows outside the grid.
-    Elements of chunks at a dim-2 face that lie outside the grid are zeroed, or, under
-    a dim-2 rule that copies values, fetched by that rule from global memory (one loop
-    after the shift keeps that code out of the unrolled chunks)."""
+    Elements of chunks at a dim-2 face that lie outside the grid are then fetched from
+    global memory under a dim-2 rule that copies values, or zeroed under the zero rule
+    (one loop after the shift keeps that code out of the unrolled chunks); otherwise
+    they stay as copied: they feed only voxels that are not kept, or ghost layers that
+    the ghost fill writes."""
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     sl = f.slot
     ct = CTYPE[f.dtype]
@@ -1353,13 +1371,17 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
     rj = (spec.ghosts or {}).get((f.slot, 1)) if ghost else None
     rk = (spec.ghosts or {}).get((f.slot, 2)) if ghost else None
     gather = rk in _REMAP_RULES
+    # without a dim-2 rule that copies values or asks for zeros, columns outside the
+    # grid feed only voxels that are not kept (and ghost layers the ghost fill writes)
+    face = gather or rk == "zero"
     L = [f"auto rs_shift{sl} = [&](int q) {{",
          f"  const int zq = {zexpr};",
          "  const bool zok_ = zq >= 0 && zq < p.nl;",
          f"  const u32 sz_ = (u32)(unsigned long long)p.fld[{sl}] + (u32)zq * ((u32)p.n1 * rsB{sl}_)"
          f" + (u32)((tk0 - {spec.hk(f)}) * {f.nc * es});",
-         f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((q - p_first) % NSLOT) * {plane_bytes(spec, f)};",
-         "  u32 kx_ = 0u;   // chunks at a dim-2 face"]
+         f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((q - p_first) % NSLOT) * {plane_bytes(spec, f)};"]
+    if face:
+        L.append("  u32 kx_ = 0u;   // chunks at a dim-2 face")
     for i in range(ni):
         L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
               f"    unsigned char* d_ = slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4);",
@@ -1367,9 +1389,13 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
               "    uint4 v_ = make_uint4(0u, 0u, 0u, 0u);",
               f"    if (cp_) v_ = shifted16<{es}>(d_, (sz_ + (m_ >> {RS_SHIFT})) & 15u);",
               "    __syncwarp();   // every lane has read the chunks it needs before any is overwritten",
-              f"    if (m_ & {RS_VALID}u) *(uint4*)d_ = v_;",
-              f"    if (cp_ && (m_ & {RS_KX}u)) kx_ |= {1 << i}u;",
-              "  }"]
+              f"    if (m_ & {RS_VALID}u) *(uint4*)d_ = v_;"]
+        if face:
+            L.append(f"    if (cp_ && (m_ & {RS_KX}u)) kx_ |= {1 << i}u;")
+        L.append("  }")
+    if not face:
+        L.append("};")
+        return L
     L += ["  #pragma unroll 1",
           "  for (; kx_ != 0u; kx_ &= kx_ - 1u) {",
           "    const int ix = (__ffs(kx_) - 1) * 32 + (tid & 31);",
@@ -1781,8 +1807,10 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         zexpr = ("(q < 0 || q >= p.nl) ? sten_plane(p, q + p.i_base) : q" if ghost and spec.i_periodic else "q")
         if staged:
             K.append("  if (tid == 0) {")
-            # with row-staged fields every warp arrives once per plane (its rows' copies)
-            K.append(f"    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], {'NT / 32' if lsu_fields else '1'});")
+            # with row-staged fields every thread arrives once per plane (its copies),
+            # thread 0 once more with the TMA boxes
+            cnt = ("NT + 1" if tma_fields else "NT") if lsu_fields else "1"
+            K.append(f"    for (int s = 0; s < NSLOT; ++s) mbar_init(&bars[s], {cnt});")
             K.append("    fence_mbar_init();")
             for ti in range(len(tmaps)):
                 K.append(f"    tma_prefetch_desc(&p.tmap[{ti}]);")
@@ -1825,25 +1853,20 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                     tma_size.append(f"if (tj0 == 0) bytes_ += {jw * jh * es}u;")
                     tma_size.append(f"if (tj0 + TJ >= p.n1) bytes_ += {jw * jh * es}u;")
             if lsu_fields:
-                # every warp sizes the copies of its rows, arrives once with their bytes
-                # (warp 0 also with the TMA boxes), then its lanes issue them
+                # every thread copies its units and arrives once they landed; thread 0
+                # also arrives with the TMA boxes' bytes
                 K.append("    const bool zok = zq >= 0 && zq < p.nl;")
-                K.append("    u32 tot_ = 0u;")
                 for f in lsu_fields:
-                    K += ["    " + x for x in _rs_request(spec, f, cfg, ghost, rings, "size")]
-                K.append("    tot_ = __reduce_add_sync(0xffffffffu, tot_);")
-                K.append("    fence_proxy_async();   // this CTA's earlier generic writes of the slot come first")
-                K.append("    if ((tid & 31) == 0) {")
-                K.append("      unsigned int bytes_ = tot_;")
+                    K += ["    " + x for x in _rs_request(spec, f, cfg, rings)]
+                K.append("    cp_async_mbar_arrive(&bars[s]);")
                 if tma_fields:
-                    K.append(f"      if (tid == 0) {{ bytes_ += {tma_bytes}u; " + " ".join(tma_size) + " }")
-                K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
-                if tma_fields:
-                    K.append("      if (tid == 0) { " + " ".join(tma_issue) + " }")
-                K.append("    }")
-                K.append("    __syncwarp();")
-                for f in lsu_fields:
-                    K += ["    " + x for x in _rs_request(spec, f, cfg, ghost, rings, "issue")]
+                    K.append("    if (tid == 0) {")
+                    K.append("      fence_proxy_async();")
+                    K.append(f"      unsigned int bytes_ = {tma_bytes}u;")
+                    K += ["      " + x for x in tma_size]
+                    K.append("      mbar_arrive_expect_tx(&bars[s], bytes_);")
+                    K += ["      " + x for x in tma_issue]
+                    K.append("    }")
             else:
                 K.append("    if (tid == 0) {")
                 K.append("      fence_proxy_async();")

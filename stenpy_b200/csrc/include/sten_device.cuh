@@ -238,6 +238,16 @@ STEN_DEV uint4 keep_bytes16(uint4 v, u32 lo, u32 hi) {
   }
   return make_uint4(w[0], w[1], w[2], w[3]);
 }
+// 16-byte asynchronous global->shared copy (L2 only) of which the first src_bytes
+// (16 or 0) come from gsrc, the rest zero; completion tracked by cp_async_mbar_arrive.
+STEN_DEV void cp_async16_cg(u32 sdst, const void* gsrc, u32 src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" :: "r"(sdst), "l"(gsrc), "r"(src_bytes) : "memory");
+}
+// One arrival on `bar` once every cp.async this thread issued so far has completed
+// (the barrier's expected count includes it).
+STEN_DEV void cp_async_mbar_arrive(u64* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
 // Untiled bulk copy of `bytes` (a multiple of 16) from the 16-byte aligned global
 // address gsrc to the 16-byte aligned shared address sdst; completion counted on `bar`.
 STEN_DEV void bulk_load(u32 sdst, const void* gsrc, u32 bytes, u64* bar) {

@@ -433,6 +433,10 @@ class Planner:
             es = ESIZE[f.dtype]
             f.tma = (n2 * f.nc * es) % 16 == 0 and (w * es) % 16 == 0 and w <= 256 and h <= 256
             f.staged = f.tma or f.slot in offset_read
+            if f.staged and not f.tma and self.shape[1] * n2 * f.nc * es + 4 * w * es >= 1 << 31:
+                # row staging addresses a unit by its 32-bit offset from the plane start
+                raise FusionError(f"a plane of {self.shape[1]} x {n2} rows too large to row-stage "
+                                  f"({n2 * f.nc * es} B rows are not 16-byte multiples)")
             if radius == 0 and not has_scan:
                 f.tma = f.staged = False     # flat pass: vector loads straight from HBM
         if self.ghosts:

@@ -430,13 +430,14 @@ def test_2d_fields_plan_as_one_plane_grids():
 
 
 def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
-    """Host model of the row staging of one plane (the generated request and in-place
+    """Host model of the row staging of one plane (the generated copies and in-place
     shift, formula for formula, on a one-plane field starting at byte ``fb``): returns
-    {box element: global element, or None for zero}, checking that every bulk copy is
-    16-byte aligned, fits its ring row and reads only 16-byte units that overlap the
-    field; that a warp reads all chunks of an iteration before it writes any, with
-    every read inside its row; and that no element takes a byte that was not copied
-    from the field."""
+    {box element: global element, None for zero, or "free" for a column outside the
+    grid that no rule asks for}, checking that every copy unit is 16-byte aligned,
+    lies in the ring slot and reads only 16-byte units that overlap the field; that a
+    warp reads all chunks of an iteration before it writes any, with every read inside
+    its row; and that no other element takes a byte that was not copied from the
+    field."""
     from stenpy_b200.codegen import ESIZE, rs_geometry
     es, nc = ESIZE[f.dtype], f.nc
     hk = spec.hk(f)
@@ -459,22 +460,22 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
         return x
 
     slot = [None] * (h * sr)               # ring slot byte -> global byte ("outside": not the field)
-    for r in range(h):                      # request: one bulk copy per box row inside the grid
+    lo, hi = fb - fb % 16, (fe + 15) // 16 * 16
+    for q in range(h * (c + 1)):            # request: unit q of the slot, one 16-byte copy
+        r, u = divmod(q, c + 1)
         jg = remap(tj0 - f.halo + r, n1, rj)
         if not 0 <= jg < n1:
             continue
         a0 = fb + ((jg * n2 + (tk0 - hk)) * nc) * es
-        al = a0 - a0 % 16
-        s_ = max(al, fb - fb % 16)
-        e_ = min((a0 + rb + 15) // 16 * 16, (fe + 15) // 16 * 16)
-        if e_ <= s_:
-            continue
-        assert s_ % 16 == 0 and e_ % 16 == 0
-        assert e_ - al <= sr, "copy fits the ring row"
-        for u in range(s_, e_, 16):
-            assert u < fe and u + 16 > fb, "a copied unit overlaps the field"
-        for g in range(s_, e_):
-            slot[r * sr + (g - al)] = g if fb <= g < fe else "outside"
+        g = a0 - a0 % 16 + 16 * u
+        assert g % 16 == 0 and 16 * q + 16 <= h * sr
+        if lo <= g < hi:                    # a unit that overlaps the field (first/last plane check)
+            assert g < fe and g + 16 > fb
+            for t in range(16):
+                slot[16 * q + t] = g + t if fb <= g + t < fe else "outside"
+        else:
+            for t in range(16):
+                slot[16 * q + t] = "zero-filled"
 
     sz = fb + (tk0 - hk) * nc * es            # plane 0
     fixes = []
@@ -514,6 +515,9 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
             kg = tk0 + xr // nc
             if 0 <= kg < n2:
                 continue
+            if rk not in ("periodic", "replicate", "reflect", "zero"):
+                fixed[r * w + cc * epc + e] = "free"      # as copied: feeds no kept voxel
+                continue
             ccomp = xr - (kg - tk0) * nc
             kg = remap(kg, n2, rk)
             okk = 0 <= kg < n2
@@ -538,7 +542,7 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
 
 
 @pytest.mark.parametrize("es,nc", [(4, 1), (4, 3), (2, 1), (2, 3), (8, 1)])
-@pytest.mark.parametrize("rule", [None, "periodic", "replicate", "reflect"])
+@pytest.mark.parametrize("rule", [None, "periodic", "replicate", "reflect", "zero"])
 def test_row_staging_covers_every_box_element_once(es, nc, rule):
     """Row staging (fields whose rows TMA cannot describe): every element of a staged
     box is written exactly once — with the element its axis rules map it to, or zero
@@ -572,6 +576,8 @@ def test_row_staging_covers_every_box_element_once(es, nc, rule):
                         got = _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rule, rule, nt, fb)
                         assert len(got) == w * h
                         for dst, g in got.items():
+                            if g == "free":
+                                continue
                             r, x = divmod(dst, w)
                             xr = x - hk * nc
                             kg, c = tk0 + xr // nc, xr % nc

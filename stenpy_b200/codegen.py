@@ -892,6 +892,10 @@ def slot_layout(spec: PassSpec, f: FieldSpec) -> Dict[str, int]:
     es = ESIZE[f.dtype]
     off = {"box": 0}
     o = _a128(ring_w(spec, f) * h * es)
+    rule, ns = rs_strip(spec, f)
+    if rule:                              # row-staged dim-2 strips: 2 faces x box rows
+        off["rs_strip"] = ring_w(spec, f) * h * es
+        o = _a128(off["rs_strip"] + 2 * h * ns * 16)
     (kw, kh), (jw, jh) = strip_boxes(spec, f)
     if f.wrap_k:
         off["kl"], off["kr"] = o, o + _a128(kw * kh * es)
@@ -1289,6 +1293,28 @@ def rs_units(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig") -> Tuple[int, 
     return h * (c + 1), -(-(h * (c + 1)) // cfg.threads)
 
 
+def rs_strip(spec: "PassSpec", f: "FieldSpec") -> Tuple[Optional[str], int]:
+    """(dim-2 rule that copies values across a dim-2 face, or None; 16-byte units per
+    strip). Under such a rule a tile at a dim-2 face copies, per box row and face, the
+    ``halo`` grid columns its ghost layers take their values from (a strip) next to
+    the plane; the shift fills the ghost layers from it."""
+    rk = (spec.ghosts or {}).get((f.slot, 2))
+    if f.tma or rk not in _REMAP_RULES or f.halo == 0:
+        return None, 0
+    es = ESIZE[f.dtype]
+    return rk, -(-(16 - es + f.halo * f.nc * es) // 16)
+
+
+def _rs_window(rule: str, side: int, halo: int) -> str:
+    """First grid column of the strip of face ``side`` (0: column 0, 1: column n2 - 1)
+    under ``rule``: the columns [ws, ws + halo) hold every column the rule maps the
+    ghost layers to."""
+    ws = {("periodic", 0): f"p.n2 - {halo}", ("periodic", 1): "0",
+          ("replicate", 0): "0", ("replicate", 1): f"p.n2 - {halo}",
+          ("reflect", 0): "1", ("reflect", 1): f"p.n2 - 1 - {halo}"}[(rule, side)]
+    return f"min(max({ws}, 0), max(p.n2 - {halo}, 0))"
+
+
 def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -> List[str]:
     """Per-thread tables of a row-staged field, fixed for the whole march. Copy units:
     for unit q = tid + i NT (unit u of box row r), its byte offset from a plane's start
@@ -1330,7 +1356,8 @@ def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -
 def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[int, int]) -> List[str]:
     """Copies of plane ``zq`` into ring slot ``s`` by every thread, its units only: 16
     bytes from the aligned address at or below the unit's offset from the plane
-    start; in the field's first and last planes, units outside the field are zero."""
+    start; in the field's first and last planes, units outside the field are zero.
+    Under a dim-2 rule that copies values, tiles at a dim-2 face also copy strips."""
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     units, nu = rs_units(spec, f, cfg)
     sl = f.slot
@@ -1349,7 +1376,29 @@ def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict
               f"      const unsigned long long g_ = bz_ + (long long)(w_ - (int)(((u32)bz_ + (u32)w_) & 15u));",
               f"      const bool in_ = g_ >= lo_ && g_ < hi_;",
               f"      cp_async16_cg(dst_ + {i * cfg.threads * 16}u, (const void*)(in_ ? g_ : lo_), in_ ? 16u : 0u); }}"]
-    L += ["  }", "}"]
+    L.append("  }")
+    rule, ns = rs_strip(spec, f)
+    if rule:
+        # tiles at a dim-2 face: per box row and face, the strip of grid columns the
+        # ghost layers map to (only the units that hold its bytes)
+        hb = f.halo * f.nc * es
+        lay = slot_layout(spec, f)
+        rj = (spec.ghosts or {}).get((f.slot, 1))
+        L += [f"  if (tk0 == 0 || tk0 + TK + {spec.hk(f)} > p.n2) {{",
+              f"    const u32 sdst_ = smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)} + {lay['rs_strip']});",
+              f"    #pragma unroll 1\n    for (int t = tid; t < {2 * h * ns}; t += NT) {{",
+              f"      const int rs2 = t / {ns}, sd = rs2 & 1, r = rs2 >> 1, u = t - rs2 * {ns};",
+              f"      if (sd == 0 ? tk0 != 0 : tk0 + TK + {spec.hk(f)} <= p.n2) continue;",
+              f"      int jg = tj0 - {f.halo} + r;"]
+        L += _remap_line("jg", "p.n1", rj, "      ")
+        L += ["      if (jg < 0 || jg >= p.n1) continue;",
+              f"      const int ws = sd ? {_rs_window(rule, 1, f.halo)} : {_rs_window(rule, 0, f.halo)};",
+              f"      const unsigned long long g0 = bz_ + (unsigned long long)((long long)jg * rsB{sl}_ + (long long)ws * {f.nc * es});",
+              "      const unsigned long long al = g0 & ~15ull;",
+              f"      if ((u32)(g0 - al) + {hb}u > 16u * (u32)u) cp_async16_cg(sdst_ + (u32)t * 16u, (const void*)(al + 16ull * u), 16u);",
+              "    }",
+              "  }"]
+    L.append("}")
     return L
 
 
@@ -1357,8 +1406,8 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
               zexpr: str) -> List[str]:
     """``rs_shift{slot}(q)``, once plane q's copies landed in its ring slot: each ring
     chunk becomes the 16 bytes that start ``shift`` bytes into it (the row's byte
-    offset mod 16), in place — a warp loads all its chunks of an iteration before it
-    stores any, and a row's chunks go in order — zero for rows outside the grid.
+    offset mod 16), in place — a warp reads all its chunks before it writes any (a
+    warp's rows are its own) — zero for rows outside the grid.
     Elements of chunks at a dim-2 face that lie outside the grid are then fetched from
     global memory under a dim-2 rule that copies values, or zeroed under the zero rule
     (one loop after the shift keeps that code out of the unrolled chunks); otherwise
@@ -1382,16 +1431,21 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
          f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((q - p_first) % NSLOT) * {plane_bytes(spec, f)};"]
     if face:
         L.append("  u32 kx_ = 0u;   // chunks at a dim-2 face")
+    # every chunk of this thread is read before any is written (one warp barrier):
+    # a chunk's second unit is the next chunk's first, written by the next lane
+    L.append(f"  uint4 v_[{ni}];")
     for i in range(ni):
         L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
-              f"    unsigned char* d_ = slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4);",
-              f"    const bool cp_ = zok_ && (m_ & {RS_ROWOK}u);",
-              "    uint4 v_ = make_uint4(0u, 0u, 0u, 0u);",
-              f"    if (cp_) v_ = shifted16<{es}>(d_, (sz_ + (m_ >> {RS_SHIFT})) & 15u);",
-              "    __syncwarp();   // every lane has read the chunks it needs before any is overwritten",
-              f"    if (m_ & {RS_VALID}u) *(uint4*)d_ = v_;"]
+              f"    v_[{i}] = make_uint4(0u, 0u, 0u, 0u);",
+              f"    if (zok_ && (m_ & {RS_ROWOK}u))",
+              f"      v_[{i}] = shifted16<{es}>(slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4), (sz_ + (m_ >> {RS_SHIFT})) & 15u);",
+              "  }"]
+    L.append("  __syncwarp();")
+    for i in range(ni):
+        L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
+              f"    if (m_ & {RS_VALID}u) *(uint4*)(slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4)) = v_[{i}];"]
         if face:
-            L.append(f"    if (cp_ && (m_ & {RS_KX}u)) kx_ |= {1 << i}u;")
+            L.append(f"    if (zok_ && (m_ & {RS_ROWOK}u) && (m_ & {RS_KX}u)) kx_ |= {1 << i}u;")
         L.append("  }")
     if not face:
         L.append("};")
@@ -1402,17 +1456,28 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
           f"    const int m = ix / {c}, cc = ix - m * {c}, r = (tid >> 5) + m * (NT / 32);",
           f"    unsigned char* d_ = slot_ + r * {sr} + cc * 16;"]
     if gather:
+        # ghost layers only (columns within halo of a face): from the strip, or from
+        # global memory where the rule leaves the strip (grids narrower than 2 halo)
+        _, ns = rs_strip(spec, f)
+        lay = slot_layout(spec, f)
         L += [f"    int jg = tj0 - {f.halo} + r;"]
         L += _remap_line("jg", "p.n1", rj, "    ")
         L += [f"    const char* rowb = (const char*)p.fld[{sl}] + ((size_t)zq * p.n1 + jg) * ((size_t)p.n2 * {f.nc * es});",
+              f"    const u32 rlo_ = (u32)(unsigned long long)rowb;",
               f"    {ct}* d = ({ct}*)d_;",
               f"    #pragma unroll 1\n    for (int e = 0; e < {epc}; ++e) {{",
               f"      const int x0_ = cc * {epc} + e - {spec.hk(f) * f.nc};",
               f"      const int k0_ = tk0 + (x0_ >= 0 ? x0_ / {f.nc} : -((-x0_ + {f.nc - 1}) / {f.nc}));",
-              "      if (k0_ >= 0 && k0_ < p.n2) continue;   // inside the grid: the shifted copy holds it"]
-        L += _lsu_elem(spec, f, f"cc * {epc} + e", rk, "      ", "")
-        L += [f"      {ct} v_; " + ("v_.bits = 0;" if es == 2 else f"v_ = ({ct})0;"),
-              f"      if (ok) v_ = ldg_raw((const {ct}*)(rowb + off));",
+              f"      if ((k0_ >= 0 && k0_ < p.n2) || k0_ < -{f.halo} || k0_ >= p.n2 + {f.halo}) continue;",
+              f"      const int cm = x0_ - (k0_ - tk0) * {f.nc}, sd = k0_ < 0 ? 0 : 1;",
+              "      int kr = k0_;"]
+        L += _remap_line("kr", "p.n2", rk, "      ")
+        L += [f"      const int ws = sd ? {_rs_window(rk, 1, f.halo)} : {_rs_window(rk, 0, f.halo)};",
+              f"      {ct} v_; " + ("v_.bits = 0;" if es == 2 else f"v_ = ({ct})0;"),
+              f"      if (kr >= ws && kr < ws + {f.halo}) {{",
+              f"        const u32 b_ = ((rlo_ + (u32)ws * {f.nc * es}u) & 15u) + (u32)(((kr - ws) * {f.nc} + cm) * {es});",
+              f"        v_ = *(const {ct}*)(slot_ + {lay['rs_strip']} + (r * 2 + sd) * {ns * 16} + b_);",
+              f"      }} else if (kr >= 0 && kr < p.n2) v_ = ldg_raw((const {ct}*)(rowb + (size_t)(kr * {f.nc} + cm) * {es}));",
               "      d[e] = v_;",
               "    }"]
     else:

@@ -435,7 +435,7 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
     {box element: global element, None for zero, or "free" for a column outside the
     grid that no rule asks for}, checking that every copy unit is 16-byte aligned,
     lies in the ring slot and reads only 16-byte units that overlap the field; that a
-    warp reads all chunks of an iteration before it writes any, with every read inside
+    warp reads all its chunks before it writes any, with every read inside
     its row; and that no other element takes a byte that was not copied from the
     field."""
     from stenpy_b200.codegen import ESIZE, rs_geometry
@@ -477,11 +477,37 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
             for t in range(16):
                 slot[16 * q + t] = "zero-filled"
 
+    gather = rk in ("periodic", "replicate", "reflect") and f.halo > 0
+    ns = -(-(16 - es + f.halo * nc * es) // 16)
+    strip = {}
+
+    def window(side):
+        ws = {("periodic", 0): n2 - f.halo, ("periodic", 1): 0, ("replicate", 0): 0,
+              ("replicate", 1): n2 - f.halo, ("reflect", 0): 1, ("reflect", 1): n2 - 1 - f.halo}[(rk, side)]
+        return min(max(ws, 0), max(n2 - f.halo, 0))
+
+    if gather:                              # strips of tiles at a dim-2 face
+        for r in range(h):
+            jg = remap(tj0 - f.halo + r, n1, rj)
+            if not 0 <= jg < n1:
+                continue
+            for sd in (0, 1):
+                if (sd == 0 and tk0 != 0) or (sd == 1 and tk0 + spec.cfg.tk + hk <= n2):
+                    continue
+                g0 = fb + (jg * n2 + window(sd)) * nc * es
+                al = g0 - g0 % 16
+                for u in range(ns):
+                    if g0 - al + f.halo * nc * es > 16 * u:
+                        assert lo <= al + 16 * u < hi
+                        for t in range(16):
+                            g = al + 16 * u + t
+                            strip[((2 * r + sd) * ns + u) * 16 + t] = g if fb <= g < fe else "outside"
+
     sz = fb + (tk0 - hk) * nc * es            # plane 0
     fixes = []
     for v in range(nw):                      # warps touch disjoint rows: one at a time
+        lanes = []
         for i in range(ni):
-            lanes = []
             for lane in range(32):
                 ix = i * 32 + lane
                 m, cc = divmod(ix, c)
@@ -501,8 +527,8 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
                 else:
                     val = [None] * 16
                 lanes.append((off, val))
-            for off, val in lanes:                             # ... before any lane writes
-                slot[off:off + 16] = val
+        for off, val in lanes:                                 # ... before any lane writes
+            slot[off:off + 16] = val
     zero = object()
     for r in range(h):                       # rows outside the grid were written as zeros
         if not 0 <= remap(tj0 - f.halo + r, n1, rj) < n1:
@@ -515,15 +541,25 @@ def _emulate_row_staging(spec, f, tk0, tj0, n1, n2, rj, rk, nt, fb=0):
             kg = tk0 + xr // nc
             if 0 <= kg < n2:
                 continue
-            if rk not in ("periodic", "replicate", "reflect", "zero"):
+            if rk == "zero":
+                fixed[r * w + cc * epc + e] = None
+                continue
+            if not gather or not -f.halo <= kg < n2 + f.halo:
                 fixed[r * w + cc * epc + e] = "free"      # as copied: feeds no kept voxel
                 continue
             ccomp = xr - (kg - tk0) * nc
-            kg = remap(kg, n2, rk)
-            okk = 0 <= kg < n2
-            if okk:
-                assert fb <= rowb + (kg * nc + ccomp) * es < fe
-            fixed[r * w + cc * epc + e] = (rowb + (kg * nc + ccomp) * es - fb) // es if okk else None
+            sd = 0 if kg < 0 else 1
+            kr = remap(kg, n2, rk)
+            ws = window(sd)
+            if ws <= kr < ws + f.halo:                    # from the strip
+                b0 = (rowb + ws * nc * es) % 16 + ((kr - ws) * nc + ccomp) * es
+                by = [strip[(2 * r + sd) * ns * 16 + b0 + t] for t in range(es)]
+                assert all(isinstance(x, int) for x in by) and all(by[t] == by[0] + t for t in range(es))
+                assert by[0] == rowb + (kr * nc + ccomp) * es
+                fixed[r * w + cc * epc + e] = (by[0] - fb) // es
+            else:
+                okk = 0 <= kr < n2
+                fixed[r * w + cc * epc + e] = (rowb + (kr * nc + ccomp) * es - fb) // es if okk else None
     out = {}
     for r in range(h):
         for x in range(w):

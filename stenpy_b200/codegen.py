@@ -302,11 +302,6 @@ def _lit(x: float) -> str:
 
 
 # ----------------------------------------------------------------------------- emitter
-# ops a pass may contain to evaluate two k-adjacent voxels at once in packed FP32
-PAIR_OPS = frozenset(("field", "scalar", "d1", "lap", "taps", "add", "sub", "mul", "mulk", "neg", "abs",
-                      "select", "stack", "trace", "norm"))
-
-
 class _Emitter:
     def __init__(self, spec: PassSpec):
         self.s = spec
@@ -328,15 +323,6 @@ class _Emitter:
         for n in self.g.nodes:
             if n.op in STENCIL_PRIMS and n.id in live:
                 self._mark(n.ins[0])
-        # passes of PAIR_OPS only round every operation explicitly (no contraction), in
-        # one-voxel and two-voxel code alike: the two give the same bits
-        self.explicit = (not self.flat and all(self.g.nodes[x].op in PAIR_OPS for x in live)
-                         and all(f.staged for f in spec.fields))
-        self.pair = False       # emitting the two-voxel (float2) form
-
-    @property
-    def V(self) -> str:
-        return "float2" if self.pair else "float"
 
     def _mark(self, nid: int) -> None:
         if nid in self.need_fn:
@@ -357,29 +343,6 @@ class _Emitter:
         def comp(arr, nid, c):
             return f"{arr}[{0 if g.nodes[nid].nc == 1 else c}]"
 
-        if self.explicit and op in ("add", "sub", "mul", "mulk", "neg", "abs", "trace", "norm"):
-            # explicitly rounded (the one- and two-voxel forms give the same bits)
-            if op in ("add", "sub", "mul"):
-                for c in range(n.nc):
-                    out.append(f"{o}[{c}] = s{op}({comp(ins[0], n.ins[0], c)}, {comp(ins[1], n.ins[1], c)});")
-            elif op == "mulk":
-                for c in range(n.nc):
-                    out.append(f"{o}[{c}] = smul({ins[0]}[{c}], {_lit(n.a('k'))});")
-            elif op in ("neg", "abs"):
-                for c in range(n.nc):
-                    out.append(f"{o}[{c}] = s{op}({ins[0]}[{c}]);")
-            elif op == "trace":
-                a = ins[0]
-                out.append(f"{o}[0] = sadd(sadd({a}[0], {a}[4]), {a}[8]);")
-            else:
-                a = ins[0]
-                nc_in = self.g.nodes[n.ins[0]].nc
-                acc = f"smul({a}[0], {a}[0])"
-                for c in range(1, nc_in):
-                    acc = f"sfma({a}[{c}], {a}[{c}], {acc})"
-                eps = n.a("eps")
-                out.append(f"{o}[0] = ssqrt({acc});" if eps is None else f"{o}[0] = sfmax(ssqrt({acc}), {_lit(eps)});")
-            return
         if op in ("add", "sub", "mul", "div"):
             a, b = ins
             for c in range(n.nc):
@@ -482,44 +445,31 @@ class _Emitter:
 
     # -- fast (interior) functions: template offsets
     def emit_fast_fns(self) -> None:
-        for pair in ((False, True) if self.explicit else (False,)):
-            self.pair = pair
-            for n in self.g.nodes:
-                if n.id not in self.need_fn:
-                    continue
-                body: List[str] = []
-                self.fast_value(n, "DI", "DJ", "DK", "o", body)
-                # FP: the same node at voxels DK and DK + 1 (packed FP32)
-                self.lines.append(f"template <int DI, int DJ, int DK> __device__ __forceinline__ void "
-                                  f"{'FP' if pair else 'FF'}{n.id}(const FCtx& x, {self.V}* o) {{")
-                self.lines += ["  " + b for b in body]
-                self.lines.append("}")
-        self.pair = False
+        for n in self.g.nodes:
+            if n.id not in self.need_fn:
+                continue
+            body: List[str] = []
+            self.fast_value(n, "DI", "DJ", "DK", "o", body)
+            self.lines.append(f"template <int DI, int DJ, int DK> __device__ __forceinline__ void "
+                              f"FF{n.id}(const FCtx& x, float* o) {{")
+            self.lines += ["  " + b for b in body]
+            self.lines.append("}")
 
     def fast_call(self, nid: int, di: str, dj: str, dk: str, body: List[str]) -> str:
         arr = self.t()
-        body.append(f"{self.V} {arr}[{self.g.nodes[nid].nc}];")
+        body.append(f"float {arr}[{self.g.nodes[nid].nc}];")
         n = self.g.nodes[nid]
         if n.op == "field":
             self.field_fast(n, di, dj, dk, arr, body)
         elif n.op == "scalar":
-            body.append(f"{arr}[0] = {self.scalar_val(n)};")
+            body.append(f"{arr}[0] = x.sc[{n.a('index')}];")
         else:
-            body.append(f"{'FP' if self.pair else 'FF'}{nid}<{di}, {dj}, {dk}>(x, {arr});")
+            body.append(f"FF{nid}<{di}, {dj}, {dk}>(x, {arr});")
         return arr
-
-    def scalar_val(self, n: PNode) -> str:
-        v = f"x.sc[{n.a('index')}]"
-        return f"f2s({v})" if self.pair else v
 
     def field_fast(self, n: PNode, di, dj, dk, arr, body):
         f = self.s.fields[n.a("field")]
-        if f.staged and self.pair:
-            # voxels k and k + 1: element (dk) * nc + c and the one nc further
-            for c in range(n.nc):
-                body.append(f"{arr}[{c}] = make_float2(LDF{f.slot}<{di}, {dj}, ({dk}) * {f.nc} + {c}>(x), "
-                            f"LDF{f.slot}<{di}, {dj}, (({dk}) + 1) * {f.nc} + {c}>(x));")
-        elif f.staged:
+        if f.staged:
             for c in range(n.nc):
                 body.append(f"{arr}[{c}] = LDF{f.slot}<{di}, {dj}, ({dk}) * {f.nc} + {c}>(x);")
         elif di != "0" or dj not in ("0", "M") or dk not in ("0", "KK"):
@@ -537,7 +487,7 @@ class _Emitter:
             self.field_fast(n, di, dj, dk, o, body)
             return
         if n.op == "scalar":
-            body.append(f"{o}[0] = {self.scalar_val(n)};")
+            body.append(f"{o}[0] = x.sc[{n.a('index')}];")
             return
         if n.op == "d1":
             ax = n.a("axis")
@@ -545,7 +495,7 @@ class _Emitter:
             mode = n.a("mode")
             if mode == "zero":
                 for c in range(n.nc):
-                    body.append(f"{o}[{c}] = {self.zero()};")
+                    body.append(f"{o}[{c}] = 0.0f;")
                 return
             off = [di, dj, dk]
             plus = list(off); plus[ax] = f"({off[ax]}) + 1"
@@ -555,11 +505,7 @@ class _Emitter:
             s = _lit(n.a("inv2h"))
             for c in range(n.nc):
                 cc = c if comp is None else comp
-                if self.explicit:
-                    d = f"ssub({a}[{cc}], {b}[{cc}])"
-                    body.append(f"{o}[{c}] = {d if n.a('inv2h') == 1.0 else f'smul({d}, {s})'};")
-                else:
-                    body.append(f"{o}[{c}] = ({a}[{cc}] - {b}[{cc}]) * {s};")
+                body.append(f"{o}[{c}] = ({a}[{cc}] - {b}[{cc}]) * {s};")
             return
         if n.op == "lap":
             off = [di, dj, dk]
@@ -572,15 +518,8 @@ class _Emitter:
                 b = self.fast_call(n.ins[0], *minus, body)
                 terms.append((a, b, _lit(n.a("invh2")[ax])))
             for c in range(n.nc):
-                if self.explicit:
-                    parts = []
-                    for (a, b, s), ax in zip(terms, range(3)):
-                        d = f"sfma(-2.0f, {ctr}[{c}], sadd({a}[{c}], {b}[{c}]))"
-                        parts.append(d if n.a("invh2")[ax] == 1.0 else f"smul({d}, {s})")
-                    body.append(f"{o}[{c}] = sadd(sadd({parts[0]}, {parts[1]}), {parts[2]});")
-                else:
-                    parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
-                    body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
+                parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
+                body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
             return
         if n.op == "taps":
             off = [di, dj, dk]
@@ -595,26 +534,8 @@ class _Emitter:
         ins = [self.fast_call(i, di, dj, dk, body) for i in n.ins]
         self.pointwise(n, ins, o, body)
 
-    def zero(self) -> str:
-        return "f2s(0.0f)" if self.pair else "0.0f"
-
     def _tap_sum(self, n: PNode, vals, o: str, body: List[str]) -> None:
         """o = scale * Σ w·v over (array, weight) pairs, accumulated in tap order."""
-        if self.explicit:
-            for c in range(n.nc):
-                acc = None
-                for arr, w in vals:
-                    if acc is None:
-                        acc = self.t()
-                        term = f"{arr}[{c}]" if w == 1.0 else f"smul({arr}[{c}], {_lit(w)})"
-                        body.append(f"{self.V} {acc} = {term};")
-                    elif w == 1.0:
-                        body.append(f"{acc} = sadd({acc}, {arr}[{c}]);")
-                    else:
-                        body.append(f"{acc} = sfma({arr}[{c}], {_lit(w)}, {acc});")
-                sc = n.a("scale")
-                body.append(f"{o}[{c}] = {acc if sc == 1.0 else f'smul({acc}, {_lit(sc)})'};")
-            return
         for c in range(n.nc):
             acc = None
             for arr, w in vals:
@@ -853,12 +774,12 @@ class _Emitter:
             n = self.g.nodes[nid]
             if n.op in STENCIL_PRIMS or n.op == "field" or n.op == "scalar":
                 arr = self.t()
-                body.append(f"{self.V} {arr}[{n.nc}];")
+                body.append(f"float {arr}[{n.nc}];")
                 self.fast_value(n, "0", "M", "KK", arr, body)
             else:
                 ins = [point(i) for i in n.ins]
                 arr = self.t()
-                body.append(f"{self.V} {arr}[{n.nc}];")
+                body.append(f"float {arr}[{n.nc}];")
                 self.pointwise(n, ins, arr, body)
             memo[nid] = arr
             return arr
@@ -870,20 +791,6 @@ class _Emitter:
         self.lines.append("template <int M, int KK> __device__ __forceinline__ void eval_fast(const FCtx& x, float* rv) {")
         self.lines += ["  " + b for b in body]
         self.lines.append("}")
-        if self.explicit:
-            # voxels KK and KK + 1 of row M in packed FP32, the same roundings as eval_fast
-            self.pair = True
-            body = []
-            memo = {}
-            for r, off in zip(roots, self.offsets):
-                arr = point(r.node)
-                for c in range(self.g.nodes[r.node].nc):
-                    body.append(f"rv0[{off + c}] = {arr}[{c}].x; rv1[{off + c}] = {arr}[{c}].y;")
-            self.lines.append("template <int M, int KK> __device__ __forceinline__ void "
-                              "eval_pair(const FCtx& x, float* rv0, float* rv1) {")
-            self.lines += ["  " + b for b in body]
-            self.lines.append("}")
-            self.pair = False
         # slow
         body = []
         memo_s: Dict[int, str] = {}
@@ -2137,11 +2044,6 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             if eager:
                 B.append(f"    float rvk[VPT][KV][{nroot}];")
                 for m in range(vpt):
-                    if e.explicit and kvn % 2 == 0:
-                        # two k-adjacent voxels per call, packed FP32 (same bits as one by one)
-                        for kk in range(0, kvn, 2):
-                            B.append(f"    eval_pair<{m}, {kk}>(x, rvk[{m}][{kk}], rvk[{m}][{kk + 1}]);")
-                        continue
                     for kk in range(kvn):
                         B.append(f"    eval_fast<{m}, {kk}>(x, rvk[{m}][{kk}]);")
                 B += ["    " + k for k in _plane_open(spec, e)]

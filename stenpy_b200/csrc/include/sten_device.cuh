@@ -58,30 +58,6 @@ STEN_DEV void st_from_f64(bf16_t* p, double v) { st_from_f32(p, (float)v); }
 STEN_DEV void st_from_f64(f16_t* p, double v) { st_from_f32(p, (float)v); }
 
 // ------------------------------------------------------------------ math helpers
-// Explicitly rounded arithmetic for passes that evaluate two k-adjacent voxels at once
-// in packed FP32 (f32x2) instructions: the one-voxel (float) and two-voxel (float2)
-// forms round each operation the same way (nothing is contracted), so both give the
-// same bits. Subtraction a - b is one rounding of a + (-1) b; negation is exact.
-STEN_DEV float sadd(float a, float b) { return __fadd_rn(a, b); }
-STEN_DEV float ssub(float a, float b) { return __fsub_rn(a, b); }
-STEN_DEV float smul(float a, float b) { return __fmul_rn(a, b); }
-STEN_DEV float sfma(float a, float b, float c) { return fmaf(a, b, c); }
-STEN_DEV float sneg(float a) { return -a; }
-STEN_DEV float sabs(float a) { return fabsf(a); }
-STEN_DEV float ssqrt(float a) { return sqrtf(a); }
-STEN_DEV float sfmax(float a, float b) { return fmaxf(a, b); }
-STEN_DEV float2 f2s(float a) { return make_float2(a, a); }
-STEN_DEV float2 sadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-STEN_DEV float2 ssub(float2 a, float2 b) { return __ffma2_rn(b, f2s(-1.0f), a); }   // (-1) b is exact
-STEN_DEV float2 smul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-STEN_DEV float2 smul(float2 a, float b) { return __fmul2_rn(a, f2s(b)); }
-STEN_DEV float2 sfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-STEN_DEV float2 sfma(float a, float2 b, float2 c) { return __ffma2_rn(f2s(a), b, c); }
-STEN_DEV float2 sfma(float2 a, float b, float2 c) { return __ffma2_rn(a, f2s(b), c); }
-STEN_DEV float2 sneg(float2 a) { return __fmul2_rn(a, f2s(-1.0f)); }
-STEN_DEV float2 sabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
-STEN_DEV float2 ssqrt(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
-STEN_DEV float2 sfmax(float2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
 // ------------------------------------------------------------------ k-vector chunks
 // A thread's KV k-adjacent voxels of one row are one contiguous chunk of CW bytes in
 // shared memory, aligned to 16 (CW % 16 == 0), 8 (CW % 8 == 0) or 4 bytes. Element

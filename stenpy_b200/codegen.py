@@ -138,11 +138,28 @@ class PassSpec:
     nested_ok: bool = False    # dims 1 and 2 have >= 4 points (two-layer extrapolation)
 
     def hk(self, f: FieldSpec) -> int:
-        """k-halo in elements, rounded so TMA x-coordinates stay 16-byte aligned."""
+        """k-halo in elements. TMA-staged fields: rounded so TMA x-coordinates stay
+        16-byte aligned. Row-staged fields: the least halo >= f.halo that keeps each
+        thread's vector chunk aligned in the ring and the box row a whole number of
+        16-byte units."""
         if f.halo == 0:
             return 0
-        a = 16 // ESIZE[f.dtype]
-        return ((f.halo + a - 1) // a) * a
+        es = ESIZE[f.dtype]
+        if f.tma:
+            a = 16 // es
+            return ((f.halo + a - 1) // a) * a
+        cw = self.cfg.kv * f.nc * es
+        vec = 16 if cw % 16 == 0 else (8 if cw % 8 == 0 else (4 if cw % 4 == 0 else es))
+        hk = f.halo
+        # an extrapolated ghost at the last column reads the 3 (two layers: 4) columns
+        # before it, which a tile holding only that column has in its halo only
+        rk = (self.ghosts or {}).get((f.slot, 2))
+        if rk in ("edge2", "edge2x2"):
+            hk = max(hk, 3 if rk == "edge2x2" else 2)
+        while (hk * f.nc * es) % vec or ((self.cfg.tk + 2 * hk) * f.nc * es) % 16:
+            hk += 1
+            assert hk <= f.halo + 64, "no k-halo keeps row-staged chunks aligned"
+        return hk
 
     def box(self, f: FieldSpec) -> Tuple[int, int]:
         """(row width in elements, rows) of one staged plane tile."""

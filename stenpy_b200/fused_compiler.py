@@ -429,9 +429,10 @@ class Planner:
             # every field goes through a TMA-filled plane ring when the layout allows;
             # fields read at offsets carry a halo of the pass radius
             f.halo = radius if f.slot in offset_read else 0
-            w, h = spec.box(f)
             es = ESIZE[f.dtype]
-            f.tma = (n2 * f.nc * es) % 16 == 0 and (w * es) % 16 == 0 and w <= 256 and h <= 256
+            f.tma = (n2 * f.nc * es) % 16 == 0        # the box (and its k-halo) as TMA stages it
+            w, h = spec.box(f)
+            f.tma = f.tma and (w * es) % 16 == 0 and w <= 256 and h <= 256
             f.staged = f.tma or f.slot in offset_read
             if f.staged and not f.tma and self.shape[1] * n2 * f.nc * es + 4 * w * es >= 1 << 31:
                 # row staging addresses a unit by its 32-bit offset from the plane start

@@ -135,17 +135,20 @@ def test_16bit_fields_with_one_sided_edges_keep_fp32_accuracy(dtype):
                 assert rel_err(got, ref) <= 1e-5, (expr, shape, ghost, rel_err(got, ref))
 
 
+@pytest.mark.parametrize("kv", [1, 2])
 @pytest.mark.parametrize("tk,tj", [(32, 16), (64, 8)])
 @pytest.mark.parametrize("shape", [(10, 17, 65), (9, 33, 97), (12, 18, 66)])
-def test_second_derivative_ghosts_where_tile_halos_cross_faces(shape, tk, tj):
+def test_second_derivative_ghosts_where_tile_halos_cross_faces(shape, tk, tj, kv):
     """Two-layer ghost cells of d1(d1(f)) (reach 2): tiles whose own voxels stop one
-    short of a face still read past it and must get the extrapolated values."""
+    short of a face still read past it and must get the extrapolated values; a last
+    tile holding one column reads the four before it (row-staged grids: the k-halo
+    depends on the voxels per thread)."""
     import stenpy_b200 as S
     from stenpy_b200.codegen import PassConfig
     from stenpy_b200.synth import sinusoid_field
     dev = _dev()
     f = sinusoid_field(shape, seed=9)
-    cfg = PassConfig(tj=tj, tk=tk, threads=128, seg_len=8)
+    cfg = PassConfig(tj=tj, tk=tk, threads=128, seg_len=8, kv=kv)
     g, sink, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": f.to(dev)})
     got = S.Runtime(device=dev, config=cfg).run(g)[sink]
     g2, sink2, *_ = S.compile_expression("trace(_hessian(f))", boundary="neumann", field_map={"f": f.double()})

@@ -56,10 +56,11 @@ FORM_DT = {k: v[0] for k, v in FORMS.items()}
 # f + u(3) + out, each once at storage dtype
 ALG_BYTES = {k: 4 * i.itemsize + o.itemsize for k, (i, o) in FORMS.items()}
 HEADLINE = "fp16"
-# DRAM bytes (read + write) of one launch of the headline form's dominant pass at
-# 512^3, from an ncu capture of this command's kernels (profiles/ summary of
-# sten_kernel at 512^3, FP16); null for other sizes or forms
-NCU_TRAFFIC = {("fp16", 512): 284091392 + 230927360}
+# DRAM bytes (read + write) of one launch of each z-march pass of the headline form
+# at 512^3 (pass 0: curl-norm partials, pass 1: Laplacian with statistics), from an
+# ncu capture of these kernels (profiles/ summary of sten_kernel at 512^3, FP16); the
+# line reports the dominant pass's; null for other sizes or forms
+NCU_TRAFFIC = {("fp16", 512, 0): 829506304 + 3847680, ("fp16", 512, 1): 286126592 + 231464448}
 
 
 def _peaks():
@@ -159,7 +160,8 @@ def make_fields(size, device):
 def build(form, f, u, device, tune=True, schedule=None):
     """Plan the step for one storage form; with ``tune`` every pass gets the schedule
     the autotuner measured fastest (exhaustive over its candidates, cached); a fixed
-    ``schedule`` (PassConfig) applies to every pass instead."""
+    ``schedule`` (PassConfig) applies to every pass instead, or a list of them, one
+    per pass in plan order."""
     import stenpy_b200 as S
     from stenpy_b200 import autotune as AT
     from stenpy_b200 import fused_compiler as FC
@@ -169,7 +171,15 @@ def build(form, f, u, device, tune=True, schedule=None):
     wanted = [sink] + [g.add(r, (sink,), {}) for r in REDS]
     if schedule is not None:
         tune = False
-    plan = FC.get_plan(g, wanted, out_dtype=odt, config=schedule)
+    per_pass = isinstance(schedule, list)
+    plan = FC.get_plan(g, wanted, out_dtype=odt, config=None if per_pass else schedule)
+    if per_pass:
+        from stenpy_b200.codegen import with_config
+        if len(schedule) != len(plan.passes):
+            raise SystemExit(f"--schedule lists {len(schedule)} schedules for {len(plan.passes)} passes")
+        for pp, cfg in zip(plan.passes, schedule):
+            pp.spec = with_config(pp.spec, cfg)
+            pp.module = pp.shell_module = None
     values, back = FC.bind(plan, g, wanted)
     tuned = AT.tune_plan(plan, values, device, tag=f"bench-{form}") if tune else []
     prog = FC.build_program(plan, values, device)
@@ -762,7 +772,8 @@ def main():
     ap.add_argument("--batch-lo", type=int, default=32)
     ap.add_argument("--batch-hi", type=int, default=320)
     ap.add_argument("--tune-log", default="")
-    ap.add_argument("--schedule", default="", help="JSON PassConfig for every pass (no autotuning), "
+    ap.add_argument("--schedule", default="", help="JSON PassConfig for every pass, or a JSON list of them "
+                                                    "(one per pass, in plan order); no autotuning, "
                                                     "e.g. '{\"tj\": 16, \"tk\": 32, \"seg_len\": 32}'")
     ap.add_argument("--dags", type=int, default=2000)
     ap.add_argument("--heldout", type=int, default=200)
@@ -795,7 +806,8 @@ def main():
     schedule = None
     if args.schedule:
         from stenpy_b200.codegen import PassConfig
-        schedule = PassConfig(**json.loads(args.schedule))
+        sch = json.loads(args.schedule)
+        schedule = [PassConfig(**c) for c in sch] if isinstance(sch, list) else PassConfig(**sch)
     f, u = make_fields(args.size, dev)
     n_vox = args.size ** 3
     stream = torch.cuda.Stream(dev)
@@ -846,7 +858,8 @@ def main():
             "schedules": [dict(vars(p.spec.cfg)) for p in plan.passes],
             "kernels_ms": [round(t, 4) for _, t in kt],
             "dominant": {"ms": dom_ms, "alg_bytes": alg, "GBps": alg / (dom_ms * 1e-3) / 1e9,
-                         "frac_of_peak": alg / (dom_ms * 1e-3) / 1e9 / peak},
+                         "frac_of_peak": alg / (dom_ms * 1e-3) / 1e9 / peak,
+                         "pass": plan.passes.index(dom_pass)},
             "pass_frac": pass_frac,
         }
         del cg
@@ -876,7 +889,7 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(head["dominant"]["GBps"], 1), "peak": peak,
                          "unit": "GB/s", "frac": round(head["dominant"]["GBps"] / peak, 4), "peak_kind": peak_kind,
-                         "traffic": NCU_TRAFFIC.get((head_form, args.size)),
+                         "traffic": NCU_TRAFFIC.get((head_form, args.size, head["dominant"]["pass"])),
                          "kernel": "dominant pass of the headline form",
                          "step_frac": round(head["step_frac_of_peak"], 4), "forms": summary},
             "gpu_launches": head["launches_per_step"] * args.steps, "clocks": clocks}

@@ -60,7 +60,7 @@ HEADLINE = "fp16"
 # at 512^3 (pass 0: curl-norm partials, pass 1: Laplacian with statistics), from an
 # ncu capture of these kernels (profiles/ summary of sten_kernel at 512^3, FP16); the
 # line reports the dominant pass's; null for other sizes or forms
-NCU_TRAFFIC = {("fp16", 512, 0): 829506304 + 3847680, ("fp16", 512, 1): 286126592 + 231464448}
+NCU_TRAFFIC = {("fp16", 512, 0): 831392256 + 6005504, ("fp16", 512, 1): 285747456 + 232748288}
 
 
 def _peaks():

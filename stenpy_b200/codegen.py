@@ -1349,12 +1349,13 @@ def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -
     L = [f"// row staging of field {sl}: {h} box rows of {c} chunks; {nu} copy units and {ni} chunks per thread",
          f"const u32 rsB{sl}_ = (u32)p.n2 * {f.nc * es}u;  // bytes of a grid row (mod 2^32)",
          f"int rsw{sl}_[{nu}];",
-         f"u32 rsok{sl}_ = 0u;",
+         f"u32 rsok{sl}_ = 0u, rsex{sl}_ = 0u;  // unit's row inside the grid / unit exists",
          f"#pragma unroll\nfor (int i = 0; i < {nu}; ++i) {{",
          f"  const int q = tid + i * NT, r = q / {c + 1}, u = q - r * {c + 1};",
          f"  int jg = tj0 - {f.halo} + r;"]
     L += _remap_line("jg", "p.n1", rj, "  ")
     L += [f"  rsw{sl}_[i] = (int)((u32)jg * rsB{sl}_ + (u32)((tk0 - {spec.hk(f)}) * {f.nc * es}) + 16u * (u32)u);",
+          f"  if (q < {units}) rsex{sl}_ |= 1u << i;",
           f"  if (q < {units} && jg >= 0 && jg < p.n1) rsok{sl}_ |= 1u << i;",
           "}",
           f"u32 rsit{sl}_[{ni}];",
@@ -1373,25 +1374,28 @@ def _rs_plan(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", ghost: bool) -
 def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[int, int]) -> List[str]:
     """Copies of plane ``zq`` into ring slot ``s`` by every thread, its units only: 16
     bytes from the aligned address at or below the unit's offset from the plane
-    start; in the field's first and last planes, units outside the field are zero.
-    Under a dim-2 rule that copies values, tiles at a dim-2 face also copy strips."""
+    start; units of rows outside the grid, of planes outside the field and (in the
+    field's first and last planes) outside the field are zero. Under a dim-2 rule
+    that copies values, tiles at a dim-2 face also copy strips."""
     w, h, es, rb, c, sr, rpw, ni = rs_geometry(spec, f, cfg)
     units, nu = rs_units(spec, f, cfg)
     sl = f.slot
-    L = ["if (zok) {",
+    L = ["{",
          f"  const unsigned long long fb_ = (unsigned long long)p.fld[{sl}];",
          f"  const unsigned long long bz_ = fb_ + (unsigned long long)zq * p.n1 * rsB{sl}_;   // plane start",
          f"  const u32 dst_ = smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)}) + (u32)tid * 16u;",
-         "  if (zq > 0 && zq < p.nl - 1) {   // every unit lies inside the field"]
+         "  if (zok && zq > 0 && zq < p.nl - 1) {   // every unit lies inside the field",
+         "    // rows outside the grid are zero (nothing read): the shift needs no test"]
     for i in range(nu):
-        L.append(f"    if (rsok{sl}_ & {1 << i}u) {{ const int w_ = rsw{sl}_[{i}];"
-                 f" cp_async16_cg(dst_ + {i * cfg.threads * 16}u, (const void*)(bz_ + (long long)(w_ - (int)(((u32)bz_ + (u32)w_) & 15u))), 16u); }}")
-    L += ["  } else {",
+        L.append(f"    if (rsex{sl}_ & {1 << i}u) {{ const int w_ = rsw{sl}_[{i}];"
+                 f" cp_async16_cg(dst_ + {i * cfg.threads * 16}u, (const void*)(bz_ + (long long)(w_ - (int)(((u32)bz_ + (u32)w_) & 15u))),"
+                 f" (rsok{sl}_ >> {i}) << 4 & 16u); }}")
+    L += ["  } else {   // the field's first and last planes, and planes outside it",
           f"    const unsigned long long lo_ = fb_ & ~15ull, hi_ = (fb_ + (unsigned long long)p.nl * p.n1 * rsB{sl}_ + 15ull) & ~15ull;"]
     for i in range(nu):
-        L += [f"    if (rsok{sl}_ & {1 << i}u) {{ const int w_ = rsw{sl}_[{i}];",
+        L += [f"    if (rsex{sl}_ & {1 << i}u) {{ const int w_ = rsw{sl}_[{i}];",
               f"      const unsigned long long g_ = bz_ + (long long)(w_ - (int)(((u32)bz_ + (u32)w_) & 15u));",
-              f"      const bool in_ = g_ >= lo_ && g_ < hi_;",
+              f"      const bool in_ = zok && (rsok{sl}_ & {1 << i}u) && g_ >= lo_ && g_ < hi_;",
               f"      cp_async16_cg(dst_ + {i * cfg.threads * 16}u, (const void*)(in_ ? g_ : lo_), in_ ? 16u : 0u); }}"]
     L.append("  }")
     rule, ns = rs_strip(spec, f)
@@ -1401,7 +1405,7 @@ def _rs_request(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict
         hb = f.halo * f.nc * es
         lay = slot_layout(spec, f)
         rj = (spec.ghosts or {}).get((f.slot, 1))
-        L += [f"  if (tk0 == 0 || tk0 + TK + {spec.hk(f)} > p.n2) {{",
+        L += [f"  if (zok && (tk0 == 0 || tk0 + TK + {spec.hk(f)} > p.n2)) {{",
               f"    const u32 sdst_ = smem_u32(smem + {rings[f.slot]} + s * {plane_bytes(spec, f)} + {lay['rs_strip']});",
               f"    #pragma unroll 1\n    for (int t = tid; t < {2 * h * ns}; t += NT) {{",
               f"      const int rs2 = t / {ns}, sd = rs2 & 1, r = rs2 >> 1, u = t - rs2 * {ns};",
@@ -1423,8 +1427,9 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
               zexpr: str) -> List[str]:
     """``rs_shift{slot}(q)``, once plane q's copies landed in its ring slot: each ring
     chunk becomes the 16 bytes that start ``shift`` bytes into it (the row's byte
-    offset mod 16), in place — a warp reads all its chunks before it writes any (a
-    warp's rows are its own) — zero for rows outside the grid.
+    offset mod 16), in place — per chunk, every lane of a warp reads before any
+    writes; a warp's rows are its own and a row's chunks come in order; rows outside
+    the grid arrive as zeros.
     Elements of chunks at a dim-2 face that lie outside the grid are then fetched from
     global memory under a dim-2 rule that copies values, or zeroed under the zero rule
     (one loop after the shift keeps that code out of the unrolled chunks); otherwise
@@ -1448,21 +1453,22 @@ def _rs_shift(spec: "PassSpec", f: "FieldSpec", cfg: "PassConfig", rings: Dict[i
          f"  unsigned char* slot_ = smem + {rings[f.slot]} + ((q - p_first) % NSLOT) * {plane_bytes(spec, f)};"]
     if face:
         L.append("  u32 kx_ = 0u;   // chunks at a dim-2 face")
-    # every chunk of this thread is read before any is written (one warp barrier):
-    # a chunk's second unit is the next chunk's first, written by the next lane
-    L.append(f"  uint4 v_[{ni}];")
+    # per chunk, every lane of the warp reads before any lane writes (a warp barrier):
+    # a chunk's second unit is the next chunk's first, written by the next lane; a
+    # warp's rows are its own and a row's chunks come in order. Rows outside the grid
+    # (and planes outside the field) were copied as zeros, so every chunk takes the
+    # same path; only chunks past a warp's last row are skipped.
+    nw = cfg.threads // 32
+    full_chunks = (h // nw) * c        # chunks of the warp with the fewest rows
+    L.append(f"  const u32 slot32_ = smem_u32(slot_);")
     for i in range(ni):
-        L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
-              f"    v_[{i}] = make_uint4(0u, 0u, 0u, 0u);",
-              f"    if (zok_ && (m_ & {RS_ROWOK}u))",
-              f"      v_[{i}] = shifted16<{es}>(slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4), (sz_ + (m_ >> {RS_SHIFT})) & 15u);",
-              "  }"]
-    L.append("  __syncwarp();")
-    for i in range(ni):
-        L += [f"  {{ const u32 m_ = rsit{sl}_[{i}];",
-              f"    if (m_ & {RS_VALID}u) *(uint4*)(slot_ + ((m_ & {(1 << RS_SHIFT) - 1}u) << 4)) = v_[{i}];"]
+        a = f"slot32_ + ((rsit{sl}_[{i}] & {(1 << RS_SHIFT) - 1}u) << 4)"
+        st = f"st_shared_v4({a}, v_);"
+        L += [f"  {{ const uint4 v_ = shifted16s<{es}>({a}, (sz_ + (rsit{sl}_[{i}] >> {RS_SHIFT})) & 15u);",
+              "    __syncwarp();",
+              f"    {st}" if (i + 1) * 32 <= full_chunks else f"    if (rsit{sl}_[{i}] & {RS_VALID}u) {st}"]
         if face:
-            L.append(f"    if (zok_ && (m_ & {RS_ROWOK}u) && (m_ & {RS_KX}u)) kx_ |= {1 << i}u;")
+            L.append(f"    if (zok_ && (rsit{sl}_[{i}] & {RS_ROWOK}u) && (rsit{sl}_[{i}] & {RS_KX}u)) kx_ |= {1 << i}u;")
         L.append("  }")
     if not face:
         L.append("};")

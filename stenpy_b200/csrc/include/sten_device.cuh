@@ -248,6 +248,33 @@ STEN_DEV void cp_async16_cg(u32 sdst, const void* gsrc, u32 src_bytes) {
 STEN_DEV void cp_async_mbar_arrive(u64* bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
 }
+// 16-byte shared-memory load / store at a 32-bit shared address.
+STEN_DEV uint4 ld_shared_v4(u32 saddr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(saddr) : "memory");
+  return v;
+}
+STEN_DEV void st_shared_v4(u32 saddr, uint4 v) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" :: "r"(saddr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+// shifted16 at a 32-bit shared address.
+template <int ES> STEN_DEV uint4 shifted16s(u32 src, u32 sh) {
+  const uint4 a = ld_shared_v4(src), b = ld_shared_v4(src + 16u);
+  const u32 w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+  const bool s8 = (sh & 8u) != 0u, s4 = (sh & 4u) != 0u;
+  u32 x[6], y[5];
+  #pragma unroll
+  for (int j = 0; j < 6; ++j) x[j] = s8 ? w[j + 2] : w[j];
+  if constexpr (ES >= 8) return make_uint4(x[0], x[1], x[2], x[3]);
+  #pragma unroll
+  for (int j = 0; j < 5; ++j) y[j] = s4 ? x[j + 1] : x[j];
+  if constexpr (ES == 4) return make_uint4(y[0], y[1], y[2], y[3]);
+  const u32 bs = (sh & 3u) * 8u;
+  return make_uint4(__funnelshift_r(y[0], y[1], bs), __funnelshift_r(y[1], y[2], bs),
+                    __funnelshift_r(y[2], y[3], bs), __funnelshift_r(y[3], y[4], bs));
+}
 // Untiled bulk copy of `bytes` (a multiple of 16) from the 16-byte aligned global
 // address gsrc to the 16-byte aligned shared address sdst; completion counted on `bar`.
 STEN_DEV void bulk_load(u32 sdst, const void* gsrc, u32 bytes, u64* bar) {

@@ -259,21 +259,41 @@ STEN_DEV void st_shared_v4(u32 saddr, uint4 v) {
   asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" :: "r"(saddr), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
                : "memory");
 }
-// shifted16 at a 32-bit shared address.
+STEN_DEV uint2 ld_shared_v2(u32 saddr) {
+  uint2 v;
+  asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(saddr) : "memory");
+  return v;
+}
+// shifted16 at a 32-bit shared address. 2- and 8-byte elements: the 8-byte half of
+// the offset taken by the load address (8-byte loads), the rest by one select step and
+// funnel shifts; 4-byte elements: two 16-byte loads and two select steps (measured
+// faster for them at 509^3).
 template <int ES> STEN_DEV uint4 shifted16s(u32 src, u32 sh) {
-  const uint4 a = ld_shared_v4(src), b = ld_shared_v4(src + 16u);
-  const u32 w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-  const bool s8 = (sh & 8u) != 0u, s4 = (sh & 4u) != 0u;
-  u32 x[6], y[5];
-  #pragma unroll
-  for (int j = 0; j < 6; ++j) x[j] = s8 ? w[j + 2] : w[j];
-  if constexpr (ES >= 8) return make_uint4(x[0], x[1], x[2], x[3]);
-  #pragma unroll
-  for (int j = 0; j < 5; ++j) y[j] = s4 ? x[j + 1] : x[j];
-  if constexpr (ES == 4) return make_uint4(y[0], y[1], y[2], y[3]);
-  const u32 bs = (sh & 3u) * 8u;
-  return make_uint4(__funnelshift_r(y[0], y[1], bs), __funnelshift_r(y[1], y[2], bs),
-                    __funnelshift_r(y[2], y[3], bs), __funnelshift_r(y[3], y[4], bs));
+  if constexpr (ES == 4) {
+    const uint4 a = ld_shared_v4(src), b = ld_shared_v4(src + 16u);
+    const u32 w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    const bool s8 = (sh & 8u) != 0u, s4 = (sh & 4u) != 0u;
+    u32 x[5];
+    #pragma unroll
+    for (int j = 0; j < 5; ++j) x[j] = s8 ? w[j + 2] : w[j];
+    return s4 ? make_uint4(x[1], x[2], x[3], x[4]) : make_uint4(x[0], x[1], x[2], x[3]);
+  } else {
+    const u32 base = src + (sh & 8u);
+    const uint2 a = ld_shared_v2(base), b = ld_shared_v2(base + 8u);
+    if constexpr (ES >= 8) {
+      return make_uint4(a.x, a.y, b.x, b.y);
+    } else {
+      const uint2 c = ld_shared_v2(base + 16u);
+      const u32 v[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
+      const bool s4 = (sh & 4u) != 0u;
+      u32 y[5];
+      #pragma unroll
+      for (int j = 0; j < 5; ++j) y[j] = s4 ? v[j + 1] : v[j];
+      const u32 bs = (sh & 3u) * 8u;
+      return make_uint4(__funnelshift_r(y[0], y[1], bs), __funnelshift_r(y[1], y[2], bs),
+                        __funnelshift_r(y[2], y[3], bs), __funnelshift_r(y[3], y[4], bs));
+    }
+  }
 }
 // Untiled bulk copy of `bytes` (a multiple of 16) from the 16-byte aligned global
 // address gsrc to the 16-byte aligned shared address sdst; completion counted on `bar`.

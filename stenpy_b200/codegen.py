@@ -534,7 +534,14 @@ class _Emitter:
                 a = self.fast_call(n.ins[0], *plus, body)
                 b = self.fast_call(n.ins[0], *minus, body)
                 terms.append((a, b, _lit(n.a("invh2")[ax])))
+            h2 = n.a("invh2")
             for c in range(n.nc):
+                if h2[0] == h2[1] == h2[2]:
+                    # equal spacing: the six neighbours summed, then one fused -6 c
+                    ssum = " + ".join(f"({a}[{c}] + {b}[{c}])" for a, b, _ in terms)
+                    v = f"fmaf(-6.0f, {ctr}[{c}], {ssum})"
+                    body.append(f"{o}[{c}] = {v if h2[0] == 1.0 else f'{v} * {terms[0][2]}'};")
+                    continue
                 parts = [f"(({a}[{c}] + {b}[{c}]) - 2.0f * {ctr}[{c}]) * {s}" for a, b, s in terms]
                 body.append(f"{o}[{c}] = ({parts[0]} + {parts[1]}) + {parts[2]};")
             return
@@ -548,8 +555,39 @@ class _Emitter:
                 vals.append((self.fast_call(n.ins[0], *q, body), tap[3]))
             self._tap_sum(n, vals, o, body)
             return
+        if self.d1_pair(n):
+            self.d1_pair_value(n, di, dj, dk, o, body)
+            return
         ins = [self.fast_call(i, di, dj, dk, body) for i in n.ins]
         self.pointwise(n, ins, o, body)
+
+    def d1_pair(self, n: PNode) -> bool:
+        """A sum or difference of two central first differences with one spacing (the
+        curl's components): scaled once, after the difference of the differences."""
+        if n.op not in ("add", "sub") or len(n.ins) != 2:
+            return False
+        a, b = (self.g.nodes[i] for i in n.ins)
+        return (a.op == b.op == "d1" and a.a("mode") != "zero" and b.a("mode") != "zero"
+                and a.a("inv2h") == b.a("inv2h") and a.nc == b.nc == n.nc)
+
+    def d1_pair_value(self, n: PNode, di: str, dj: str, dk: str, o: str, body: List[str]) -> None:
+        """o = ((a1 - b1) +/- (a2 - b2)) * inv2h for the two d1 inputs of n (the same
+        value as scaling each difference first when inv2h is a power of two)."""
+        raws = []
+        for nid in n.ins:
+            d = self.g.nodes[nid]
+            off = [di, dj, dk]
+            ax, comp = d.a("axis"), d.a("comp")
+            plus = list(off); plus[ax] = f"({off[ax]}) + 1"
+            minus = list(off); minus[ax] = f"({off[ax]}) - 1"
+            a = self.fast_call(d.ins[0], *plus, body)
+            b = self.fast_call(d.ins[0], *minus, body)
+            raws.append([f"({a}[{c if comp is None else comp}] - {b}[{c if comp is None else comp}])"
+                         for c in range(d.nc)])
+        sym = "+" if n.op == "add" else "-"
+        s = _lit(self.g.nodes[n.ins[0]].a("inv2h"))
+        for c in range(n.nc):
+            body.append(f"{o}[{c}] = ({raws[0][c]} {sym} {raws[1][c]}) * {s};")
 
     def _tap_sum(self, n: PNode, vals, o: str, body: List[str]) -> None:
         """o = scale * Σ w·v over (array, weight) pairs, accumulated in tap order."""
@@ -794,8 +832,13 @@ class _Emitter:
                 body.append(f"float {arr}[{n.nc}];")
                 self.fast_value(n, "0", "M", "KK", arr, body)
             else:
-                ins = [point(i) for i in n.ins]
                 arr = self.t()
+                if self.d1_pair(n):
+                    body.append(f"float {arr}[{n.nc}];")
+                    self.d1_pair_value(n, "0", "M", "KK", arr, body)
+                    memo[nid] = arr
+                    return arr
+                ins = [point(i) for i in n.ins]
                 body.append(f"float {arr}[{n.nc}];")
                 self.pointwise(n, ins, arr, body)
             memo[nid] = arr

@@ -25,8 +25,9 @@ Kernel shape (``emit_pass``): a CTA owns a TJ × TK tile of the (dim1, dim2) pla
 and marches along dim 0 over a segment of planes. Every field read at an offset
 is staged plane by plane into a shared-memory ring of 2R+1+P slots (R = the
 pass's stencil reach, P = prefetch depth), by TMA (``cp.async.bulk.tensor``, one
-elected thread, mbarrier completion) when the layout allows it, else by plain
-cooperative loads. Voxels at least R away from every face take the *fast* path:
+elected thread, mbarrier completion) when the layout allows it, else by row staging
+(16-byte ``cp.async`` copies of the units covering each row, shifted into place in
+shared memory). Voxels at least R away from every face take the *fast* path:
 central formulas reading the ring at compile-time offsets. Voxels within R of a
 face take the *slow* path: the same DAG evaluated from global memory with each
 operator's own boundary rule. Compute is FP32; reductions accumulate in FP64.
@@ -89,7 +90,7 @@ class FieldSpec:
     dtype: str          # f32 / bf16 / f16 / f64
     nc: int             # interleaved components per voxel (1, 3, 9)
     staged: bool = False  # held in a shared-memory plane ring
-    tma: bool = False     # ring filled by TMA (else by cooperative loads)
+    tma: bool = False     # ring filled by TMA (else by row staging)
     halo: int = 0         # j/k halo of the staged tile (0 for fields read only at the voxel)
     wrap_k: bool = False  # periodic ghosts along dim 2 come from extra TMA strips
     wrap_j: bool = False  # periodic ghosts along dim 1 come from extra TMA strips
@@ -1588,7 +1589,7 @@ def _ghost_fill(spec: PassSpec, rings: Dict[int, int]) -> List[str]:
     tile in the ring slot of plane q (edge tiles only). Sources: the tile itself
     (replicate / reflect / extrapolation; along dim 1 the tile may be too thin at the
     last face, then global memory), the TMA wrap strips (periodic), or nothing when
-    the cooperative fill already applied the rule (remap rules without TMA)."""
+    the row staging already applied the rule (remap rules without TMA)."""
     K = ["auto ghost_fill = [&](int q) {",
          "  const int s = (q - p_first) % NSLOT;",
          "  const int zq = sten_plane(p, q + p.i_base);",
@@ -2175,8 +2176,8 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 if not f.staged:
                     B.append(f"    frow{f.slot} += plane_n * {f.nc};")
             # the next plane (i+1+RAD) must be resident and ghosted before the barrier;
-            # ghosts derived from cooperatively staged (asynchronous) rows wait for every
-            # thread's copies: an extra barrier, in edge tiles only
+            # ghosts derived from row-staged rows wait for every warp's shift: an extra
+            # barrier, in edge tiles only
             lsu_ghost = ghost and any(
                 (spec.ghosts or {}).get((f.slot, ax)) in _EXTRAPOLATED for f in lsu_fields for ax in (1, 2))
             if staged:

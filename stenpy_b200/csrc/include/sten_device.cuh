@@ -192,39 +192,10 @@ STEN_DEV void mbar_inval(u64* bar) {
 STEN_DEV void fence_mbar_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// 4-byte asynchronous global->shared copy (completion by commit / wait groups)
-// asynchronous copy of N (4, 8 or 16) bytes to the shared address sdst, of which the
-// first src_bytes come from gsrc and the rest are zero (src_bytes 0: nothing is read;
-// gsrc must still be a mapped, N-aligned address)
-template <int N> STEN_DEV void cp_async_n(u32 sdst, const void* gsrc, u32 src_bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;"
-               :: "r"(sdst), "l"(gsrc), "n"(N), "r"(src_bytes) : "memory");
-}
 STEN_DEV void st_shared_u32(u32 saddr, u32 v) { asm volatile("st.shared.u32 [%0], %1;" :: "r"(saddr), "r"(v) : "memory"); }
 STEN_DEV void st_shared_u64(u32 saddr, u64 v) { asm volatile("st.shared.u64 [%0], %1;" :: "r"(saddr), "l"(v) : "memory"); }
 STEN_DEV void st_shared_u128(u32 saddr, u32 a, u32 b, u32 c, u32 d) {
   asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" :: "r"(saddr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
-}
-STEN_DEV void st_shared_zero16(u32 saddr) {
-  asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" :: "r"(saddr), "r"(0u) : "memory");
-}
-// The 16 bytes that start `sh` (0..15, a multiple of ES) bytes into the 32 bytes at
-// the 16-byte aligned shared src: the word offset sh / 4 picked in two select steps,
-// the byte offset sh % 4 by funnel shifts.
-template <int ES> STEN_DEV uint4 shifted16(const unsigned char* src, u32 sh) {
-  const uint4 a = *(const uint4*)src, b = *(const uint4*)(src + 16);
-  const u32 w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-  const bool s8 = (sh & 8u) != 0u, s4 = (sh & 4u) != 0u;
-  u32 x[6], y[5];
-  #pragma unroll
-  for (int j = 0; j < 6; ++j) x[j] = s8 ? w[j + 2] : w[j];
-  if constexpr (ES >= 8) return make_uint4(x[0], x[1], x[2], x[3]);
-  #pragma unroll
-  for (int j = 0; j < 5; ++j) y[j] = s4 ? x[j + 1] : x[j];
-  if constexpr (ES == 4) return make_uint4(y[0], y[1], y[2], y[3]);
-  const u32 bs = (sh & 3u) * 8u;
-  return make_uint4(__funnelshift_r(y[0], y[1], bs), __funnelshift_r(y[1], y[2], bs),
-                    __funnelshift_r(y[2], y[3], bs), __funnelshift_r(y[3], y[4], bs));
 }
 // The 16 bytes of v with bytes outside [lo, hi) zeroed.
 STEN_DEV uint4 keep_bytes16(uint4 v, u32 lo, u32 hi) {
@@ -264,7 +235,8 @@ STEN_DEV uint2 ld_shared_v2(u32 saddr) {
   asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(saddr) : "memory");
   return v;
 }
-// shifted16 at a 32-bit shared address. 2- and 8-byte elements: the 8-byte half of
+// The 16 bytes that start `sh` (0..15, a multiple of ES) bytes into the 32 bytes at the
+// 16-byte aligned 32-bit shared address src. 2- and 8-byte elements: the 8-byte half of
 // the offset taken by the load address (8-byte loads), the rest by one select step and
 // funnel shifts; 4-byte elements: two 16-byte loads and two select steps (measured
 // faster for them at 509^3).
@@ -295,14 +267,6 @@ template <int ES> STEN_DEV uint4 shifted16s(u32 src, u32 sh) {
     }
   }
 }
-// Untiled bulk copy of `bytes` (a multiple of 16) from the 16-byte aligned global
-// address gsrc to the 16-byte aligned shared address sdst; completion counted on `bar`.
-STEN_DEV void bulk_load(u32 sdst, const void* gsrc, u32 bytes, u64* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               :: "r"(sdst), "l"(gsrc), "r"(bytes), "r"(smem_u32(bar)) : "memory");
-}
-STEN_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> STEN_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
 STEN_DEV void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

@@ -137,6 +137,8 @@ class PassSpec:
     ghosts: Optional[Dict[Tuple[int, int], str]] = None
     i_periodic: bool = False   # every tap along dim 0 wraps: planes are loaded wrapped
     nested_ok: bool = False    # dims 1 and 2 have >= 4 points (two-layer extrapolation)
+    idx32: bool = False        # every element offset of every array fits in an int: the
+                               # boundary (shell) code indexes in 32-bit arithmetic
 
     def hk(self, f: FieldSpec) -> int:
         """k-halo in elements. TMA-staged fields: rounded so TMA x-coordinates stay
@@ -638,8 +640,12 @@ class _Emitter:
         f = self.s.fields[n.a("field")]
         ct = CTYPE[f.dtype]
         base = self.t()
-        body.append(f"const {ct}* {base} = (const {ct}*)p.fld[{f.slot}] + "
-                    f"(((size_t)sten_plane(p, {i}) * p.n1 + ({j})) * p.n2 + ({k})) * {f.nc};")
+        if self.s.idx32:
+            body.append(f"const {ct}* {base} = (const {ct}*)p.fld[{f.slot}] + "
+                        f"((sten_plane(p, {i}) * p.n1 + ({j})) * p.n2 + ({k})) * {f.nc};")
+        else:
+            body.append(f"const {ct}* {base} = (const {ct}*)p.fld[{f.slot}] + "
+                        f"(((size_t)sten_plane(p, {i}) * p.n1 + ({j})) * p.n2 + ({k})) * {f.nc};")
         for c in range(n.nc):
             body.append(f"{arr}[{c}] = ldg_as_f32({base} + {c});")
 
@@ -687,43 +693,36 @@ class _Emitter:
             for c in range(n.nc):
                 body.append(f"{o}[{c}] = ({a}[{cc(c)}] - {b}[{cc(c)}]) * {s2};")
             return
-        # torch.gradient edges: second order (edge2) or first order (edge1)
-        body.append(f"if (({x}) == 0) {{")
+        # torch.gradient edges, second order (edge2: (-3f0 + 4f1 - f2) / 2h) or first
+        # order (edge1: (f1 - f0) / h), both faces in one branch: the face point x
+        # and the inward step d (+1 at 0, -1 at n - 1); the last face's formula is the
+        # first's mirrored, (3f0 - 4f1 + f2) / 2h = -(first at d = -1), so the scale
+        # takes d's sign (an exact negation). One branch keeps a warp whose lanes
+        # hold both faces' voxels (a row's first and last columns) from running both.
+        body.append(f"if (({x}) > 0 && ({x}) < {nn} - 1) {{")
         sub: List[str] = []
-        if mode == "edge2":
-            e0 = self.slow_call(n.ins[0], *at("0"), sub)
-            e1 = self.slow_call(n.ins[0], *at("1"), sub)
-            e2 = self.slow_call(n.ins[0], *at("2"), sub)
-            for c in range(n.nc):
-                sub.append(f"{o}[{c}] = ((-3.0f * {e0}[{cc(c)}] + 4.0f * {e1}[{cc(c)}]) - {e2}[{cc(c)}]) * {s2};")
-        else:
-            s1 = _lit(n.a("invh"))
-            e0 = self.slow_call(n.ins[0], *at("0"), sub)
-            e1 = self.slow_call(n.ins[0], *at("1"), sub)
-            for c in range(n.nc):
-                sub.append(f"{o}[{c}] = ({e1}[{cc(c)}] - {e0}[{cc(c)}]) * {s1};")
-        body += ["  " + s for s in sub]
-        body.append(f"}} else if (({x}) == {nn} - 1) {{")
-        sub = []
-        if mode == "edge2":
-            e0 = self.slow_call(n.ins[0], *at(f"{nn} - 1"), sub)
-            e1 = self.slow_call(n.ins[0], *at(f"{nn} - 2"), sub)
-            e2 = self.slow_call(n.ins[0], *at(f"{nn} - 3"), sub)
-            for c in range(n.nc):
-                sub.append(f"{o}[{c}] = ((3.0f * {e0}[{cc(c)}] - 4.0f * {e1}[{cc(c)}]) + {e2}[{cc(c)}]) * {s2};")
-        else:
-            s1 = _lit(n.a("invh"))
-            e0 = self.slow_call(n.ins[0], *at(f"{nn} - 1"), sub)
-            e1 = self.slow_call(n.ins[0], *at(f"{nn} - 2"), sub)
-            for c in range(n.nc):
-                sub.append(f"{o}[{c}] = ({e0}[{cc(c)}] - {e1}[{cc(c)}]) * {s1};")
-        body += ["  " + s for s in sub]
-        body.append("} else {")
-        sub = []
         a = self.slow_call(n.ins[0], *at(f"({x}) + 1"), sub)
         b = self.slow_call(n.ins[0], *at(f"({x}) - 1"), sub)
         for c in range(n.nc):
             sub.append(f"{o}[{c}] = ({a}[{cc(c)}] - {b}[{cc(c)}]) * {s2};")
+        body += ["  " + s for s in sub]
+        body.append("} else {")
+        dd = self.t()
+        sub = [f"const int {dd} = ({x}) == 0 ? 1 : -1;"]
+        e0 = self.slow_call(n.ins[0], *at(f"({x})"), sub)
+        e1 = self.slow_call(n.ins[0], *at(f"({x}) + {dd}"), sub)
+        if mode == "edge2":
+            e2 = self.slow_call(n.ins[0], *at(f"({x}) + 2 * {dd}"), sub)
+            sc = self.t()
+            sub.append(f"const float {sc} = {dd} > 0 ? {s2} : -{s2};")
+            for c in range(n.nc):
+                sub.append(f"{o}[{c}] = ((-3.0f * {e0}[{cc(c)}] + 4.0f * {e1}[{cc(c)}]) - {e2}[{cc(c)}]) * {sc};")
+        else:
+            s1 = _lit(n.a("invh"))
+            sc = self.t()
+            sub.append(f"const float {sc} = {dd} > 0 ? {s1} : -{s1};")
+            for c in range(n.nc):
+                sub.append(f"{o}[{c}] = ({e1}[{cc(c)}] - {e0}[{cc(c)}]) * {sc};")
         body += ["  " + s for s in sub]
         body.append("}")
 
@@ -2233,35 +2232,39 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             K.append(f"  __shared__ double red_scratch[{RED_SCRATCH_DOUBLES}];")
         K.append("  const int tid = threadIdx.x;")
         K += ["  " + k for k in _red_decls(spec, "shell")]
-        K.append("  const long long n0 = p.n0g, n1 = p.n1, n2 = p.n2;")
-        K.append("  const long long g_lo = (long long)p.out_lo + p.i_base, g_hi = g_lo + p.n_out;")
-        K.append("  const long long a1 = max(n1 - 2 * RAD, 0ll), a2 = max(n2 - 2 * RAD, 0ll);")
-        K.append("  const long long c_low = max(0ll, min(g_hi, (long long)RAD) - g_lo);")
-        K.append("  const long long hs = max(g_lo, max(n0 - RAD, (long long)RAD));")
-        K.append("  const long long c_high = max(0ll, g_hi - hs);")
-        K.append("  const long long ii0 = max(g_lo, (long long)RAD), n_int = max(0ll, min(g_hi, n0 - RAD) - ii0);")
+        # 32-bit decode when every count fits an int (unsigned divisions are a few
+        # instructions; 64-bit ones a long emulated sequence per thread)
+        T, Z = ("int", "0") if spec.idx32 else ("long long", "0ll")
+        dv = (lambda a, b: f"(int)((unsigned)({a}) / (unsigned)({b}))") if spec.idx32 else (lambda a, b: f"({a}) / ({b})")
+        K.append(f"  const {T} n0 = p.n0g, n1 = p.n1, n2 = p.n2;")
+        K.append(f"  const {T} g_lo = ({T})p.out_lo + p.i_base, g_hi = g_lo + p.n_out;")
+        K.append(f"  const {T} a1 = max(n1 - 2 * RAD, {Z}), a2 = max(n2 - 2 * RAD, {Z});")
+        K.append(f"  const {T} c_low = max({Z}, min(g_hi, ({T})RAD) - g_lo);")
+        K.append(f"  const {T} hs = max(g_lo, max(n0 - RAD, ({T})RAD));")
+        K.append(f"  const {T} c_high = max({Z}, g_hi - hs);")
+        K.append(f"  const {T} ii0 = max(g_lo, ({T})RAD), n_int = max({Z}, min(g_hi, n0 - RAD) - ii0);")
         if regions == "A":
-            K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = 0, cC = 0;")
+            K.append(f"  const {T} cA = (c_low + c_high) * n1 * n2, cB = 0, cC = 0;")
         else:
-            K.append("  const long long cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
-        K.append("  const long long t = (long long)bx * blockDim.x + tid;")
+            K.append(f"  const {T} cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
+        K.append(f"  const {T} t = ({T})bx * blockDim.x + tid;")
         K.append("  if (t < cA + cB + cC) {")
-        K.append("    long long i, j, k;")
+        K.append(f"    {T} i, j, k;")
         K.append("    if (t < cA) {            // planes within RAD of a dim-0 face")
-        K.append("      const long long q = t / (n1 * n2), r = t - q * n1 * n2;")
+        K.append(f"      const {T} q = {dv('t', 'n1 * n2')}, r = t - q * n1 * n2;")
         K.append("      i = q < c_low ? g_lo + q : hs + (q - c_low);")
-        K.append("      j = r / n2; k = r - j * n2;")
+        K.append(f"      j = {dv('r', 'n2')}; k = r - j * n2;")
         K.append("    } else if (t < cA + cB) { // interior planes, rows within RAD of a dim-1 face")
-        K.append("      const long long u = t - cA, w1 = n1 - a1;")
-        K.append("      const long long q = u / (w1 * n2), r = u - q * w1 * n2;")
-        K.append("      const long long jr = r / n2, lo = min((long long)RAD, n1);")
+        K.append(f"      const {T} u = t - cA, w1 = n1 - a1;")
+        K.append(f"      const {T} q = {dv('u', 'w1 * n2')}, r = u - q * w1 * n2;")
+        K.append(f"      const {T} jr = {dv('r', 'n2')}, lo = min(({T})RAD, n1);")
         K.append("      i = ii0 + q; j = jr < lo ? jr : n1 - (w1 - jr); k = r - jr * n2;")
         K.append("    } else {                  // interior rows, columns within RAD of a dim-2 face")
         # row-major (both faces' columns of a row next to each other): measured faster
         # on B200 than one face column per warp, which walks rows n2 apart
-        K.append("      const long long u = t - cA - cB, w2 = n2 - a2;")
-        K.append("      const long long q = u / (a1 * w2), r = u - q * a1 * w2;")
-        K.append("      const long long jr = r / w2, kr = r - jr * w2, lo = min((long long)RAD, n2);")
+        K.append(f"      const {T} u = t - cA - cB, w2 = n2 - a2;")
+        K.append(f"      const {T} q = {dv('u', 'a1 * w2')}, r = u - q * a1 * w2;")
+        K.append(f"      const {T} jr = {dv('r', 'w2')}, kr = r - jr * w2, lo = min(({T})RAD, n2);")
         K.append("      i = ii0 + q; j = RAD + jr; k = kr < lo ? kr : n2 - (w2 - kr);")
         K.append("    }")
         K.append("    const int gi = (int)i;")

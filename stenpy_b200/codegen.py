@@ -592,6 +592,33 @@ class _Emitter:
         for c in range(n.nc):
             body.append(f"{o}[{c}] = ({raws[0][c]} {sym} {raws[1][c]}) * {s};")
 
+    def point_raw(self, nid: int, body: List[str]) -> str:
+        """Interior value of node nid (``raw_scale(graph, nid)`` is not None) at the
+        thread's voxel (0, M, KK) without its spacing factor: central differences
+        and stacks of them left unscaled."""
+        n = self.g.nodes[nid]
+        arr = self.t()
+        if n.op == "stack":
+            parts = [self.point_raw(i, body) for i in n.ins]
+            body.append(f"float {arr}[{n.nc}];")
+            self.pointwise(n, parts, arr, body)
+            return arr
+        body.append(f"float {arr}[{n.nc}];")
+        pair = n.op != "d1"
+        raws = []
+        for d in ([self.g.nodes[i] for i in n.ins] if pair else [n]):
+            ax, comp = d.a("axis"), d.a("comp")
+            plus = ["0", "M", "KK"]; plus[ax] = f"({plus[ax]}) + 1"
+            minus = ["0", "M", "KK"]; minus[ax] = f"({minus[ax]}) - 1"
+            a = self.fast_call(d.ins[0], *plus, body)
+            b = self.fast_call(d.ins[0], *minus, body)
+            raws.append([f"({a}[{c if comp is None else comp}] - {b}[{c if comp is None else comp}])"
+                         for c in range(d.nc)])
+        for c in range(n.nc):
+            v = raws[0][c] if not pair else f"{raws[0][c]} {'+' if n.op == 'add' else '-'} {raws[1][c]}"
+            body.append(f"{arr}[{c}] = {v};")
+        return arr
+
     def _tap_sum(self, n: PNode, vals, o: str, body: List[str]) -> None:
         """o = scale * Σ w·v over (array, weight) pairs, accumulated in tap order."""
         for c in range(n.nc):
@@ -845,7 +872,7 @@ class _Emitter:
             return arr
 
         for r, off in zip(roots, self.offsets):
-            arr = point(r.node)
+            arr = self.point_raw(r.node, body) if deferred_scale(self.s, r) else point(r.node)
             for c in range(self.g.nodes[r.node].nc):
                 body.append(f"rv[{off + c}] = {arr}[{c}];")
         self.lines.append("template <int M, int KK> __device__ __forceinline__ void eval_fast(const FCtx& x, float* rv) {")
@@ -1252,6 +1279,42 @@ def _sum_from_var(spec: PassSpec, r: RootSpec) -> Optional[int]:
     return None
 
 
+def raw_scale(g: "PGraph", nid: int) -> Optional[float]:
+    """s when node nid's interior value is s times an unscaled expression that
+    ``_Emitter.point_raw`` gives: a central difference (s = 1/2h), a sum or
+    difference of two central differences with one spacing, or a stack of those
+    with one s."""
+    n = g.nodes[nid]
+    if n.op == "d1":
+        return None if n.a("mode") == "zero" else float(n.a("inv2h"))
+    if n.op in ("add", "sub") and len(n.ins) == 2:
+        a, b = (g.nodes[i] for i in n.ins)
+        if (a.op == b.op == "d1" and a.a("mode") != "zero" and b.a("mode") != "zero"
+                and a.a("inv2h") == b.a("inv2h") and a.nc == b.nc == n.nc):
+            return float(a.a("inv2h"))
+        return None
+    if n.op == "stack":
+        got = {raw_scale(g, i) for i in n.ins}
+        return got.pop() if len(got) == 1 and None not in got else None
+    return None
+
+
+def deferred_scale(spec: PassSpec, r: RootSpec) -> Optional[float]:
+    """Factor s^2 applied once to the main z-march's FP64 accumulator of the sum of
+    squares ``r``, whose voxels then accumulate unscaled (three multiplies fewer per
+    voxel for a curl's norm). Only where every voxel of that kernel is an interior
+    evaluation (faces in the shell kernel, which keeps its own scaled partial rows,
+    or in ghost cells) and s is a power of two: scaling by 2^e commutes with every
+    FP32 and FP64 rounding, so the sums are bit for bit those of scaled values
+    (outside the exponent range's ends)."""
+    if r.kind != "red" or r.red != "sumsq" or spec.radius == 0 or spec.has_scan:
+        return None
+    s = raw_scale(spec.graph, r.node)
+    if s is None or s == 1.0 or s <= 0.0 or math.frexp(s)[0] != 0.5:
+        return None
+    return s * s
+
+
 def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
     """Block-reduce each accumulator and write this CTA's partial row; add the
     CTA's histogram counts to the global (integer, order-free) histogram."""
@@ -1291,7 +1354,9 @@ def _red_flush(spec: PassSpec, cta: str, where: str = "main") -> List[str]:
             K.append(f"{{ const double a_ = block_min(rv{ri}_a, red_scratch); const double b_ = block_max(rv{ri}_b, red_scratch);")
             K.append(f"  if (tid == 0) {{ {base}] = a_; {base} + 1] = b_; }} }}")
         else:
-            K.append(f"{{ const double a_ = block_sum(rv{ri}_a, red_scratch); if (tid == 0) {base}] = a_; }}")
+            ds = deferred_scale(spec, r) if where == "main" else None
+            acc = f"rv{ri}_a" if ds is None else f"rv{ri}_a * {ds!r}"
+            K.append(f"{{ const double a_ = block_sum({acc}, red_scratch); if (tid == 0) {base}] = a_; }}")
     return K
 
 

@@ -135,6 +135,28 @@ def test_16bit_fields_with_one_sided_edges_keep_fp32_accuracy(dtype):
                 assert rel_err(got, ref) <= 1e-5, (expr, shape, ghost, rel_err(got, ref))
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
+def test_norm_of_curl_scales_exactly_with_power_of_two_spacing(dtype):
+    """The z-march sums the squares of unscaled central differences and applies
+    (1/2h)^2 once to each CTA's partial (the faces' kernel keeps scaled values in
+    rows of its own). With power-of-two spacings that is bit for bit the sum of the
+    scaled squares, so halving dx exactly doubles the norm; other spacings scale per
+    voxel and meet the oracle as before."""
+    import stenpy_b200 as S
+    from stenpy_b200.synth import smoothed_vector
+    dev = _dev()
+    for shape in [(20, 33, 130), (9, 16, 64)]:
+        u = smoothed_vector(shape, seed=11).to(dtype)
+        vals = {}
+        for dx in (1.0, 0.5, 0.25, 0.3):
+            g, sink, *_ = S.compile_expression("l2norm(curl(u))", dx=dx, boundary="neumann", field_map={"u": u.to(dev)})
+            vals[dx] = float(S.Runtime(device=dev).run(g)[sink])
+            g2, s2, *_ = S.compile_expression("l2norm(curl(u))", dx=dx, boundary="neumann", field_map={"u": u.double()})
+            ref = float(O.evaluate(g2, [s2])[s2])
+            assert abs(vals[dx] - ref) <= 1e-6 * abs(ref), (shape, dx, vals[dx], ref)
+        assert vals[1.0] * 2 == vals[0.5] and vals[0.5] * 2 == vals[0.25], (shape, vals)
+
+
 @pytest.mark.parametrize("kv", [1, 2])
 @pytest.mark.parametrize("tk,tj", [(32, 16), (64, 8)])
 @pytest.mark.parametrize("shape", [(10, 17, 65), (9, 33, 97), (12, 18, 66)])

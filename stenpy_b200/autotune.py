@@ -29,7 +29,7 @@ import torch
 from . import _native as N
 from . import fused_compiler as FC
 from .codegen import (ESIZE, SHELL_THREADS, PassConfig, PassSpec, emit_pass, is_flat, pass_grid, plane_bytes,
-                      shell_count, shell_regions, smem_layout, valid_shape, with_config)
+                      shell_count, shell_ctas, shell_regions, smem_layout, valid_shape, with_config)
 
 LOG_PATH = os.environ.get("STENPY_TUNE_LOG", os.path.join(os.path.dirname(os.path.abspath(__file__)),
                                                           "_tune", "timings.jsonl"))
@@ -173,7 +173,7 @@ def _launches(pp: FC.PassPlan, spec: PassSpec, values: Dict[str, Any], shape, de
                 seg_len=cfg.seg_len, tiles_k=tiles_k, cta_off=0)
     ls = [(grid, (cfg.threads, 1, 1), FC.pack_params(spec, vals, tmaps))]
     if FC.has_shell(spec):
-        sh = -(-shell_count(shape, spec.radius, regions=shell_regions(spec)) // SHELL_THREADS)
+        sh = shell_ctas(shell_count(shape, spec.radius, regions=shell_regions(spec)))
         ls.append(((sh, 1, 1), (SHELL_THREADS, 1, 1), FC.pack_params(spec, dict(vals, cta_off=ncta), tmaps)))
     return ls, outs, ncta
 
@@ -188,7 +188,7 @@ def time_schedule(pp: FC.PassPlan, cfg: PassConfig, values: Dict[str, Any], shap
     key, cubin = N.compile_cached(src, FC.NVRTC_OPTS)
     mod = N.load_module(key, cubin, "sten_kernel", smem, dev_idx)
     shell_mod = N.load_module(key + ":shell", cubin, "sten_shell", 0, dev_idx) if FC.has_shell(spec) else None
-    n_shell = -(-shell_count(shape, spec.radius, regions=shell_regions(spec)) // SHELL_THREADS)
+    n_shell = shell_ctas(shell_count(shape, spec.radius, regions=shell_regions(spec)))
     gx, gy = pass_grid(spec, shape[1], shape[2], shape[0])
     tiles = gx * gy
     part = torch.empty(max((tiles + n_shell) * spec.nslots, 1), dtype=torch.float64, device=device)

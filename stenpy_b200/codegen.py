@@ -1761,6 +1761,13 @@ def shell_count(shape: Tuple[int, int, int], R: int, g_lo: int = 0, g_hi: Option
 
 
 SHELL_THREADS = 256
+SHELL_MAX_CTAS = 148 * 8   # blocks of the shell launch: 8 resident per SM on 148 SMs
+
+
+def shell_ctas(n_shell: int) -> int:
+    """Blocks of a ``sten_shell`` launch over ``n_shell`` voxels (the kernel strides
+    over the rest); each writes one partial row."""
+    return min(-(-n_shell // SHELL_THREADS), SHELL_MAX_CTAS)
 
 
 def _flat_body(spec: PassSpec, e: "_Emitter", red_off: int, batch: bool) -> List[str]:
@@ -1850,8 +1857,9 @@ def _flat_body(spec: PassSpec, e: "_Emitter", red_off: int, batch: bool) -> List
 
 def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int = 0) -> str:
     """Source of the pass: ``sten_kernel`` (z-march over the tile grid) and, when the
-    pass has a stencil reach R > 0 and no scan, ``sten_shell`` (one thread per voxel
-    within R of a face, evaluated from global memory with boundary rules); with
+    pass has a stencil reach R > 0 and no scan, ``sten_shell`` (the voxels within R
+    of a face, one per thread per stride of the grid, evaluated from global memory
+    with boundary rules); with
     histogram roots also ``sten_hist_final`` (entropy from the counts).
 
     With ``batch_ns`` the same code is emitted as device functions in that
@@ -2312,8 +2320,14 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
             K.append(f"  const {T} cA = (c_low + c_high) * n1 * n2, cB = 0, cC = 0;")
         else:
             K.append(f"  const {T} cA = (c_low + c_high) * n1 * n2, cB = n_int * (n1 - a1) * n2, cC = n_int * a1 * (n2 - a2);")
-        K.append(f"  const {T} t = ({T})bx * blockDim.x + tid;")
-        K.append("  if (t < cA + cB + cC) {")
+        if batch:
+            # a work item is one block of shell voxels
+            K.append(f"  const {T} t = ({T})bx * blockDim.x + tid;")
+            K.append("  if (t < cA + cB + cC) {")
+        else:
+            # at most SHELL_MAX_CTAS blocks stride over the shell: fewer partial rows
+            # for the finalize and one block reduction per resident block
+            K.append(f"  for ({T} t = ({T})bx * blockDim.x + tid; t < cA + cB + cC; t += ({T})gridDim.x * blockDim.x) {{")
         K.append(f"    {T} i, j, k;")
         K.append("    if (t < cA) {            // planes within RAD of a dim-0 face")
         K.append(f"      const {T} q = {dv('t', 'n1 * n2')}, r = t - q * n1 * n2;")

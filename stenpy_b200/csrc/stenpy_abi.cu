@@ -372,38 +372,33 @@ __global__ void __launch_bounds__(256) sten_finalize_kernel(const double* __rest
   }
   double x0 = 0.0, x1 = 0.0, x2 = 0.0;
   if (d.kind == STENPY_RED_MIN_MAX) { x0 = INFINITY; x1 = -INFINITY; }
-  // rows t, t + 256, ... folded in that order; the loads of FOLD_U rows are issued
-  // before their folds so that their latencies overlap (the order, and so the result,
-  // is the same as one row at a time)
+  // rows t, t + 256, ... folded in that order; the loads of up to FOLD_U rows are
+  // issued before their folds so that their latencies overlap, the last group's
+  // only for the rows that exist (the order, and so the result, is the same as one
+  // row at a time)
   const int width = d.kind == STENPY_RED_VARIANCE ? 3 : (d.kind == STENPY_RED_ENTROPY || d.kind == STENPY_RED_MIN_MAX ? 2 : 1);
-  constexpr int FOLD_U = 8;
-  int c = t;
-  for (; c + (FOLD_U - 1) * 256 < ncta; c += FOLD_U * 256) {
+  constexpr int FOLD_U = 16;
+  for (int c = t; c < ncta; c += FOLD_U * 256) {
     double v[FOLD_U][3];
 #pragma unroll
     for (int u = 0; u < FOLD_U; ++u) {
-      const double* row = part + (size_t)(c + u * 256) * nslots + d.slot;
-      v[u][0] = row[0];
-      v[u][1] = width > 1 ? row[1] : 0.0;
-      v[u][2] = width > 2 ? row[2] : 0.0;
+      v[u][0] = v[u][1] = v[u][2] = 0.0;
+      if (c + u * 256 < ncta) {
+        const double* row = part + (size_t)(c + u * 256) * nslots + d.slot;
+        v[u][0] = row[0];
+        if (width > 1) v[u][1] = row[1];
+        if (width > 2) v[u][2] = row[2];
+      }
     }
 #pragma unroll
     for (int u = 0; u < FOLD_U; ++u) {
+      if (c + u * 256 >= ncta) break;
       switch (d.kind) {
         case STENPY_RED_VARIANCE: chan(x0, x1, x2, v[u][0], v[u][1], v[u][2]); break;
         case STENPY_RED_ENTROPY: x0 += v[u][0]; x1 += v[u][1]; break;
         case STENPY_RED_MIN_MAX: x0 = fmin(x0, v[u][0]); x1 = fmax(x1, v[u][1]); break;
         default: x0 += v[u][0]; break;
       }
-    }
-  }
-  for (; c < ncta; c += 256) {
-    const double* row = part + (size_t)c * nslots + d.slot;
-    switch (d.kind) {
-      case STENPY_RED_VARIANCE: chan(x0, x1, x2, row[0], row[1], row[2]); break;
-      case STENPY_RED_ENTROPY: x0 += row[0]; x1 += row[1]; break;
-      case STENPY_RED_MIN_MAX: x0 = fmin(x0, row[0]); x1 = fmax(x1, row[1]); break;
-      default: x0 += row[0]; break;
     }
   }
   s0[t] = x0; s1[t] = x1; s2[t] = x2;

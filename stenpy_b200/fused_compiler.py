@@ -34,7 +34,7 @@ import torch
 
 from . import _native as N
 from .codegen import (ESIZE, SHELL_THREADS, STENCIL_PRIMS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec,
-                      analyse_ghosts, emit_pass, param_layout, pass_grid, shell_count, shell_regions,
+                      analyse_ghosts, emit_pass, param_layout, pass_grid, shell_count, shell_ctas, shell_regions,
                       smem_layout, tmap_specs)
 from .graph import Graph
 from .lowering import LoweringError, OpLowerer, dx3
@@ -699,8 +699,8 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
             if nid in plan.wanted:
                 results[nid] = o
         n_shell = shell_count(plan.shape, spec.radius, regions=shell_regions(spec))
-        shell_ctas = -(-n_shell // SHELL_THREADS)
-        total_cta = ncta + shell_ctas
+        n_sh_cta = shell_ctas(n_shell)
+        total_cta = ncta + n_sh_cta
         part = plan.buffers.get(f"part{pi}")
         need = total_cta * spec.nslots
         if part is None or part.numel() < need:
@@ -711,13 +711,13 @@ def build_program(plan: FusedPlan, values: Dict[str, Any], device: torch.device,
                                         n2=n2, nl=n0, i_base=0, out_lo=0, n_out=n0, seg_len=cfg.seg_len,
                                         tiles_k=tiles_k, cta_off=0), tmaps)
         ops.append(Launch(pp.module, grid, (cfg.threads, 1, 1), pp.smem, params))
-        if shell_ctas:
+        if n_sh_cta:
             shell_params = pack_params(spec, dict(fld=fptrs, out=[o.data_ptr() for o in outs],
                                                   scal=table.data_ptr(), part=part.data_ptr(), hist=hist_ptr,
                                                   err=err.data_ptr(), n0g=n0, n1=n1, n2=n2, nl=n0, i_base=0,
                                                   out_lo=0, n_out=n0, seg_len=cfg.seg_len, tiles_k=tiles_k,
                                                   cta_off=ncta), tmaps)
-            ops.append(Launch(pp.shell_module, (shell_ctas, 1, 1), (SHELL_THREADS, 1, 1), 0, shell_params))
+            ops.append(Launch(pp.shell_module, (n_sh_cta, 1, 1), (SHELL_THREADS, 1, 1), 0, shell_params))
         if pp.reductions:
             descs = [N.ReduceDesc(r.kind, r.slot, r.table_index, r.unbiased, r.count, r.eps)
                      for r in pp.reductions]

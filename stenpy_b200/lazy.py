@@ -32,7 +32,7 @@ import torch
 
 from . import _native as N
 from . import fused_compiler as FC
-from .codegen import SHELL_THREADS, PassConfig, pass_grid, shell_count, shell_regions
+from .codegen import SHELL_THREADS, PassConfig, pass_grid, shell_count, shell_ctas, shell_regions
 from .graph import Graph
 
 
@@ -82,7 +82,7 @@ def chunk_launches(pp: FC.PassPlan, c: Chunk, shape: Tuple[int, int, int], fptrs
                 tiles_k=-(-n2 // cfg.tk), cta_off=cta_off)
     ncta = grid[0] * grid[1]
     n_shell = shell_count(shape, spec.radius, c.s, c.e, shell_regions(spec)) if FC.has_shell(spec) else 0
-    sh = -(-n_shell // SHELL_THREADS)
+    sh = shell_ctas(n_shell)
     main = FC.Launch(pp.module, grid, (cfg.threads, 1, 1), pp.smem, FC.pack_params(spec, vals, tmaps))
     shell = None
     if sh:
@@ -97,7 +97,7 @@ def chunk_rows(pp: FC.PassPlan, c: Chunk, shape: Tuple[int, int, int]) -> int:
     spec = pp.spec
     gx, gy = pass_grid(spec, n1, n2, c.e - c.s)
     n_shell = shell_count(shape, spec.radius, c.s, c.e, shell_regions(spec)) if FC.has_shell(spec) else 0
-    return gx * gy + -(-n_shell // SHELL_THREADS)
+    return gx * gy + shell_ctas(n_shell)
 
 
 def slab_pieces(c: Chunk, n0: int) -> List[Tuple[int, int, int]]:

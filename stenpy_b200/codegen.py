@@ -501,6 +501,25 @@ class _Emitter:
             for c in range(n.nc):
                 body.append(f"{arr}[{c}] = ldg_as_f32(x.gp{f.slot} + {c});")
 
+    def central_diffs(self, d: PNode, di: str, dj: str, dk: str, body: List[str]) -> List[str]:
+        """Per component, the unscaled central difference f(+1) - f(-1) of the d1 node d
+        along its axis at offset (di, dj, dk). From a 16-bit staged field the minuend
+        is not converted: one mixed-precision subtraction (LDS) takes it as stored
+        and the subtrahend as FP32 (the same rounding as the FP32 difference)."""
+        off = [di, dj, dk]
+        ax, comp = d.a("axis"), d.a("comp")
+        plus = list(off); plus[ax] = f"({off[ax]}) + 1"
+        minus = list(off); minus[ax] = f"({off[ax]}) - 1"
+        src = self.g.nodes[d.ins[0]]
+        b = self.fast_call(d.ins[0], *minus, body)
+        cs = [c if comp is None else comp for c in range(d.nc)]
+        if src.op == "field":
+            f = self.s.fields[src.a("field")]
+            if f.staged and ESIZE[f.dtype] == 2:
+                return [f"LDS{f.slot}<{plus[0]}, {plus[1]}, ({plus[2]}) * {f.nc} + {c}>(x, {b}[{c}])" for c in cs]
+        a = self.fast_call(d.ins[0], *plus, body)
+        return [f"({a}[{c}] - {b}[{c}])" for c in cs]
+
     def fast_value(self, n: PNode, di: str, dj: str, dk: str, o: str, body: List[str]) -> None:
         """Statements computing node n at offset (di,dj,dk) into array o (interior)."""
         if n.op == "field":
@@ -517,15 +536,9 @@ class _Emitter:
                 for c in range(n.nc):
                     body.append(f"{o}[{c}] = 0.0f;")
                 return
-            off = [di, dj, dk]
-            plus = list(off); plus[ax] = f"({off[ax]}) + 1"
-            minus = list(off); minus[ax] = f"({off[ax]}) - 1"
-            a = self.fast_call(n.ins[0], *plus, body)
-            b = self.fast_call(n.ins[0], *minus, body)
             s = _lit(n.a("inv2h"))
-            for c in range(n.nc):
-                cc = c if comp is None else comp
-                body.append(f"{o}[{c}] = ({a}[{cc}] - {b}[{cc}]) * {s};")
+            for c, dv in enumerate(self.central_diffs(n, di, dj, dk, body)):
+                body.append(f"{o}[{c}] = {dv} * {s};")
             return
         if n.op == "lap":
             off = [di, dj, dk]
@@ -576,17 +589,7 @@ class _Emitter:
     def d1_pair_value(self, n: PNode, di: str, dj: str, dk: str, o: str, body: List[str]) -> None:
         """o = ((a1 - b1) +/- (a2 - b2)) * inv2h for the two d1 inputs of n (the same
         value as scaling each difference first when inv2h is a power of two)."""
-        raws = []
-        for nid in n.ins:
-            d = self.g.nodes[nid]
-            off = [di, dj, dk]
-            ax, comp = d.a("axis"), d.a("comp")
-            plus = list(off); plus[ax] = f"({off[ax]}) + 1"
-            minus = list(off); minus[ax] = f"({off[ax]}) - 1"
-            a = self.fast_call(d.ins[0], *plus, body)
-            b = self.fast_call(d.ins[0], *minus, body)
-            raws.append([f"({a}[{c if comp is None else comp}] - {b}[{c if comp is None else comp}])"
-                         for c in range(d.nc)])
+        raws = [self.central_diffs(self.g.nodes[nid], di, dj, dk, body) for nid in n.ins]
         sym = "+" if n.op == "add" else "-"
         s = _lit(self.g.nodes[n.ins[0]].a("inv2h"))
         for c in range(n.nc):
@@ -605,15 +608,8 @@ class _Emitter:
             return arr
         body.append(f"float {arr}[{n.nc}];")
         pair = n.op != "d1"
-        raws = []
-        for d in ([self.g.nodes[i] for i in n.ins] if pair else [n]):
-            ax, comp = d.a("axis"), d.a("comp")
-            plus = ["0", "M", "KK"]; plus[ax] = f"({plus[ax]}) + 1"
-            minus = ["0", "M", "KK"]; minus[ax] = f"({minus[ax]}) - 1"
-            a = self.fast_call(d.ins[0], *plus, body)
-            b = self.fast_call(d.ins[0], *minus, body)
-            raws.append([f"({a}[{c if comp is None else comp}] - {b}[{c if comp is None else comp}])"
-                         for c in range(d.nc)])
+        raws = [self.central_diffs(d, "0", "M", "KK", body)
+                for d in ([self.g.nodes[i] for i in n.ins] if pair else [n])]
         for c in range(n.nc):
             v = raws[0][c] if not pair else f"{raws[0][c]} {'+' if n.op == 'add' else '-'} {raws[1][c]}"
             body.append(f"{arr}[{c}] = {v};")
@@ -1959,6 +1955,16 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
         else:
             L.append(f"  return ld_as_f32((const {ct}*)row_ + E);")
         L.append("}")
+        if es == 2:
+            # the same element minus an FP32 value, in one mixed-precision subtraction
+            L.append(f"template <int DI, int DJ, int E> __device__ __forceinline__ float LDS{f.slot}(const FCtx& x, float c) {{")
+            L.append(f"  const unsigned char* row_ = sten_smem + x.sb{f.slot}[DI + RAD] + DJ * {ring_w(spec, f) * es};")
+            if chunk:
+                L.append(f"  if constexpr (E >= 0 && E < {cfg.kv * f.nc}) return chunk_sub<{ct}, {cw}, E * {es}>(row_, c);")
+                L.append(f"  else return sub_as_f32((const {ct}*)row_ + E, c);")
+            else:
+                L.append(f"  return sub_as_f32((const {ct}*)row_ + E, c);")
+            L.append("}")
     e.emit_fast_fns()
     e.emit_slow_fns()
     e.emit_eval()

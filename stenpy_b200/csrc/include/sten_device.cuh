@@ -74,6 +74,48 @@ STEN_DEV float f16_lo_to_f32(u32 w) {
 STEN_DEV float f16_hi_to_f32(u32 w) {
   float f; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; cvt.f32.f16 %0, h_; }" : "=f"(f) : "r"(w)); return f;
 }
+// a - c for a 16-bit element a (the low / high half of a 32-bit word) and an FP32 c
+// in one mixed-precision subtraction (sm_100 sub.f32.f16 / sub.f32.bf16): a is
+// widened exactly and the difference rounded once to FP32, the value of the FP32
+// subtraction of the converted element, without the conversion instruction.
+STEN_DEV float f16_lo_sub_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; sub.rn.f32.f16 %0, l_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float f16_hi_sub_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; sub.rn.f32.f16 %0, h_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float bf16_lo_sub_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; sub.rn.f32.bf16 %0, l_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float bf16_hi_sub_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; sub.rn.f32.bf16 %0, h_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float sub_as_f32(const f16_t* p, float c) {
+  float d; asm("sub.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(p->bits), "f"(c)); return d;
+}
+STEN_DEV float sub_as_f32(const bf16_t* p, float c) {
+  float d; asm("sub.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(p->bits), "f"(c)); return d;
+}
+// element at byte B of the chunk minus c (16-bit T)
+template <typename T, int CW, int B>
+STEN_DEV float chunk_sub(const unsigned char* row, float c) {
+  u32 w;
+  if constexpr (CW % 16 == 0) {
+    const uint4 v = *(const uint4*)(row + (B / 16) * 16);
+    constexpr int q = (B % 16) / 4;
+    w = q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+  } else if constexpr (CW % 8 == 0) {
+    const uint2 v = *(const uint2*)(row + (B / 8) * 8);
+    w = ((B % 8) / 4) == 0 ? v.x : v.y;
+  } else {
+    w = *(const u32*)(row + (B / 4) * 4);
+  }
+  if constexpr (is_bf16_t<T>::value) {
+    return (B % 4) ? bf16_hi_sub_f32(w, c) : bf16_lo_sub_f32(w, c);
+  } else {
+    return (B % 4) ? f16_hi_sub_f32(w, c) : f16_lo_sub_f32(w, c);
+  }
+}
 template <typename T, int CW, int B>
 STEN_DEV float chunk_elem(const unsigned char* row) {
   u32 w;

@@ -135,6 +135,32 @@ def test_16bit_fields_with_one_sided_edges_keep_fp32_accuracy(dtype):
                 assert rel_err(got, ref) <= 1e-5, (expr, shape, ghost, rel_err(got, ref))
 
 
+@pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
+def test_16bit_central_differences_equal_fp32_of_the_stored_values(dtype):
+    """Interior central differences of 16-bit fields take the stored minuend in one
+    mixed-precision subtraction: bit for bit the FP32 difference of the converted
+    values, so FP32 results equal those of the same values stored in FP32 at every
+    voxel off the faces (whose one-sided rules run in another order)."""
+    import stenpy_b200 as S
+    from stenpy_b200.synth import sinusoid_field, smoothed_vector
+    dev = _dev()
+    for shape in [(12, 20, 64), (9, 17, 37)]:
+        u = smoothed_vector(shape, seed=21).to(dtype)
+        f = sinusoid_field(shape, seed=22).to(dtype)
+        for expr in ("curl(u)", "divergence(u)", "gradient(f)", "l2norm(curl(u))"):
+            outs = []
+            for cast in (lambda t: t, lambda t: t.float()):
+                fm = {"u": cast(u).to(dev)} if "(u)" in expr else {"f": cast(f).to(dev)}
+                g, sink, *_ = S.compile_expression(expr, boundary="periodic", field_map=fm)
+                outs.append(S.Runtime(device=dev, out_dtype=torch.float32).run(g)[sink])
+            if outs[0].dim() == 0:
+                # the norm's faces come from the shell (16-bit) or ghost cells (FP32)
+                assert abs(float(outs[0]) - float(outs[1])) <= 1e-6 * abs(float(outs[1])), (expr, shape)
+                continue
+            a, b = (o[1:-1, 1:-1, 1:-1] for o in outs)
+            assert torch.equal(a, b), (expr, shape, (a - b).abs().max().item())
+
+
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
 def test_norm_of_curl_scales_exactly_with_power_of_two_spacing(dtype):
     """The z-march sums the squares of unscaled central differences and applies

@@ -551,10 +551,24 @@ class _Emitter:
                 b = self.fast_call(n.ins[0], *minus, body)
                 terms.append((a, b, _lit(n.a("invh2")[ax])))
             h2 = n.a("invh2")
+            src = self.g.nodes[n.ins[0]]
+            f16 = None
+            if src.op == "field":
+                fs = self.s.fields[src.a("field")]
+                f16 = fs if fs.staged and ESIZE[fs.dtype] == 2 else None
             for c in range(n.nc):
                 if h2[0] == h2[1] == h2[2]:
-                    # equal spacing: the six neighbours summed, then one fused -6 c
-                    ssum = " + ".join(f"({a}[{c}] + {b}[{c}])" for a, b, _ in terms)
+                    # equal spacing: the six neighbours summed, then one fused -6 c; from a
+                    # 16-bit staged field each pair's first value is added as stored
+                    # (add.f32.f16: the rounding of the FP32 sum, without its conversion)
+                    if f16 is not None:
+                        pairs = []
+                        for ax in range(3):
+                            q = list(off); q[ax] = f"({off[ax]}) + 1"
+                            pairs.append(f"LDA{f16.slot}<{q[0]}, {q[1]}, ({q[2]}) * {f16.nc} + {c}>(x, {terms[ax][1]}[{c}])")
+                        ssum = " + ".join(f"({t})" for t in pairs)
+                    else:
+                        ssum = " + ".join(f"({a}[{c}] + {b}[{c}])" for a, b, _ in terms)
                     v = f"fmaf(-6.0f, {ctr}[{c}], {ssum})"
                     body.append(f"{o}[{c}] = {v if h2[0] == 1.0 else f'{v} * {terms[0][2]}'};")
                     continue
@@ -1964,6 +1978,15 @@ def emit_pass(spec: PassSpec, batch_ns: Optional[str] = None, batch_threads: int
                 L.append(f"  else return sub_as_f32((const {ct}*)row_ + E, c);")
             else:
                 L.append(f"  return sub_as_f32((const {ct}*)row_ + E, c);")
+            L.append("}")
+            # ... and plus an FP32 value
+            L.append(f"template <int DI, int DJ, int E> __device__ __forceinline__ float LDA{f.slot}(const FCtx& x, float c) {{")
+            L.append(f"  const unsigned char* row_ = sten_smem + x.sb{f.slot}[DI + RAD] + DJ * {ring_w(spec, f) * es};")
+            if chunk:
+                L.append(f"  if constexpr (E >= 0 && E < {cfg.kv * f.nc}) return chunk_sub<{ct}, {cw}, E * {es}, true>(row_, c);")
+                L.append(f"  else return add_as_f32((const {ct}*)row_ + E, c);")
+            else:
+                L.append(f"  return add_as_f32((const {ct}*)row_ + E, c);")
             L.append("}")
     e.emit_fast_fns()
     e.emit_slow_fns()

@@ -90,14 +90,33 @@ STEN_DEV float bf16_lo_sub_f32(u32 w, float c) {
 STEN_DEV float bf16_hi_sub_f32(u32 w, float c) {
   float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; sub.rn.f32.bf16 %0, h_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
 }
+// a + c likewise (add.f32.f16 / add.f32.bf16)
+STEN_DEV float f16_lo_add_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; add.rn.f32.f16 %0, l_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float f16_hi_add_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; add.rn.f32.f16 %0, h_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float bf16_lo_add_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; add.rn.f32.bf16 %0, l_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float bf16_hi_add_f32(u32 w, float c) {
+  float d; asm("{ .reg .b16 l_, h_; mov.b32 {l_, h_}, %1; add.rn.f32.bf16 %0, h_, %2; }" : "=f"(d) : "r"(w), "f"(c)); return d;
+}
+STEN_DEV float add_as_f32(const f16_t* p, float c) {
+  float d; asm("add.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(p->bits), "f"(c)); return d;
+}
+STEN_DEV float add_as_f32(const bf16_t* p, float c) {
+  float d; asm("add.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(p->bits), "f"(c)); return d;
+}
 STEN_DEV float sub_as_f32(const f16_t* p, float c) {
   float d; asm("sub.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(p->bits), "f"(c)); return d;
 }
 STEN_DEV float sub_as_f32(const bf16_t* p, float c) {
   float d; asm("sub.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(p->bits), "f"(c)); return d;
 }
-// element at byte B of the chunk minus c (16-bit T)
-template <typename T, int CW, int B>
+// element at byte B of the chunk minus c (ADD false) or plus c (ADD true), 16-bit T
+template <typename T, int CW, int B, bool ADD = false>
 STEN_DEV float chunk_sub(const unsigned char* row, float c) {
   u32 w;
   if constexpr (CW % 16 == 0) {
@@ -110,8 +129,12 @@ STEN_DEV float chunk_sub(const unsigned char* row, float c) {
   } else {
     w = *(const u32*)(row + (B / 4) * 4);
   }
-  if constexpr (is_bf16_t<T>::value) {
+  if constexpr (is_bf16_t<T>::value && ADD) {
+    return (B % 4) ? bf16_hi_add_f32(w, c) : bf16_lo_add_f32(w, c);
+  } else if constexpr (is_bf16_t<T>::value) {
     return (B % 4) ? bf16_hi_sub_f32(w, c) : bf16_lo_sub_f32(w, c);
+  } else if constexpr (ADD) {
+    return (B % 4) ? f16_hi_add_f32(w, c) : f16_lo_add_f32(w, c);
   } else {
     return (B % 4) ? f16_hi_sub_f32(w, c) : f16_lo_sub_f32(w, c);
   }

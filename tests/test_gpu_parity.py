@@ -137,17 +137,18 @@ def test_16bit_fields_with_one_sided_edges_keep_fp32_accuracy(dtype):
 
 @pytest.mark.parametrize("dtype", [torch.float16, torch.bfloat16])
 def test_16bit_central_differences_equal_fp32_of_the_stored_values(dtype):
-    """Interior central differences of 16-bit fields take the stored minuend in one
-    mixed-precision subtraction: bit for bit the FP32 difference of the converted
-    values, so FP32 results equal those of the same values stored in FP32 at every
-    voxel off the faces (whose one-sided rules run in another order)."""
+    """Interior central differences (and the Laplacian's neighbour pairs) of 16-bit
+    fields take one stored value in a mixed-precision subtraction (addition): bit
+    for bit the FP32 result of the converted values, so FP32 results equal those of
+    the same values stored in FP32 at every voxel off the faces (whose one-sided
+    rules run in another order)."""
     import stenpy_b200 as S
     from stenpy_b200.synth import sinusoid_field, smoothed_vector
     dev = _dev()
     for shape in [(12, 20, 64), (9, 17, 37)]:
         u = smoothed_vector(shape, seed=21).to(dtype)
         f = sinusoid_field(shape, seed=22).to(dtype)
-        for expr in ("curl(u)", "divergence(u)", "gradient(f)", "l2norm(curl(u))"):
+        for expr in ("curl(u)", "divergence(u)", "gradient(f)", "laplacian(f)", "l2norm(curl(u))"):
             outs = []
             for cast in (lambda t: t, lambda t: t.float()):
                 fm = {"u": cast(u).to(dev)} if "(u)" in expr else {"f": cast(f).to(dev)}

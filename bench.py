@@ -60,7 +60,7 @@ HEADLINE = "fp16"
 # at 512^3 (pass 0: curl-norm partials, pass 1: Laplacian with statistics), from an
 # ncu capture of these kernels (profiles/ summary of sten_kernel at 512^3, FP16); the
 # line reports the dominant pass's; null for other sizes or forms
-NCU_TRAFFIC = {("fp16", 512, 0): 829520384 + 3828480, ("fp16", 512, 1): 286163712 + 232444160}
+NCU_TRAFFIC = {("fp16", 512, 0): 829856000 + 3907584, ("fp16", 512, 1): 284617984 + 231344640}
 
 
 def _peaks():

@@ -198,6 +198,59 @@ def test_shell_decode_matches_boundary_shell():
                 assert set(got) == truth and len(set(got)) == cnt, (shape, R, g_lo, g_hi)
 
 
+def test_shell_blocks_stride_over_every_voxel_once():
+    """The shell launch has at most SHELL_MAX_CTAS blocks; their grid-stride loop
+    (t = block * 256 + thread, step blocks * 256) visits every shell voxel index once,
+    and the partial rows the finalize folds are the blocks launched."""
+    from stenpy_b200.codegen import SHELL_MAX_CTAS, SHELL_THREADS, shell_ctas
+    for n in (1, 255, 256, 257, SHELL_MAX_CTAS * SHELL_THREADS - 1, SHELL_MAX_CTAS * SHELL_THREADS + 1,
+              3 * SHELL_MAX_CTAS * SHELL_THREADS + 17):
+        b = shell_ctas(n)
+        assert 1 <= b <= SHELL_MAX_CTAS and b == min(-(-n // SHELL_THREADS), SHELL_MAX_CTAS)
+        seen = torch.zeros(n, dtype=torch.int32)
+        stride = b * SHELL_THREADS
+        for first in range(stride):
+            seen[first:n:stride] += 1
+        assert bool((seen == 1).all()), n
+
+
+def test_32bit_shell_indexing_only_when_offsets_fit_an_int():
+    """The planner enables 32-bit boundary indexing from the field shapes: every
+    element offset of n0 (+ halo planes) x n1 x n2 x components must stay below 2^31."""
+    def plan(n):
+        u = torch.zeros(1).expand(n, n, n, 3)
+        g, sink, *_ = S.compile_expression("l2norm(curl(u))", boundary="neumann", field_map={"u": u})
+        return FC.Planner(g, [sink]).plan()
+    assert plan(512).passes[0].spec.idx32
+    assert not plan(1024).passes[0].spec.idx32      # 1026 * 1024 * 1024 * 3 > 2^31
+    src = FC.emit_pass(plan(1024).passes[0].spec)
+    assert "const long long n0 = p.n0g" in src and "const int n0 = p.n0g" not in src
+
+
+@pytest.mark.parametrize("dx,expect", [(1.0, 0.25), (0.25, 4.0), (0.5, None), (0.3, None)])
+def test_deferred_scale_of_curl_norm_only_for_power_of_two_spacing(dx, expect):
+    """The z-march sums unscaled squares of the curl's differences and scales its
+    block partial by (1/2h)^2 only when 1/2h is a power of two other than 1 (exact);
+    the shell keeps scaled values and an unscaled flush."""
+    from stenpy_b200.codegen import deferred_scale
+    u = torch.zeros(20, 24, 32, 3)
+    g, sink, *_ = S.compile_expression("l2norm(curl(u))", dx=dx, boundary="neumann", field_map={"u": u})
+    spec = FC.Planner(g, [sink]).plan().passes[0].spec
+    root = [r for r in spec.roots if r.kind == "red"][0]
+    assert deferred_scale(spec, root) == expect
+    src = FC.emit_pass(spec)
+    main, shell = src.split("sten_shell(")[0], src.split("sten_shell(")[1]
+    if expect is None:
+        assert "block_sum(rv0_a * " not in main
+    else:
+        assert f"block_sum(rv0_a * {expect!r}, red_scratch)" in main
+    assert "block_sum(rv0_a, red_scratch)" in shell
+    # a plain sum of the same vector keeps per-voxel scaling
+    g2, s2, *_ = S.compile_expression("sum(curl(u))", dx=dx, boundary="neumann", field_map={"u": u})
+    spec2 = FC.Planner(g2, [s2]).plan().passes[0].spec
+    assert all(deferred_scale(spec2, r) is None for r in spec2.roots)
+
+
 def test_cpu_device_is_rejected():
     with pytest.raises(NotImplementedError):
         S.Runtime(device="cpu")

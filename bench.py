@@ -14,9 +14,11 @@ Storage forms, compute always FP32 with FP64 reductions:
 
 ``value`` = Gvoxel/s of the headline form, inputs resident in HBM, one step = one
 CUDA-graph replay of the whole plan (kernels + finalizes). ``e2e`` = the same step
-through the public API (compile_expression + Runtime.run) from pinned host
-buffers, with host->device copies of f and u and device->host reads of the result
-field and the three scalars inside the timed region.
+through the public out-of-core API (compile_expression + LazyPipeline) from pinned
+host buffers, with the host->device copies of f and u and the device->host reads of
+the result field and the three scalars inside the timed region, streamed in
+64-plane chunks so that copies and kernels overlap; ``e2e.runtime_run`` is the
+whole-field call (Runtime.run: every copy, then the kernels, then the reads).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--size S] [--forms fp32,fp16,bf16]
@@ -261,6 +263,35 @@ class E2E:
         return self.out_host, self.scal_host
 
 
+E2E_CHUNK = 64   # planes per chunk of the streamed end-to-end run
+
+
+class E2EStreamed:
+    """The same step through the public out-of-core API (``LazyPipeline``, the
+    counterpart of the reference's ``Runtime.run_chunked``): the fields stay in pinned
+    host memory and every step streams them in 64-plane chunks, so each pass's uploads,
+    kernels and result downloads overlap on three streams (chunk c + 1 uploads while c
+    computes and c - 1 downloads; the Laplacian pass's field uploads start while the
+    curl pass finishes). Per-voxel results are those of the whole-field run."""
+
+    def __init__(self, f_host, u_host, form, device):
+        import stenpy_b200 as S
+        from stenpy_b200.lazy import LazyPipeline
+        self.dt, self.odt = FORMS[form]
+        g, self.sink, *_ = S.compile_expression(EXPR, dx=1.0, boundary="periodic",
+                                                field_map={"f": f_host, "u": u_host})
+        self.wanted = [self.sink] + [g.add(r, (self.sink,), {}) for r in REDS]
+        self.pipe = LazyPipeline(g, self.wanted, device, out_dtype=self.odt, chunk=E2E_CHUNK)
+        self.pipe.prepare()
+        self.idx = [self.pipe.plan.red_index[w] for w in self.wanted[1:]]
+        self.scal_host = torch.empty(len(REDS), dtype=torch.float64, pin_memory=True)
+
+    def step(self, f_host, u_host):
+        self.pipe.enqueue()
+        self.scal_host.copy_(self.pipe.table[self.idx], non_blocking=True)
+        return self.pipe.host_out[self.sink], self.scal_host
+
+
 def e2e_step(f_host, u_host, form, device, runner=None):
     """One step through the public API from pinned host buffers."""
     runner = runner or E2E(f_host, u_host, form, device)
@@ -269,11 +300,11 @@ def e2e_step(f_host, u_host, form, device, runner=None):
     return out, scal
 
 
-def measure_e2e(f, u, form, device, steps, world, dev):
+def measure_e2e(f, u, form, device, steps, world, dev, streamed=False):
     dt = FORM_DT[form]
     f_host = f.to(dt).cpu().pin_memory()
     u_host = u.to(dt).cpu().pin_memory()
-    runner = E2E(f_host, u_host, form, device)
+    runner = (E2EStreamed if streamed else E2E)(f_host, u_host, form, device)
     for _ in range(2):
         e2e_step(f_host, u_host, form, device, runner)
     torch.cuda.synchronize()
@@ -894,9 +925,14 @@ def main():
                          "step_frac": round(head["step_frac_of_peak"], 4), "forms": summary},
             "gpu_launches": head["launches_per_step"] * args.steps, "clocks": clocks}
     if not args.no_e2e:
-        ms, h2d, d2h = measure_e2e(f, u, head_form, dev, args.steps, world, dev)
+        # the headline end-to-end figure streams the host fields through the
+        # out-of-core API; the whole-field Runtime.run call is reported beside it
+        ms, h2d, d2h = measure_e2e(f, u, head_form, dev, args.steps, world, dev, streamed=True)
+        ms_run, _, _ = measure_e2e(f, u, head_form, dev, args.steps, world, dev)
         line["e2e"] = {"value": n_vox * world / (ms * 1e-3) / 1e9, "unit": "Gvoxel/s",
-                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms}
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms,
+                       "api": f"LazyPipeline, pinned host fields streamed in {E2E_CHUNK}-plane chunks",
+                       "runtime_run": {"value": n_vox * world / (ms_run * 1e-3) / 1e9, "ms_per_step": ms_run}}
     if rank == 0 and not args.no_cpu:
         sec, vox, step, sample_ref = time_reference(args.size, 3, 1)
         line["cpu_baseline"] = {"value": vox / sec / 1e9, "unit": "Gvoxel/s", "cores": torch.get_num_threads(),

@@ -110,3 +110,35 @@ def test_captured_chunk_schedule_replays_bit_identically():
         assert torch.equal(again[sinks[k]], ref[sinks2[k]].cpu()), k
     assert abs(float(again[mn]) - float(ref[mn2])) <= 1e-12 * max(1.0, abs(float(ref[mn2])))
     del graph
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16])
+def test_streamed_config1_step_equals_whole_field(dtype):
+    """The end-to-end benchmark's streamed step: the two-phase config-1 graph (curl
+    norm, then Laplacian + that scalar with sum/mean/variance) run chunk by chunk from
+    pinned host fields gives the whole-field results: the same voxels up to one
+    rounding of the output dtype (the scalar added is the same FP64 sum up to the
+    order of its partial rows) and the same statistics to FP32 rounding of the plane
+    sums (a thread's variance pivot is its first voxel, which a chunk moves)."""
+    import stenpy_b200 as S
+    from stenpy_b200.lazy import LazyPipeline
+    from stenpy_b200.synth import sinusoid_field, smoothed_vector
+    dev = _dev()
+    shape = (40, 24, 64)
+    f = sinusoid_field(shape, seed=31).to(dtype)
+    u = smoothed_vector(shape, seed=32).to(dtype)
+    expr = "divergence(gradient(f)) + l2norm(curl(u))"
+    g, sink, *_ = S.compile_expression(expr, boundary="periodic", field_map={"f": f.to(dev), "u": u.to(dev)})
+    w = [sink] + [g.add(r, (sink,), {}) for r in ("sum", "mean", "variance")]
+    whole = S.Runtime(device=dev, out_dtype=dtype).run(g, wanted=w)
+    gh, sinkh, *_ = S.compile_expression(expr, boundary="periodic",
+                                         field_map={"f": f.pin_memory(), "u": u.pin_memory()})
+    wh = [sinkh] + [gh.add(r, (sinkh,), {}) for r in ("sum", "mean", "variance")]
+    lp = LazyPipeline(gh, wh, dev, out_dtype=dtype, chunk=8)
+    res = lp.run()
+    assert len(lp.passes[0]["chunks"]) == 5
+    a, b = whole[sink].cpu().float(), res[sinkh].float()
+    tol = 1e-6 if dtype == torch.float32 else 1e-3
+    assert (a - b).abs().max().item() <= tol * a.abs().max().item()
+    for x, y in zip(w[1:], wh[1:]):
+        assert abs(float(whole[x]) - float(res[y])) <= 1e-6 * max(1e-6, abs(float(whole[x]))), (x, y)

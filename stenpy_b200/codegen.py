@@ -137,8 +137,9 @@ class PassSpec:
     ghosts: Optional[Dict[Tuple[int, int], str]] = None
     i_periodic: bool = False   # every tap along dim 0 wraps: planes are loaded wrapped
     nested_ok: bool = False    # dims 1 and 2 have >= 4 points (two-layer extrapolation)
-    idx32: bool = False        # every element offset of every array fits in an int: the
-                               # boundary (shell) code indexes in 32-bit arithmetic
+    idx32: bool = False        # every element offset of every array, plus one stride of
+                               # the shell launch, fits in an int: the boundary (shell)
+                               # code indexes in 32-bit arithmetic
 
     def hk(self, f: FieldSpec) -> int:
         """k-halo in elements. TMA-staged fields: rounded so TMA x-coordinates stay

@@ -33,7 +33,7 @@ from typing import Any, Dict, List, Optional, Sequence, Set, Tuple
 import torch
 
 from . import _native as N
-from .codegen import (ESIZE, SHELL_THREADS, STENCIL_PRIMS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec,
+from .codegen import (ESIZE, SHELL_MAX_CTAS, SHELL_THREADS, STENCIL_PRIMS, FieldSpec, PassConfig, PassSpec, PGraph, RootSpec,
                       analyse_ghosts, emit_pass, param_layout, pass_grid, shell_count, shell_ctas, shell_regions,
                       smem_layout, tmap_specs)
 from .graph import Graph
@@ -425,10 +425,11 @@ class Planner:
         spec = PassSpec(pg, fields, rspecs, self.table_size, max(nslots, 1), radius, cfg, has_scan)
         spec.nested_ok = self.shape[1] >= 4 and self.shape[2] >= 4
         # arrays hold at most n0 planes plus halo planes on both sides (a chunk of
-        # the planes holds fewer): element offsets of all of them stay below 2^31
+        # the planes holds fewer): element offsets of all of them, and the shell
+        # kernel's voxel index plus one grid stride, stay below 2^31
         max_nc = max([f.nc for f in fields] + [pg.nodes[r.node].nc for r in rspecs] + [1])
         spec.idx32 = ((self.shape[0] + 2 * radius + 2) * self.shape[1] * self.shape[2] * max_nc
-                      < 1 << 31)
+                      + SHELL_MAX_CTAS * SHELL_THREADS < 1 << 31)
         n2 = self.shape[2]
         for f in fields:
             # every field goes through a TMA-filled plane ring when the layout allows;

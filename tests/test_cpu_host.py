@@ -251,6 +251,24 @@ def test_deferred_scale_of_curl_norm_only_for_power_of_two_spacing(dx, expect):
     assert all(deferred_scale(spec2, r) is None for r in spec2.roots)
 
 
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float16, torch.bfloat16])
+def test_mixed_precision_operands_only_for_16bit_staged_fields(dtype):
+    """Central differences and Laplacian pairs of 16-bit staged fields take one value
+    as stored (LDS / LDA accessors: sub/add.f32.f16 or .bf16); FP32 fields keep plain
+    FP32 arithmetic. The kernels compile for sm_100a either way."""
+    u = torch.zeros(20, 24, 32, 3, dtype=dtype)
+    f = torch.zeros(20, 24, 32, dtype=dtype)
+    g, sink, *_ = S.compile_expression("divergence(gradient(f)) + l2norm(curl(u))", boundary="periodic",
+                                       field_map={"f": f, "u": u})
+    plan = FC.Planner(g, [sink]).plan()
+    a, b = (FC.emit_pass(pp.spec) for pp in plan.passes)
+    sixteen = dtype != torch.float32
+    assert ("LDS0<" in a) == sixteen and ("LDA0<" in b) == sixteen
+    for src in (a, b):
+        _, cubin = N.compile_cached(src, FC.NVRTC_OPTS)
+        assert len(cubin) > 1000
+
+
 def test_cpu_device_is_rejected():
     with pytest.raises(NotImplementedError):
         S.Runtime(device="cpu")
